@@ -1,0 +1,146 @@
+"""ctypes binding of libb40c_bfs.so (the C ABI in include/b40c_bfs.h).
+
+Loading fails loudly when the library has not been built: there is no CPU
+fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_PKG, "lib", "libb40c_bfs.so")
+
+# status codes (numerically equal to cudaError_t)
+SUCCESS = 0
+ERROR_INVALID_VALUE = 1
+ERROR_MEMORY_ALLOCATION = 2
+ERROR_INVALID_CONFIGURATION = 9
+ERROR_INVALID_DEVICE_FUNCTION = 98
+ERROR_NO_DEVICE = 100
+ERROR_NOT_READY = 600
+ERROR_LAUNCH_TIMEOUT = 702
+ERROR_NOT_SUPPORTED = 801
+
+VERTEX_FRONTIERS, EDGE_FRONTIERS, MIXED_FRONTIERS, MULTI_GPU_FRONTIERS = 0, 1, 2, 3
+EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID = 0, 1, 2, 3
+ENACT_FUSED, ENACT_ITERATIVE, ENACT_GRAPH = 0, 1, 2
+
+
+class Policy(C.Structure):
+    _fields_ = [
+        ("threads", C.c_int32),
+        ("ctas_per_sm", C.c_int32),
+        ("chunk_edges", C.c_int32),
+        ("warp_gather_threshold", C.c_int32),
+        ("cta_gather_threshold", C.c_int32),
+        ("saturation_quit", C.c_int32),
+        ("warp_cull", C.c_int32),
+        ("bitmask_precheck", C.c_int32),
+    ]
+
+
+class DeviceView(C.Structure):
+    _fields_ = [
+        ("d_row_offsets", C.c_void_p),
+        ("d_column_indices", C.c_void_p),
+        ("d_labels", C.c_void_p),
+        ("d_visited_mask", C.c_void_p),
+        ("visited_mask_bytes", C.c_int64),
+        ("nodes", C.c_int64),
+        ("edges", C.c_int64),
+        ("device", C.c_int32),
+        ("mark_predecessors", C.c_int32),
+    ]
+
+
+class Csr(C.Structure):
+    _fields_ = [
+        ("nodes", C.c_int64),
+        ("edges", C.c_int64),
+        ("row_offsets", C.POINTER(C.c_int32)),
+        ("column_indices", C.POINTER(C.c_int32)),
+        ("pinned", C.c_int32),
+    ]
+
+
+class B40cError(RuntimeError):
+    """A non-zero status from the library; ``.status`` is the cudaError_t value."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+_P_i32 = C.POINTER(C.c_int32)
+_P_i64 = C.POINTER(C.c_int64)
+
+# name -> (restype, argtypes); every symbol declared in include/b40c_bfs.h
+SIGNATURES: dict[str, tuple] = {
+    "b40c_last_error_string": (C.c_char_p, []),
+    "b40c_version": (C.c_char_p, []),
+    "b40c_device_count": (C.c_int, [_P_i32]),
+    "b40c_bfs_default_policy": (C.c_int, [C.c_int, C.POINTER(Policy)]),
+    "b40c_bfs_problem_create": (C.c_int, [_P_i32, _P_i32, C.c_int64, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                          C.POINTER(C.c_void_p)]),
+    "b40c_bfs_problem_destroy": (C.c_int, [C.c_void_p]),
+    "b40c_bfs_set_stream": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "b40c_bfs_problem_reset": (C.c_int, [C.c_void_p, C.c_int, C.c_double]),
+    "b40c_bfs_enact": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int32, C.c_int, C.POINTER(Policy)]),
+    "b40c_bfs_enact_limited": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int,
+                                         C.POINTER(Policy)]),
+    "b40c_bfs_extract": (C.c_int, [C.c_void_p, _P_i32]),
+    "b40c_bfs_stats": (C.c_int, [C.c_void_p, _P_i64, _P_i32, C.POINTER(C.c_double)]),
+    "b40c_bfs_last_elapsed_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
+    "b40c_bfs_recent_search_ms": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
+    "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
+    "b40c_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, C.c_int]),
+    "b40c_host_free": (C.c_int, [C.c_void_p]),
+    "b40c_build_grid2d": (C.c_int, [C.c_int32, C.c_int, C.POINTER(Csr)]),
+    "b40c_build_grid3d": (C.c_int, [C.c_int32, C.c_int, C.POINTER(Csr)]),
+    "b40c_build_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_double,
+                                  C.c_uint64, C.c_int, C.c_int, C.POINTER(Csr)]),
+    "b40c_build_random": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.POINTER(Csr)]),
+    "b40c_build_rr": (C.c_int, [C.c_int64, C.c_int32, C.c_int, C.c_uint64, C.c_int, C.POINTER(Csr)]),
+    "b40c_csr_from_coo": (C.c_int, [_P_i32, _P_i32, C.c_int64, C.c_int64, C.c_int, C.POINTER(Csr)]),
+    "b40c_sample_sources": (C.c_int, [C.POINTER(Csr), C.c_int32, C.c_uint64, _P_i32]),
+    "b40c_graph_free": (None, [C.POINTER(Csr)]),
+}
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libb40c_bfs.so (built in-tree by back40computing_b200.build)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with `python -m back40computing_b200.build` "
+                "(the BFS path has no CPU fallback)")
+        handle = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(handle, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = handle
+    return _lib
+
+
+def check(status: int, what: str = "") -> None:
+    if status != SUCCESS:
+        msg = lib().b40c_last_error_string().decode(errors="replace")
+        raise B40cError(status, f"{what}: {msg}" if what else msg)
+
+
+def i32p(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_P_i32)
+
+
+def device_count() -> int:
+    c = C.c_int32(0)
+    check(lib().b40c_device_count(C.byref(c)), "b40c_device_count")
+    return c.value

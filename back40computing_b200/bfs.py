@@ -1,0 +1,208 @@
+"""BFS problem and enactors (b40c/graph/bfs), the host-side mirror of the
+reference's C++ interface over the C ABI.
+
+* ``CsrProblem``  -- bfs::CsrProblem (csr_problem.cuh:72-756)
+* ``EnactorExpandContract`` / ``EnactorContractExpand`` / ``EnactorTwoPhase``
+  / ``EnactorHybrid`` -- the four single-GPU enactors, with
+  ``EnactFusedSearch`` / ``EnactIterativeSearch`` / ``EnactSearch`` and
+  ``GetStatistics`` returning ``(total_queued, search_depth, avg_duty)``.
+
+Methods return the cudaError_t status like the reference (0 on success); the
+``*_or_raise`` helpers and ``search()`` raise ``B40cError`` instead.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+from .graph import CsrGraph
+
+VERTEX_FRONTIERS = N.VERTEX_FRONTIERS
+EDGE_FRONTIERS = N.EDGE_FRONTIERS
+MIXED_FRONTIERS = N.MIXED_FRONTIERS
+MULTI_GPU_FRONTIERS = N.MULTI_GPU_FRONTIERS
+
+EXPAND_CONTRACT = N.EXPAND_CONTRACT
+CONTRACT_EXPAND = N.CONTRACT_EXPAND
+TWO_PHASE = N.TWO_PHASE
+HYBRID = N.HYBRID
+
+Policy = N.Policy
+
+
+def default_policy(strategy: int) -> N.Policy:
+    pol = N.Policy()
+    N.check(N.lib().b40c_bfs_default_policy(int(strategy), C.byref(pol)), "b40c_bfs_default_policy")
+    return pol
+
+
+class CsrProblem:
+    """Device-resident CSR plus per-search state (labels, visited mask, queues)."""
+
+    def __init__(self, mark_predecessors: bool = False, device: int = 0):
+        self.MARK_PREDECESSORS = bool(mark_predecessors)
+        self.device = int(device)
+        self.nodes = 0
+        self.edges = 0
+        self.num_gpus = 0
+        self._h = C.c_void_p(None)
+        self._keep = None  # host arrays kept alive for stream-from-host
+
+    # csr_problem.cuh:328-540
+    def FromHostProblem(self, stream_from_host: bool, nodes: int, edges: int, column_indices, row_offsets,
+                        num_gpus: int = 1) -> int:
+        if num_gpus != 1:
+            N.lib()  # loads (and fails loudly) even on the error path
+            return N.ERROR_INVALID_VALUE
+        self.Destroy()
+        ro = np.ascontiguousarray(row_offsets, dtype=np.int32)
+        ci = np.ascontiguousarray(column_indices, dtype=np.int32)
+        h = C.c_void_p()
+        status = N.lib().b40c_bfs_problem_create(N.i32p(ro), N.i32p(ci) if ci.size else None, int(nodes), int(edges),
+                                                 int(self.MARK_PREDECESSORS), int(bool(stream_from_host)),
+                                                 self.device, C.byref(h))
+        if status == N.SUCCESS:
+            self._h = h
+            self.nodes, self.edges, self.num_gpus = int(nodes), int(edges), 1
+            self._keep = (ro, ci) if stream_from_host else None
+        return status
+
+    @classmethod
+    def from_graph(cls, graph: CsrGraph, mark_predecessors: bool = False, device: int = 0,
+                   stream_from_host: bool = False) -> "CsrProblem":
+        p = cls(mark_predecessors, device)
+        N.check(p.FromHostProblem(stream_from_host, graph.nodes, graph.edges, graph.column_indices,
+                                  graph.row_offsets, 1), "FromHostProblem")
+        return p
+
+    @property
+    def handle(self) -> C.c_void_p:
+        if not self._h:
+            raise N.B40cError(N.ERROR_INVALID_VALUE, "problem not initialised (FromHostProblem)")
+        return self._h
+
+    # csr_problem.cuh:547-750
+    def Reset(self, frontier_type: int, queue_sizing: float = 1.3) -> int:
+        return N.lib().b40c_bfs_problem_reset(self.handle, int(frontier_type), float(queue_sizing))
+
+    # csr_problem.cuh:255-322
+    def ExtractResults(self, h_labels: np.ndarray) -> int:
+        assert h_labels.dtype == np.int32 and h_labels.size >= self.nodes
+        return N.lib().b40c_bfs_extract(self.handle, N.i32p(h_labels))
+
+    def labels(self) -> np.ndarray:
+        out = np.empty(self.nodes, dtype=np.int32)
+        N.check(self.ExtractResults(out), "ExtractResults")
+        return out
+
+    def set_stream(self, stream_handle: int | None) -> None:
+        N.check(N.lib().b40c_bfs_set_stream(self.handle, C.c_void_p(stream_handle or None)), "set_stream")
+
+    def last_elapsed_ms(self) -> float:
+        ms = C.c_float(0)
+        N.check(N.lib().b40c_bfs_last_elapsed_ms(self.handle, C.byref(ms)), "last_elapsed_ms")
+        return float(ms.value)
+
+    def recent_search_ms(self, count: int) -> np.ndarray:
+        out = (C.c_float * int(count))()
+        N.check(N.lib().b40c_bfs_recent_search_ms(self.handle, int(count), out), "recent_search_ms")
+        return np.array(out[:], dtype=np.float64)
+
+    def device_view(self) -> N.DeviceView:
+        v = N.DeviceView()
+        N.check(N.lib().b40c_bfs_device_view_get(self.handle, C.byref(v)), "device_view")
+        return v
+
+    def Destroy(self) -> None:
+        if self._h:
+            N.lib().b40c_bfs_problem_destroy(self._h)
+            self._h = C.c_void_p(None)
+
+    def __del__(self):
+        try:
+            self.Destroy()
+        except Exception:
+            pass
+
+
+class _Enactor:
+    STRATEGY = -1
+    FRONTIER = VERTEX_FRONTIERS
+
+    def __init__(self, DEBUG: bool = False, policy: N.Policy | None = None):
+        self.DEBUG = DEBUG
+        self.policy = policy
+        self._problem: CsrProblem | None = None
+
+    def GetFrontierType(self) -> int:
+        return self.FRONTIER
+
+    def _enact(self, problem: CsrProblem, src: int, mode: int, max_grid_size: int, depth_limit: int = -1) -> int:
+        self._problem = problem
+        pol = C.byref(self.policy) if self.policy is not None else None
+        return N.lib().b40c_bfs_enact_limited(problem.handle, self.STRATEGY, int(mode), int(src), int(depth_limit),
+                                              int(max_grid_size), pol)
+
+    def EnactFusedSearch(self, problem: CsrProblem, src: int, max_grid_size: int = 0) -> int:
+        return self._enact(problem, src, N.ENACT_FUSED, max_grid_size)
+
+    def EnactIterativeSearch(self, problem: CsrProblem, src: int, max_grid_size: int = 0) -> int:
+        return self._enact(problem, src, N.ENACT_ITERATIVE, max_grid_size)
+
+    def EnactGraphSearch(self, problem: CsrProblem, src: int, max_grid_size: int = 0) -> int:
+        return self._enact(problem, src, N.ENACT_GRAPH, max_grid_size)
+
+    def GetStatistics(self) -> tuple[int, int, float]:
+        if self._problem is None:
+            return 0, 0, 0.0
+        tq, depth, duty = C.c_int64(0), C.c_int32(0), C.c_double(0)
+        N.check(N.lib().b40c_bfs_stats(self._problem.handle, C.byref(tq), C.byref(depth), C.byref(duty)),
+                "GetStatistics")
+        return int(tq.value), int(depth.value), float(duty.value)
+
+
+class EnactorExpandContract(_Enactor):
+    """enactor_expand_contract.cuh:59 -- vertex frontiers, fused expand+contract."""
+    STRATEGY = EXPAND_CONTRACT
+    FRONTIER = VERTEX_FRONTIERS
+
+
+class EnactorContractExpand(_Enactor):
+    """enactor_contract_expand.cuh:61 -- edge frontiers, fused contract+expand."""
+    STRATEGY = CONTRACT_EXPAND
+    FRONTIER = EDGE_FRONTIERS
+
+
+class EnactorTwoPhase(_Enactor):
+    """enactor_two_phase.cuh:68 -- separate contract and expand kernels per level."""
+    STRATEGY = TWO_PHASE
+    FRONTIER = MIXED_FRONTIERS
+
+
+class EnactorHybrid(_Enactor):
+    """enactor_hybrid.cuh:64 -- fused contract-expand, two-phase while saturated."""
+    STRATEGY = HYBRID
+    FRONTIER = EDGE_FRONTIERS
+
+    def EnactSearch(self, problem: CsrProblem, src: int, max_grid_size: int = 0) -> int:
+        return self._enact(problem, src, N.ENACT_FUSED, max_grid_size)
+
+
+ENACTORS = {
+    EXPAND_CONTRACT: EnactorExpandContract,
+    CONTRACT_EXPAND: EnactorContractExpand,
+    TWO_PHASE: EnactorTwoPhase,
+    HYBRID: EnactorHybrid,
+}
+
+
+def search(problem: CsrProblem, src: int, strategy: int = EXPAND_CONTRACT, mode: int = N.ENACT_FUSED,
+           depth_limit: int = -1, queue_sizing: float = 1.3, policy: N.Policy | None = None,
+           max_grid_size: int = 0) -> np.ndarray:
+    """Reset + one search + extract; raises on any failure.  Returns labels[n]."""
+    enactor = ENACTORS[strategy](policy=policy)
+    N.check(problem.Reset(enactor.GetFrontierType(), queue_sizing), "Reset")
+    N.check(enactor._enact(problem, src, mode, max_grid_size, depth_limit), "Enact")
+    return problem.labels()

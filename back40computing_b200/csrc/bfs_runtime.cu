@@ -1,0 +1,690 @@
+// Host runtime of the BFS library: problem state (CsrProblem), the enactors
+// (per-level launches, persistent grid, CUDA-graph replay) and the C ABI.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "b40c_bfs.h"
+#include "bfs_kernels.cuh"
+#include "bfs_strategies.cuh"
+#include "errors.h"
+
+using namespace b40c;
+using b40c::dev::LookbackSlot;
+
+#define B40C_VERSION_STRING "b40c-b200 0.1 (sm_100a)"
+
+namespace {
+
+constexpr int kThreads = 256;
+
+#define CUDA_TRY(call, what)                                                                             \
+    do {                                                                                                 \
+        cudaError_t _e = (call);                                                                         \
+        if (_e != cudaSuccess) {                                                                         \
+            cudaGetLastError();                                                                          \
+            return b40c::fail((int)_e, "%s failed: %s", what, cudaGetErrorString(_e));                  \
+        }                                                                                                \
+    } while (0)
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace
+
+struct b40c_bfs_problem {
+    int device = 0;
+    int64_t nodes = 0, edges = 0;
+    int mark_pred = 0;
+    int stream_from_host = 0;
+    int sms = 0;
+    // CSR
+    int32_t *d_ro = nullptr, *d_ci = nullptr;
+    bool own_csr = true;
+    const void *reg_ro = nullptr, *reg_ci = nullptr;  // host arrays registered for zero-copy
+    // search arrays
+    int32_t *d_labels = nullptr;
+    uint32_t *d_mask = nullptr;
+    int32_t mask_words = 0;
+    // frontiers
+    VertexFrontier vf[2] = {};
+    int64_t vcap[2] = {0, 0};
+    EdgeFrontier ef[2] = {};
+    int64_t ecap[2] = {0, 0};
+    double queue_sizing = 1.3;
+    LookbackSlot *slots = nullptr;
+    int32_t max_slots = 0;
+    SearchState *st = nullptr;
+    SearchState *h_st = nullptr;  // pinned mirror
+    // streams / timing
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // ring of event pairs bracketing the search kernels (after source set-up)
+    // of the most recent enacts, for per-launch device times
+    static constexpr int kRing = 256;
+    cudaEvent_t ring_a[kRing] = {}, ring_b[kRing] = {};
+    int ring_pos = 0, ring_count = 0;
+    bool timed = false;
+    bool needs_init = true;  // labels/mask dirty since the last reset
+    // last search
+    int64_t total_queued = 0;
+    int32_t search_depth = 0;
+    double avg_duty = 0.0;
+    bool stats_valid = false;
+    int last_strategy = -1;
+};
+
+namespace {
+
+int alloc_dev(void **p, size_t bytes, const char *what)
+{
+    cudaError_t e = cudaMalloc(p, std::max<size_t>(bytes, 16));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "cudaMalloc %s (%zu bytes) failed: %s", what, bytes,
+                          cudaGetErrorString(e));
+    }
+    return B40C_SUCCESS;
+}
+
+void free_vf(VertexFrontier &f)
+{
+    if (f.v) cudaFree(f.v);
+    if (f.col) cudaFree(f.col);
+    if (f.P) cudaFree(f.P);
+    f = VertexFrontier{};
+}
+void free_ef(EdgeFrontier &f)
+{
+    if (f.v) cudaFree(f.v);
+    if (f.pred) cudaFree(f.pred);
+    f = EdgeFrontier{};
+}
+
+int ensure_vf(b40c_bfs_problem *p, int i, int64_t cap)
+{
+    cap = std::max<int64_t>(cap, 1);
+    if (p->vcap[i] >= cap) return B40C_SUCCESS;
+    free_vf(p->vf[i]);
+    p->vcap[i] = 0;
+    int rc;
+    if ((rc = alloc_dev((void **)&p->vf[i].v, sizeof(int32_t) * cap, "vertex frontier"))) return rc;
+    if ((rc = alloc_dev((void **)&p->vf[i].col, sizeof(int32_t) * cap, "vertex frontier"))) return rc;
+    if ((rc = alloc_dev((void **)&p->vf[i].P, sizeof(int32_t) * (cap + 1), "vertex frontier"))) return rc;
+    p->vcap[i] = cap;
+    return B40C_SUCCESS;
+}
+
+int ensure_ef(b40c_bfs_problem *p, int i, int64_t cap)
+{
+    cap = std::max<int64_t>(cap, 1);
+    if (p->ecap[i] >= cap && (!p->mark_pred || p->ef[i].pred)) return B40C_SUCCESS;
+    free_ef(p->ef[i]);
+    p->ecap[i] = 0;
+    int rc;
+    if ((rc = alloc_dev((void **)&p->ef[i].v, sizeof(int32_t) * cap, "edge frontier"))) return rc;
+    if (p->mark_pred && (rc = alloc_dev((void **)&p->ef[i].pred, sizeof(int32_t) * cap, "edge frontier"))) return rc;
+    p->ecap[i] = cap;
+    return B40C_SUCCESS;
+}
+
+int64_t cap_of(double qs, int64_t base)
+{
+    double c = std::ceil(qs * (double)base);
+    if (c > (double)INT32_MAX - 1) c = (double)INT32_MAX - 1;
+    return (int64_t)c;
+}
+
+// Look-back slots: one per chunk of the largest possible level.
+int ensure_slots(b40c_bfs_problem *p)
+{
+    const int64_t need = (std::max(p->edges, p->nodes) + 255) / 256 + 4096;
+    if (p->max_slots >= need) return B40C_SUCCESS;
+    if (p->slots) cudaFree(p->slots);
+    p->slots = nullptr;
+    p->max_slots = 0;
+    int rc = alloc_dev((void **)&p->slots, sizeof(LookbackSlot) * need, "look-back slots");
+    if (rc) return rc;
+    CUDA_TRY(cudaMemsetAsync(p->slots, 0, sizeof(LookbackSlot) * need, p->stream), "memset look-back slots");
+    p->max_slots = (int32_t)need;
+    return B40C_SUCCESS;
+}
+
+BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
+{
+    BfsParams k{};
+    k.row_offsets = p->d_ro;
+    k.column_indices = p->d_ci;
+    k.labels = p->d_labels;
+    k.mask = p->d_mask;
+    k.nodes = (int32_t)p->nodes;
+    k.edges = (int32_t)p->edges;
+    k.mask_words = p->mask_words;
+    k.vcap = (int32_t)std::min(p->vcap[0] ? p->vcap[0] : INT32_MAX, p->vcap[1] ? p->vcap[1] : INT32_MAX);
+    k.ecap = (int32_t)std::min(p->ecap[0] ? p->ecap[0] : INT32_MAX, p->ecap[1] ? p->ecap[1] : INT32_MAX);
+    k.max_chunks = p->max_slots;
+    k.vf[0] = p->vf[0];
+    k.vf[1] = p->vf[1];
+    k.ef[0] = p->ef[0];
+    k.ef[1] = p->ef[1];
+    k.slots = p->slots;
+    k.st = p->st;
+    k.max_levels = 1;
+    k.chunk_edges = pol.chunk_edges;
+    k.warp_thresh = pol.warp_gather_threshold;
+    k.cta_thresh = pol.cta_gather_threshold;
+    k.warp_cull = pol.warp_cull;
+    k.precheck = pol.bitmask_precheck;
+    k.saturation = pol.saturation_quit;
+    k.persistent = 0;
+    k.skip_arrival_cta = -1;
+    k.cond_handle = 0;
+    return k;
+}
+
+b40c_bfs_policy default_policy(int strategy)
+{
+    b40c_bfs_policy pol{};
+    pol.threads = kThreads;
+    pol.ctas_per_sm = 0;
+    pol.chunk_edges = dev::kChunkMax;
+    pol.warp_gather_threshold = 32;
+    pol.cta_gather_threshold = 512;
+    pol.saturation_quit = 512;  // SATURATION_QUIT = 4 * 128 (enactor_hybrid.cuh:571)
+    pol.warp_cull = 0;
+    pol.bitmask_precheck = 1;
+    (void)strategy;
+    return pol;
+}
+
+int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out)
+{
+    b40c_bfs_policy d = default_policy(strategy);
+    if (in) {
+        if (in->threads) d.threads = in->threads;
+        if (in->ctas_per_sm) d.ctas_per_sm = in->ctas_per_sm;
+        if (in->chunk_edges) d.chunk_edges = in->chunk_edges;
+        if (in->warp_gather_threshold) d.warp_gather_threshold = in->warp_gather_threshold;
+        if (in->cta_gather_threshold) d.cta_gather_threshold = in->cta_gather_threshold;
+        if (in->saturation_quit) d.saturation_quit = in->saturation_quit;
+        if (in->warp_cull) d.warp_cull = in->warp_cull > 0 ? 1 : 0;
+        if (in->bitmask_precheck) d.bitmask_precheck = in->bitmask_precheck > 0 ? 1 : 0;
+    }
+    if (d.threads != kThreads)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: %d)", d.threads, kThreads);
+    if (d.chunk_edges < 256 || d.chunk_edges > dev::kChunkMax || (d.chunk_edges & 31))
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.chunk_edges must be a multiple of 32 in [256, %d]",
+                          dev::kChunkMax);
+    if (d.warp_gather_threshold < 32)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.warp_gather_threshold must be >= 32");
+    if (d.cta_gather_threshold < dev::kChunkMax / dev::kMaxCtaRuns || d.cta_gather_threshold < d.warp_gather_threshold)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.cta_gather_threshold must be >= %d and >= the warp threshold",
+                          dev::kChunkMax / dev::kMaxCtaRuns);
+    if (d.saturation_quit < 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.saturation_quit must be >= 1");
+    if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
+    *out = d;
+    return B40C_SUCCESS;
+}
+
+// Reads the device state into the pinned mirror (synchronous).
+int read_state(b40c_bfs_problem *p)
+{
+    CUDA_TRY(cudaMemcpyAsync(p->h_st, p->st, sizeof(SearchState), cudaMemcpyDeviceToHost, p->stream), "state read");
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "stream synchronize");
+    return B40C_SUCCESS;
+}
+
+int check_state_errors(b40c_bfs_problem *p)
+{
+    const unsigned e = p->h_st->error;
+    if (e & dev::kErrOverflow)
+        return b40c::fail(B40C_ERROR_INVALID_CONFIGURATION,
+                          "Frontier queue overflow.  Please increase queue-sizing factor.");
+    if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk | dev::kErrInjected))
+        return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a bounded device-side wait expired (error bits 0x%x)", e);
+    return B40C_SUCCESS;
+}
+
+}  // namespace
+
+namespace b40c {
+// Shared helpers for bfs_strategies.cuh users.
+int runtime_persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_policy &pol, int max_grid,
+                            size_t smem, int *grid)
+{
+    int per_sm = 0;
+    CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem), "smem attribute");
+    CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, pol.threads, smem), "occupancy query");
+    if (per_sm < 1) return b40c::fail(B40C_ERROR_INVALID_CONFIGURATION, "kernel cannot be resident");
+    if (pol.ctas_per_sm > 0) per_sm = std::min(per_sm, pol.ctas_per_sm);
+    int g = per_sm * p->sms;
+    if (max_grid > 0) g = std::min(g, max_grid);
+    *grid = std::max(g, 1);
+    return B40C_SUCCESS;
+}
+}  // namespace b40c
+
+namespace {
+
+// ---- enactors -----------------------------------------------------------------------
+
+int finish_timing(b40c_bfs_problem *p)
+{
+    CUDA_TRY(cudaEventRecord(p->ring_b[p->ring_pos], p->stream), "event record");
+    CUDA_TRY(cudaEventRecord(p->ev1, p->stream), "event record");
+    p->ring_pos = (p->ring_pos + 1) % b40c_bfs_problem::kRing;
+    p->ring_count = std::min(p->ring_count + 1, b40c_bfs_problem::kRing);
+    p->timed = true;
+    return B40C_SUCCESS;
+}
+
+template <bool PRED>
+int launch_init(b40c_bfs_problem *p, const BfsParams &k, bool vertex_frontier, bool full)
+{
+    const int grid = full ? std::max(1, std::min<int>(p->sms * 8, (int)((p->nodes + kThreads - 1) / kThreads))) : 1;
+    if (vertex_frontier) {
+        if (full) dev::init_kernel<PRED, true, true><<<grid, kThreads, 0, p->stream>>>(k);
+        else dev::init_kernel<PRED, true, false><<<grid, kThreads, 0, p->stream>>>(k);
+    } else {
+        if (full) dev::init_kernel<PRED, false, true><<<grid, kThreads, 0, p->stream>>>(k);
+        else dev::init_kernel<PRED, false, false><<<grid, kThreads, 0, p->stream>>>(k);
+    }
+    CUDA_TRY(cudaGetLastError(), "init kernel launch");
+    return B40C_SUCCESS;
+}
+
+template <bool PRED>
+int enact_ec(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol, int32_t depth_limit)
+{
+    int rc;
+    if ((rc = ensure_vf(p, 0, cap_of(p->queue_sizing, p->nodes)))) return rc;
+    if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
+    if ((rc = ensure_slots(p))) return rc;
+    BfsParams k = make_params(p, pol);
+    const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
+    const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
+    int grid = 0;
+    if ((rc = runtime_persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
+    p->h_st->src = src;
+    p->h_st->depth_limit = depth_limit;
+    CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
+    CUDA_TRY(cudaMemcpyAsync(&p->st->src, &p->h_st->src, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
+             "source upload");
+    if ((rc = launch_init<PRED>(p, k, true, p->needs_init))) return rc;
+    CUDA_TRY(cudaEventRecord(p->ring_a[p->ring_pos], p->stream), "event record");
+    if (mode == B40C_ENACT_FUSED) {
+        k.persistent = 1;
+        k.max_levels = INT32_MAX;
+        const char *inj = getenv("B40C_TEST_SKIP_ARRIVAL_CTA");
+        if (inj) k.skip_arrival_cta = atoi(inj);
+        void *args[] = {&k};
+        CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream),
+                 "cooperative launch of the expand-contract kernel");
+    } else if (mode == B40C_ENACT_ITERATIVE) {
+        // one launch per level; the host reads the next frontier's size
+        k.persistent = 0;
+        k.max_levels = 1;
+        for (int level = 0;; level++) {
+            if ((rc = read_state(p))) return rc;
+            if (p->h_st->error || p->h_st->done) break;
+            const int q = p->h_st->q_len[level & 1], E = p->h_st->e_len[level & 1];
+            if (q == 0) break;
+            if (depth_limit >= 0 && level >= depth_limit) break;
+            const int g = std::max(1, std::min(grid, (E + 255) / 256));
+            dev::ec_kernel<kThreads, PRED><<<g, kThreads, smem, p->stream>>>(k);
+            CUDA_TRY(cudaGetLastError(), "expand-contract level launch");
+        }
+    } else {
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown enact mode %d", mode);
+    }
+    return finish_timing(p);
+}
+
+}  // namespace
+
+// ---- C ABI -----------------------------------------------------------------------------
+
+extern "C" {
+
+const char *b40c_last_error_string(void) { return b40c::error_buffer(); }
+
+const char *b40c_version(void) { return B40C_VERSION_STRING; }
+
+int b40c_device_count(int *count)
+{
+    b40c::clear_error();
+    if (!count) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null count");
+    int c = 0;
+    cudaError_t e = cudaGetDeviceCount(&c);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        c = 0;
+    }
+    *count = c;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_default_policy(int strategy, b40c_bfs_policy *policy)
+{
+    b40c::clear_error();
+    if (!policy) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null policy");
+    if (strategy < B40C_EXPAND_CONTRACT || strategy > B40C_HYBRID)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown strategy %d", strategy);
+    *policy = default_policy(strategy);
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t nodes, int64_t edges, int mark_pred,
+                            int stream_from_host, int device, b40c_bfs_problem **out)
+{
+    b40c::clear_error();
+    if (!out) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null output handle");
+    *out = nullptr;
+    if (!h_ro || (!h_ci && edges > 0) || nodes <= 0 || edges < 0 || nodes >= (int64_t)1 << 30 ||
+        edges >= (int64_t)INT32_MAX)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE,
+                          "invalid CSR (nodes %lld, edges %lld; need 0 < nodes < 2^30, edges < 2^31)", (long long)nodes,
+                          (long long)edges);
+    if (h_ro[0] != 0 || h_ro[nodes] != edges)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "row_offsets must start at 0 and end at edges");
+    // the kernels index labels and the mask by column value: reject malformed CSR up front
+    for (int64_t v = 0; v < nodes; v++)
+        if (h_ro[v + 1] < h_ro[v])
+            return b40c::fail(B40C_ERROR_INVALID_VALUE, "row_offsets decrease at vertex %lld", (long long)v);
+    for (int64_t e = 0; e < edges; e++)
+        if ((uint32_t)h_ci[e] >= (uint32_t)nodes)
+            return b40c::fail(B40C_ERROR_INVALID_VALUE, "column index %d at edge %lld out of range", h_ci[e],
+                              (long long)e);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return b40c::fail(B40C_ERROR_INVALID_VALUE, "invalid device %d", device);
+    DeviceGuard guard(device);
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return b40c::fail(B40C_ERROR_INVALID_DEVICE_FUNCTION, "kernels are built for sm_100a; device is sm_%d%d",
+                          prop.major, prop.minor);
+    auto *p = new b40c_bfs_problem();
+    p->device = device;
+    p->nodes = nodes;
+    p->edges = edges;
+    p->mark_pred = mark_pred ? 1 : 0;
+    p->stream_from_host = stream_from_host ? 1 : 0;
+    p->sms = prop.multiProcessorCount;
+    int rc = B40C_SUCCESS;
+    auto bail = [&](int code) {
+        b40c_bfs_problem_destroy(p);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "stream creation failed"));
+    }
+    p->stream = p->own_stream;
+    if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
+    }
+    for (int i = 0; i < b40c_bfs_problem::kRing; i++)
+        if (cudaEventCreate(&p->ring_a[i]) != cudaSuccess || cudaEventCreate(&p->ring_b[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
+        }
+    if (p->stream_from_host) {
+        // zero-copy: the kernels read the caller's host arrays over the bus
+        // (csr_problem.cuh:351-363); pin them in place when they are not pinned yet
+        const void *arrs[2] = {h_ro, h_ci};
+        const size_t bytes[2] = {sizeof(int32_t) * (size_t)(nodes + 1), sizeof(int32_t) * (size_t)std::max<int64_t>(edges, 1)};
+        int32_t **dst[2] = {&p->d_ro, &p->d_ci};
+        for (int i = 0; i < 2; i++) {
+            cudaPointerAttributes attr;
+            cudaError_t e = cudaPointerGetAttributes(&attr, arrs[i]);
+            if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+                cudaGetLastError();
+                e = cudaHostRegister((void *)arrs[i], bytes[i], cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+                if (e != cudaSuccess) {
+                    cudaGetLastError();
+                    return bail(b40c::fail((int)e, "cudaHostRegister for stream-from-host failed: %s", cudaGetErrorString(e)));
+                }
+                (i == 0 ? p->reg_ro : p->reg_ci) = arrs[i];
+            }
+            e = cudaHostGetDevicePointer((void **)dst[i], (void *)arrs[i], 0);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return bail(b40c::fail((int)e, "cudaHostGetDevicePointer failed: %s", cudaGetErrorString(e)));
+            }
+        }
+        p->own_csr = false;
+    } else {
+        if ((rc = alloc_dev((void **)&p->d_ro, sizeof(int32_t) * (nodes + 1), "row offsets"))) return bail(rc);
+        if ((rc = alloc_dev((void **)&p->d_ci, sizeof(int32_t) * std::max<int64_t>(edges, 1), "column indices")))
+            return bail(rc);
+        if (cudaMemcpyAsync(p->d_ro, h_ro, sizeof(int32_t) * (nodes + 1), cudaMemcpyHostToDevice, p->stream) != cudaSuccess ||
+            (edges > 0 && cudaMemcpyAsync(p->d_ci, h_ci, sizeof(int32_t) * edges, cudaMemcpyHostToDevice, p->stream) != cudaSuccess)) {
+            cudaGetLastError();
+            return bail(b40c::fail(B40C_ERROR_INVALID_VALUE, "CSR upload failed"));
+        }
+    }
+    p->mask_words = (int32_t)((nodes + 31) / 32);
+    if ((rc = alloc_dev((void **)&p->d_labels, sizeof(int32_t) * nodes, "labels"))) return bail(rc);
+    if ((rc = alloc_dev((void **)&p->d_mask, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "visited mask")))
+        return bail(rc);
+    if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
+    if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
+        cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "state allocation failed"));
+    }
+    memset(p->h_st, 0, sizeof(SearchState));
+    if ((rc = ensure_slots(p))) return bail(rc);
+    if (cudaStreamSynchronize(p->stream) != cudaSuccess) {
+        cudaError_t e = cudaGetLastError();
+        return bail(b40c::fail((int)e, "problem setup failed: %s", cudaGetErrorString(e)));
+    }
+    *out = p;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
+{
+    b40c::clear_error();
+    if (!p) return B40C_SUCCESS;
+    DeviceGuard guard(p->device);
+    if (p->stream) cudaStreamSynchronize(p->stream);
+    if (p->own_csr) {
+        if (p->d_ro) cudaFree(p->d_ro);
+        if (p->d_ci) cudaFree(p->d_ci);
+    }
+    if (p->reg_ro) cudaHostUnregister((void *)p->reg_ro);
+    if (p->reg_ci) cudaHostUnregister((void *)p->reg_ci);
+    if (p->d_labels) cudaFree(p->d_labels);
+    if (p->d_mask) cudaFree(p->d_mask);
+    for (int i = 0; i < 2; i++) {
+        free_vf(p->vf[i]);
+        free_ef(p->ef[i]);
+    }
+    if (p->slots) cudaFree(p->slots);
+    if (p->st) cudaFree(p->st);
+    if (p->h_st) cudaFreeHost(p->h_st);
+    if (p->ev0) cudaEventDestroy(p->ev0);
+    if (p->ev1) cudaEventDestroy(p->ev1);
+    for (int i = 0; i < b40c_bfs_problem::kRing; i++) {
+        if (p->ring_a[i]) cudaEventDestroy(p->ring_a[i]);
+        if (p->ring_b[i]) cudaEventDestroy(p->ring_b[i]);
+    }
+    if (p->own_stream) cudaStreamDestroy(p->own_stream);
+    cudaGetLastError();
+    delete p;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_set_stream(b40c_bfs_problem *p, void *stream)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    p->stream = stream ? (cudaStream_t)stream : p->own_stream;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_problem_reset(b40c_bfs_problem *p, int frontier_type, double queue_sizing)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    if (frontier_type < B40C_VERTEX_FRONTIERS || frontier_type > B40C_MULTI_GPU_FRONTIERS)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown frontier type %d", frontier_type);
+    if (!(queue_sizing > 0.0)) queue_sizing = 1.3;  // "0.0 is unspecified" (csr_problem.cuh:549)
+    DeviceGuard guard(p->device);
+    p->queue_sizing = queue_sizing;
+    int rc;
+    const int64_t vc = cap_of(queue_sizing, p->nodes), ec = cap_of(queue_sizing, p->edges);
+    switch (frontier_type) {
+    case B40C_VERTEX_FRONTIERS:
+        if ((rc = ensure_vf(p, 0, vc)) || (rc = ensure_vf(p, 1, vc))) return rc;
+        break;
+    case B40C_EDGE_FRONTIERS:
+        if ((rc = ensure_ef(p, 0, ec)) || (rc = ensure_ef(p, 1, ec))) return rc;
+        break;
+    default:  // MIXED (and MULTI_GPU, single GPU here)
+        if ((rc = ensure_vf(p, 0, vc)) || (rc = ensure_ef(p, 0, ec))) return rc;
+        break;
+    }
+    // labels <- -1, visited mask <- 0 (csr_problem.cuh:723-745)
+    CUDA_TRY(cudaMemsetAsync(p->d_labels, 0xff, sizeof(int32_t) * p->nodes, p->stream), "label reset");
+    CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, sizeof(uint32_t) * p->mask_words, p->stream), "mask reset");
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "reset synchronize");
+    p->needs_init = false;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_enact_limited(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int32_t depth_limit,
+                           int max_grid_size, const b40c_bfs_policy *policy)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    if (src < 0 || src >= p->nodes) return b40c::fail(B40C_ERROR_INVALID_VALUE, "source %d out of range", src);
+    if (max_grid_size < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "negative max_grid_size");
+    b40c_bfs_policy pol;
+    int rc = resolve_policy(strategy, policy, &pol);
+    if (rc) return rc;
+    DeviceGuard guard(p->device);
+    p->stats_valid = false;
+    p->timed = false;
+    p->last_strategy = strategy;
+    switch (strategy) {
+    case B40C_EXPAND_CONTRACT:
+        rc = p->mark_pred ? enact_ec<true>(p, mode, src, max_grid_size, pol, depth_limit)
+                          : enact_ec<false>(p, mode, src, max_grid_size, pol, depth_limit);
+        break;
+    case B40C_CONTRACT_EXPAND:
+    case B40C_TWO_PHASE:
+    case B40C_HYBRID:
+        rc = b40c::enact_edge_strategy(p, strategy, mode, src, max_grid_size, pol, depth_limit);
+        break;
+    default:
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown strategy %d", strategy);
+    }
+    p->needs_init = true;
+    return rc;
+}
+
+int b40c_bfs_enact(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid_size,
+                   const b40c_bfs_policy *policy)
+{
+    return b40c_bfs_enact_limited(p, strategy, mode, src, -1, max_grid_size, policy);
+}
+
+int b40c_bfs_stats(b40c_bfs_problem *p, int64_t *total_queued, int32_t *search_depth, double *avg_duty)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    DeviceGuard guard(p->device);
+    int rc = read_state(p);
+    if (rc) return rc;
+    if ((rc = check_state_errors(p))) return rc;
+    if (total_queued) *total_queued = (int64_t)p->h_st->total_queued;
+    if (search_depth) *search_depth = p->h_st->max_level + 1;
+    if (avg_duty) *avg_duty = 0.0;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_last_elapsed_ms(b40c_bfs_problem *p, float *ms)
+{
+    b40c::clear_error();
+    if (!p || !ms) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    if (!p->timed) return b40c::fail(B40C_ERROR_NOT_READY, "no timed search");
+    DeviceGuard guard(p->device);
+    CUDA_TRY(cudaEventSynchronize(p->ev1), "event synchronize");
+    CUDA_TRY(cudaEventElapsedTime(ms, p->ev0, p->ev1), "event elapsed");
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_recent_search_ms(b40c_bfs_problem *p, int count, float *out)
+{
+    b40c::clear_error();
+    if (!p || !out || count < 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    if (count > p->ring_count)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "only %d timed searches recorded (ring of %d)", p->ring_count,
+                          b40c_bfs_problem::kRing);
+    DeviceGuard guard(p->device);
+    const int R = b40c_bfs_problem::kRing;
+    const int newest = (p->ring_pos + R - 1) % R;
+    CUDA_TRY(cudaEventSynchronize(p->ring_b[newest]), "event synchronize");
+    for (int i = 0; i < count; i++) {
+        const int slot = (p->ring_pos + R - count + i) % R;
+        CUDA_TRY(cudaEventElapsedTime(&out[i], p->ring_a[slot], p->ring_b[slot]), "event elapsed");
+    }
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_extract(b40c_bfs_problem *p, int32_t *h_labels)
+{
+    b40c::clear_error();
+    if (!p || !h_labels) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    DeviceGuard guard(p->device);
+    int rc = read_state(p);
+    if (rc) return rc;
+    if ((rc = check_state_errors(p))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int32_t) * p->nodes, cudaMemcpyDeviceToHost, p->stream),
+             "label copy");
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "label copy synchronize");
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_device_view_get(b40c_bfs_problem *p, b40c_bfs_device_view *v)
+{
+    b40c::clear_error();
+    if (!p || !v) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    v->d_row_offsets = p->d_ro;
+    v->d_column_indices = p->d_ci;
+    v->d_labels = p->d_labels;
+    v->d_visited_mask = p->d_mask;
+    v->visited_mask_bytes = (p->nodes + 7) / 8;
+    v->nodes = p->nodes;
+    v->edges = p->edges;
+    v->device = p->device;
+    v->mark_predecessors = p->mark_pred;
+    return B40C_SUCCESS;
+}
+
+}  // extern "C"

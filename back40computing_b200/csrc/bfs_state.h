@@ -1,0 +1,80 @@
+// Device-resident search state and the kernel parameter block shared by the
+// host runtime (bfs_runtime.cu) and the kernels (bfs_kernels.cuh).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b40c {
+
+namespace dev {
+struct LookbackSlot;
+}
+
+// One vertex frontier: for entry i, `v[i]` is the vertex, `col[i]` the start of
+// its adjacency list and `P[i]` the exclusive prefix of the degrees of
+// entries 0..i-1 (so entry i owns edges [P[i], P[i+1]) of the level's
+// flattened edge space).  P has capacity + 1 slots.  Only vertices with at
+// least one edge are enqueued.
+struct VertexFrontier {
+    int32_t *v;
+    int32_t *col;
+    int32_t *P;
+};
+
+// One edge frontier: neighbour ids (and their predecessors when marking
+// predecessors), duplicates allowed.
+struct EdgeFrontier {
+    int32_t *v;
+    int32_t *pred;
+};
+
+// Rotating/ping-pong counters written by the kernels (the role of the
+// reference's CtaWorkProgress, util/cta_work_progress.cuh:69-223).
+struct alignas(128) SearchState {
+    int32_t q_len[2];          // frontier lengths, indexed by level parity
+    int32_t e_len[2];          // edge totals of vertex frontiers, by level parity
+    uint32_t chunk_ctr[3];     // dynamic chunk counters, by level % 3
+    int32_t cur_level;         // next level to process
+    unsigned long long epoch;  // look-back epoch base for this search
+    unsigned long long barrier;  // grid-barrier arrivals of the current persistent launch
+    uint32_t error;            // dev::kErr* bits
+    int32_t max_level;         // deepest level at which a vertex was labelled
+    int32_t done;              // 1 once the frontier emptied (or the depth limit was hit)
+    int32_t saturated;         // 1 when a hybrid fused launch handed off
+    unsigned long long total_queued;  // sum of processed frontier lengths
+    uint32_t finished;         // CTAs that finished the current non-persistent launch
+    int32_t src;               // source vertex (read by the init kernel)
+    int32_t depth_limit;       // < 0: unlimited
+    int32_t pad[5];
+};
+
+// Kernel parameter block.
+struct BfsParams {
+    const int32_t *row_offsets;
+    const int32_t *column_indices;
+    int32_t *labels;
+    uint32_t *mask;
+    int32_t nodes;
+    int32_t edges;
+    int32_t mask_words;
+    int32_t vcap;  // vertex frontier capacity (entries)
+    int32_t ecap;  // edge frontier capacity (entries)
+    int32_t max_chunks;
+    VertexFrontier vf[2];
+    EdgeFrontier ef[2];
+    dev::LookbackSlot *slots;
+    SearchState *st;
+    int32_t max_levels;       // levels this launch may process (1 = one level per launch)
+    int32_t chunk_edges;      // C_max for this launch (<= kChunkMax)
+    int32_t warp_thresh;
+    int32_t cta_thresh;
+    int32_t warp_cull;
+    int32_t precheck;
+    int32_t saturation;       // hybrid: leave the fused kernel when items > gridDim * saturation
+    int32_t persistent;       // 1: loop over levels with the grid barrier
+    int32_t skip_arrival_cta; // test-only fault injection: this CTA never arrives (-1 = off)
+    int32_t pad0;
+    unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
+};
+
+}  // namespace b40c

@@ -1,0 +1,245 @@
+// Device-side building blocks for the BFS kernels (sm_100a):
+// cache-qualified loads, the bounded software grid barrier, bulk-copy
+// (cp.async.bulk) staging with an mbarrier, and the decoupled look-back used
+// to allocate frontier-queue slots.
+//
+// Every spin in this file is bounded: after kSpinLimit polls the waiter sets
+// an error bit in the search state and gives up, so a missing arrival can
+// never hang the GPU (the reference's GlobalBarrier::Sync spins forever,
+// util/global_barrier.cuh:99-121).
+#pragma once
+#include <cstdint>
+
+namespace b40c {
+namespace dev {
+
+constexpr unsigned kErrOverflow = 1u;       // a frontier queue would overflow
+constexpr unsigned kErrBarrier = 2u;        // grid barrier wait expired
+constexpr unsigned kErrLookback = 4u;       // look-back wait expired
+constexpr unsigned kErrBulk = 8u;           // bulk-copy wait expired
+constexpr unsigned kErrInjected = 16u;      // test-only: a CTA skipped its barrier arrival
+constexpr unsigned kSpinLimit = 1u << 22;   // polls before a wait gives up (~1-2 s with backoff)
+
+// ---- loads / stores ----------------------------------------------------------
+__device__ __forceinline__ int ld_cg(const int *p)
+{
+    int v;
+    asm volatile("ld.global.cg.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned ld_cg(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.global.cg.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+// streaming read-only load (column indices: read once per search)
+__device__ __forceinline__ int ld_stream(const int *p)
+{
+    int v;
+    asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ int4 ld_stream4(const int4 *p)
+{
+    int4 v;
+    asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p));
+    return v;
+}
+// read-only load through L1 (row offsets)
+__device__ __forceinline__ int ld_ro(const int *p) { return __ldg(p); }
+// visited-word pre-check: weak load that may hit a stale L1 line; a stale
+// line can only show fewer bits set (bits only ever go 0 -> 1), so it never
+// drops an undiscovered vertex -- the atomic test-and-set decides.
+__device__ __forceinline__ unsigned ld_mask(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.global.ca.u32 %0, [%1];" : "=r"(v) : "l"(p));
+    return v;
+}
+__device__ __forceinline__ unsigned long long ld_acquire(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long *p, unsigned long long v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed(const unsigned long long *p)
+{
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ---- bounded grid barrier ------------------------------------------------------
+// Monotone arrival counter: the g-th barrier of a launch completes when the
+// counter reaches g * gridDim.x.  The counter is zeroed before each
+// persistent launch.  Requires every CTA to be resident (cooperative launch).
+// Returns false when the wait expired or another CTA reported an error.
+__device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned &generation,
+                                             unsigned *error_word, int *s_flag)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        generation++;
+        const unsigned long long target = (unsigned long long)generation * gridDim.x;
+        __threadfence();
+        atomicAdd(counter, 1ull);
+        unsigned spins = 0;
+        int ok = 1;
+        while (ld_acquire(counter) < target) {
+            if (++spins > kSpinLimit) {
+                atomicOr(error_word, kErrBarrier);
+                ok = 0;
+                break;
+            }
+            if ((spins & 7) == 0 && ld_cg(error_word) != 0) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(spins < 64 ? 32 : 256);
+        }
+        __threadfence();
+        if (ok && ld_cg(error_word) != 0) ok = 0;
+        *s_flag = ok;
+    }
+    __syncthreads();
+    return *s_flag != 0;
+}
+
+// ---- mbarrier + bulk copy (cp.async.bulk, global -> this CTA's shared) ----------
+__device__ __forceinline__ unsigned smem_addr(const void *p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.release.cta.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+// Copies `bytes` (multiple of 16; both addresses 16-byte aligned) into shared memory.
+__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, unsigned bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cta.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(smem_dst)),
+        "l"(gmem_src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// ---- decoupled look-back ---------------------------------------------------------
+// One slot per work chunk of a level.  `status` = epoch << 2 | flag, where flag
+// 1 = aggregate published, 2 = inclusive prefix published; the epoch is
+// unique per (search, level), so slots never need clearing between levels.
+// Values are (count << 32 | degree_sum) pairs that add component-wise.
+struct alignas(32) LookbackSlot {
+    unsigned long long status;
+    unsigned long long aggregate;
+    unsigned long long inclusive;
+    unsigned long long pad;
+};
+constexpr unsigned long long kFlagAggregate = 1ull;
+constexpr unsigned long long kFlagInclusive = 2ull;
+
+__device__ __forceinline__ void lookback_publish(LookbackSlot *slot, unsigned long long epoch,
+                                                 unsigned long long flag, unsigned long long value)
+{
+    if (flag == kFlagAggregate)
+        st_relaxed(&slot->aggregate, value);
+    else
+        st_relaxed(&slot->inclusive, value);
+    st_release(&slot->status, (epoch << 2) | flag);
+}
+
+// Called by one full warp.  Returns the exclusive prefix of chunk `chunk`
+// (sum of the values of chunks 0..chunk-1); chunk 0 must not call it.  On
+// a wait that expires it sets kErrLookback and returns ~0ull.
+__device__ __forceinline__ unsigned long long lookback_exclusive(LookbackSlot *slots, unsigned chunk,
+                                                                 unsigned long long epoch, unsigned *error_word)
+{
+    const unsigned lane = threadIdx.x & 31;
+    unsigned long long prefix = 0;
+    long long window_end = (long long)chunk - 1;  // nearest predecessor
+    unsigned spins = 0;
+    while (true) {
+        long long j = window_end - lane;
+        unsigned long long flag = kFlagInclusive, value = 0;
+        if (j >= 0) {
+            // wait until this lane's slot carries a flag of the current epoch
+            while (true) {
+                unsigned long long st = ld_acquire(&slots[j].status);
+                if ((st >> 2) == epoch && (st & 3ull) != 0) {
+                    flag = st & 3ull;
+                    value = (flag == kFlagInclusive) ? ld_relaxed(&slots[j].inclusive)
+                                                     : ld_relaxed(&slots[j].aggregate);
+                    break;
+                }
+                if (++spins > kSpinLimit) {
+                    atomicOr(error_word, kErrLookback);
+                    flag = kFlagInclusive;
+                    value = ~0ull;
+                    break;
+                }
+                __nanosleep(spins < 32 ? 20 : 200);
+            }
+        }
+        unsigned incl = __ballot_sync(0xffffffffu, flag == kFlagInclusive);
+        unsigned bad = __ballot_sync(0xffffffffu, value == ~0ull);
+        if (bad) return ~0ull;
+        // only lanes up to (and including) the nearest inclusive slot count
+        int stop = incl ? (__ffs(incl) - 1) : 31;
+        unsigned long long contrib = ((int)lane <= stop) ? value : 0ull;
+        for (int off = 16; off > 0; off >>= 1) contrib += __shfl_down_sync(0xffffffffu, contrib, off);
+        contrib = __shfl_sync(0xffffffffu, contrib, 0);
+        prefix += contrib;
+        if (incl) return prefix;
+        window_end -= 32;
+    }
+}
+
+}  // namespace dev
+}  // namespace b40c

@@ -1,0 +1,371 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 BFS path (one JSON line on stdout, rank 0).
+
+Workload (default): plain single-source BFS on an R-MAT graph, scale 22
+(4,194,304 vertices), edge factor 16 (67,108,864 undirected edges stored as
+134,217,728 directed CSR edges), a/b/c/d = .57/.19/.19/.05, self-loops and
+duplicates kept, vertex ids permuted by a seeded permutation; 64 sources
+drawn with seed 0 among vertices of nonzero degree, each searched
+separately.  One step = the 64 searches.  Inputs (the CSR, 554 MB) are
+resident in HBM and larger than L2.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Metric: GTEPS = sum over searches of E_c / device time, E_c = sum of the CSR
+degrees of the reached vertices (test/bfs/test_bfs.cu:359-367).  Under
+torchrun each rank runs the same workload on its own GPU (replicas: the
+search does not shard), value = all ranks' edges / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from concurrent.futures import ThreadPoolExecutor
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BFS GTEPS on 1 B200 (plain vs 64-source batched); served p50/p99 latency"
+
+CONFIGS = {
+    "rmat22": dict(kind="rmat", scale=22, ef=16,
+                   workload="plain single-source BFS, R-MAT scale 22 edge factor 16 (a=.57 b=.19 c=.19 d=.05), "
+                            "ids permuted, 64 seeded sources searched separately"),
+    "grid2d1000": dict(kind="grid2d", width=1000,
+                       workload="plain single-source BFS, 2D 5-point lattice 1000x1000, source 0"),
+    "grid3d256": dict(kind="grid3d", width=256,
+                      workload="high-diameter BFS, 3D 7-point lattice 256^3, source = centre"),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat22")
+    ap.add_argument("--strategy", type=int, default=0, help="0 EC, 1 CE, 2 two-phase, 3 hybrid")
+    ap.add_argument("--mode", type=int, default=0, help="0 fused (persistent), 1 per-level launches, 2 CUDA graph")
+    ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound on the CPU-baseline sample")
+    return ap.parse_args()
+
+
+def build_graph(cfg_name):
+    from back40computing_b200 import CsrGraph, BuildRmatGraph, BuildGrid2dGraph, BuildGrid3dGraph, sample_sources
+    cfg = CONFIGS[cfg_name]
+    g = CsrGraph()
+    if cfg["kind"] == "rmat":
+        n = 1 << cfg["scale"]
+        BuildRmatGraph(n, cfg["ef"] * n, g, True, 0.57, 0.19, 0.19, seed=0, permute=True)
+        return g, None
+    if cfg["kind"] == "grid2d":
+        BuildGrid2dGraph(cfg["width"], g)
+        return g, np.array([0], np.int32)
+    w = cfg["width"]
+    BuildGrid3dGraph(w, g)
+    c = w // 2
+    return g, np.array([c * w * w + c * w + c], np.int32)
+
+
+def sources_for(g, fixed, count):
+    from back40computing_b200 import sample_sources
+    if fixed is not None:
+        return fixed
+    return sample_sources(g, count, seed=0)
+
+
+def visited(deg, labels):
+    reached = labels >= 0 if labels is not None else None
+    return int(reached.sum()), int(deg[reached].sum())
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for k, nm in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(cfg_name):
+    """DRAM bytes per search of the dominant kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{cfg_name}.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_search_fn():
+    """The CPU BFS to time: the reference's SimpleReferenceBfs when its harness
+    was built (kind "reference"), else the C restatement (kind "port")."""
+    import oracle
+    if oracle.have_ref():
+        def run(ro, ci, s):
+            return oracle.ref_bfs(ro, ci, int(s))[0]
+        return run, "reference"
+
+    def run(ro, ci, s):
+        return oracle.bfs(ro, ci, int(s))[0]
+    return run, "port"
+
+
+def cpu_baseline(g, srcs, deg, budget_s):
+    """Serial CPU BFS on a bounded sample of the sources (one core)."""
+    run, kind = cpu_search_fn()
+    edges, t, used = 0, 0.0, 0
+    for s in srcs:
+        t0 = time.perf_counter()
+        labels = run(g.row_offsets, g.column_indices, s)
+        t += time.perf_counter() - t0
+        edges += visited(deg, labels)[1]
+        used += 1
+        if t >= budget_s:
+            break
+    return {"value": edges / t / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+            "sample": f"{used} of {len(srcs)} sources, serial SimpleReferenceBfs, wall clock ({t:.1f} s)"}
+
+
+def run_reference(args, rank):
+    """--impl reference: the reference's CPU BFS on the host cores (independent
+    searches in parallel threads; ctypes releases the GIL during each call)."""
+    if rank != 0:
+        return
+    g, fixed = build_graph(args.config)
+    srcs = sources_for(g, fixed, args.sources)
+    deg = np.diff(g.row_offsets).astype(np.int64)
+    run, kind = cpu_search_fn()
+    threads = max(1, min(os.cpu_count() or 1, 64))
+    per_step = list(srcs[:max(1, min(len(srcs), threads))])
+    if len(per_step) < threads:
+        per_step = (per_step * threads)[:threads]
+    ec_cache = {}
+
+    def one(s):
+        labels = run(g.row_offsets, g.column_indices, s)
+        if s not in ec_cache:
+            ec_cache[int(s)] = visited(deg, labels)[1]
+        return int(s)
+
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for _ in range(args.warmup):
+            list(ex.map(one, per_step))
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            list(ex.map(one, per_step))
+        dt = time.perf_counter() - t0
+    edges = sum(ec_cache[int(s)] for s in per_step) * args.steps
+    value = edges / dt / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "GTEPS", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
+        "data": "synthetic (seeded generator, no dataset)",
+        "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
+                   "sample_per_step": f"{len(per_step)} searches in parallel threads"},
+        "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": kind,
+                         "sample": f"{len(per_step)} independent searches per step on {threads} threads"},
+        "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    from back40computing_b200 import CsrProblem
+    from back40computing_b200 import _native as N
+    from back40computing_b200.bfs import ENACTORS
+
+    g, fixed = build_graph(args.config)
+    srcs = sources_for(g, fixed, args.sources)
+    deg = np.diff(g.row_offsets).astype(np.int64)
+    problem = CsrProblem.from_graph(g, device=local)
+    stream = torch.cuda.current_stream()
+    problem.set_stream(stream.cuda_stream)
+    enactor = ENACTORS[args.strategy]()
+    N.check(problem.Reset(enactor.GetFrontierType(), 1.3), "Reset")
+
+    def enact(s):
+        N.check(enactor._enact(problem, int(s), args.mode, 0), "enact")
+
+    # untimed pass: per-source reached vertices/edges, and parity with the oracle on one source
+    ec, vc = [], []
+    for i, s in enumerate(srcs):
+        enact(s)
+        labels = problem.labels()
+        v, e = visited(deg, labels)
+        vc.append(v)
+        ec.append(e)
+        if i == 0 and rank == 0:
+            import oracle
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            if oracle.compare_labels(labels, want) != -1:
+                raise SystemExit("parity failure against the oracle")
+    ec, vc = np.array(ec, np.int64), np.array(vc, np.int64)
+
+    def step():
+        for s in srcs:
+            enact(s)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    n_timed = min(len(srcs) * args.steps, 256)
+    kernel_ms = problem.recent_search_ms(n_timed)
+    order = [srcs[(len(srcs) * args.steps - n_timed + i) % len(srcs)] for i in range(n_timed)]
+    idx = {int(s): i for i, s in enumerate(srcs)}
+    balg = np.array([4 * ec[idx[int(s)]] + 8 * vc[idx[int(s)]] for s in order], np.float64)
+    peak, peak_kind = measured_peak()
+    achieved = balg.sum() / (kernel_ms.sum() * 1e-3) / 1e9
+    total_edges = float(ec.sum()) * args.steps * world
+    value = total_edges / (ms * 1e-3) / 1e9
+
+    # end to end through the public API: enact + labels read back into pinned host memory
+    host = torch.empty(g.nodes, dtype=torch.int32, pin_memory=True)
+    hview = host.numpy()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for s in srcs:
+            enact(s)
+            N.check(problem.ExtractResults(hview), "ExtractResults")
+    e2e_s = time.perf_counter() - t0
+    e2e = {"value": float(ec.sum()) * args.steps / e2e_s / 1e9, "unit": "GTEPS",
+           "h2d_bytes_per_step": 8 * len(srcs), "d2h_bytes_per_step": 4 * g.nodes * len(srcs)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(g, srcs, deg, args.cpu_seconds)
+    traffic = profiled_traffic(args.config)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
+            "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
+                       "vertices": g.nodes, "edges": g.edges, "searches_per_step": len(srcs),
+                       "strategy": ["expand-contract", "contract-expand", "two-phase", "hybrid"][args.strategy],
+                       "mode": ["fused persistent", "per-level launches", "cuda graph"][args.mode],
+                       "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6),
+                       "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": (traffic or {}).get("dram_bytes_per_search"),
+                         "bytes_per_search_alg": float(balg.mean()),
+                         "kernel_ms_per_search": float(kernel_ms.mean())},
+            "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": 2 * len(srcs) * args.steps,
+            "clocks": clk,
+            "edges_per_search": float(ec.mean()), "search_gteps_mean": float((ec / 1e9).mean()
+                                                                              / (kernel_ms.mean() * 1e-3)),
+        }
+        print(json.dumps(line), flush=True)
+    problem.Destroy()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,231 @@
+/*
+ * b40c_bfs.h — C-ABI boundary of the B200-native single-GPU BFS library
+ * (libb40c_bfs.so).  Plain pointers and sizes only; no CUDA or torch types.
+ *
+ * The reference (b40c, "Back40Computing" v1.0.1042) exposes this path as a
+ * header-only C++ template API; its C++ callers keep that API through the
+ * shims under include/b40c/, which forward to the entry points below.  Each
+ * entry point names the reference interface it replaces (file:line in the
+ * reference tree).
+ *
+ * Conventions
+ *  - Every function returns an int status whose values are the cudaError_t
+ *    values the reference returns for the same condition (0 = success).
+ *    b40c_last_error_string() describes the last failure of the calling
+ *    thread.
+ *  - The caller owns host buffers; a problem handle owns its device buffers.
+ *  - A handle is used by one host thread at a time; its work is ordered on
+ *    the handle's CUDA stream (b40c_bfs_set_stream), default: a stream the
+ *    handle creates.
+ *  - Vertex ids, row offsets and labels are int32 (the reference's
+ *    VertexId = SizeT = int for every graph type its driver builds).
+ */
+#ifndef B40C_BFS_H
+#define B40C_BFS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (numerically equal to cudaError_t) -------------------- */
+#define B40C_SUCCESS                        0
+#define B40C_ERROR_INVALID_VALUE            1    /* cudaErrorInvalidValue */
+#define B40C_ERROR_MEMORY_ALLOCATION        2    /* cudaErrorMemoryAllocation */
+#define B40C_ERROR_INVALID_CONFIGURATION    9    /* cudaErrorInvalidConfiguration: frontier queue overflow
+                                                    (enactor_contract_expand.cuh:319-324) */
+#define B40C_ERROR_INVALID_DEVICE_FUNCTION  98   /* cudaErrorInvalidDeviceFunction: no kernel for this device */
+#define B40C_ERROR_NO_DEVICE                100  /* cudaErrorNoDevice */
+#define B40C_ERROR_NOT_READY                600  /* cudaErrorNotReady */
+#define B40C_ERROR_LAUNCH_TIMEOUT           702  /* cudaErrorLaunchTimeout: a bounded device-side wait expired */
+#define B40C_ERROR_NOT_SUPPORTED            801  /* cudaErrorNotSupported */
+
+/* ---- enums ---------------------------------------------------------------- */
+
+/* bfs::FrontierType, csr_problem.cuh:54-61 */
+enum {
+    B40C_VERTEX_FRONTIERS = 0,   /* two O(n) vertex frontiers */
+    B40C_EDGE_FRONTIERS = 1,     /* two O(m) edge frontiers */
+    B40C_MIXED_FRONTIERS = 2,    /* one O(n) vertex frontier, one O(m) edge frontier */
+    B40C_MULTI_GPU_FRONTIERS = 3 /* accepted for API compatibility; treated as MIXED (single GPU only) */
+};
+
+/* Strategy, test/bfs/test_bfs.cu:72-79 (same numbering) */
+enum {
+    B40C_EXPAND_CONTRACT = 0, /* EnactorExpandContract   (enactor_expand_contract.cuh:59) */
+    B40C_CONTRACT_EXPAND = 1, /* EnactorContractExpand   (enactor_contract_expand.cuh:61) */
+    B40C_TWO_PHASE = 2,       /* EnactorTwoPhase         (enactor_two_phase.cuh:68) */
+    B40C_HYBRID = 3           /* EnactorHybrid           (enactor_hybrid.cuh:64) */
+};
+
+/* How the levels of one search are launched. */
+enum {
+    B40C_ENACT_FUSED = 0,     /* EnactFusedSearch: one persistent grid, bounded software barrier between levels */
+    B40C_ENACT_ITERATIVE = 1, /* EnactIterativeSearch: one launch per level, host reads the frontier size */
+    B40C_ENACT_GRAPH = 2      /* whole search replayed as one CUDA graph (conditional WHILE node over levels) */
+};
+
+/* Runtime kernel policy (replaces the reference's compile-time KernelPolicy
+ * template parameters, e.g. enactor_contract_expand.cuh:339-373).  A zero
+ * field means "use the tuned default". */
+typedef struct b40c_bfs_policy {
+    int32_t threads;               /* CTA size: 128, 256 or 512 */
+    int32_t ctas_per_sm;           /* resident CTAs per SM for persistent grids (0 = occupancy limit) */
+    int32_t chunk_edges;           /* edges per CTA work chunk in the edge-balanced expansion (<= 4096) */
+    int32_t warp_gather_threshold; /* run length at or above which a warp gathers cooperatively (>= 32) */
+    int32_t cta_gather_threshold;  /* run length at or above which the CTA gathers with bulk staging */
+    int32_t saturation_quit;       /* hybrid: queue items per CTA above which the search leaves the fused kernel */
+    int32_t warp_cull;             /* 1: drop duplicate neighbours within a warp before the bitmask test,
+                                      -1: do not (default) */
+    int32_t bitmask_precheck;      /* 1: read the visited word before the atomic test-and-set (default),
+                                      -1: go straight to the atomic */
+} b40c_bfs_policy;
+
+typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
+
+/* Device pointers of a problem (GraphSlice members, csr_problem.cuh:99-173). */
+typedef struct b40c_bfs_device_view {
+    void *d_row_offsets;    /* int32[nodes + 1] */
+    void *d_column_indices; /* int32[edges] */
+    void *d_labels;         /* int32[nodes] */
+    void *d_visited_mask;   /* bit v&7 of byte v>>3 (same layout as the reference's uchar mask) */
+    int64_t visited_mask_bytes;
+    int64_t nodes;
+    int64_t edges;
+    int32_t device;
+    int32_t mark_predecessors;
+} b40c_bfs_device_view;
+
+/* ---- library ---------------------------------------------------------------- */
+
+/* Text of the last error raised on the calling thread ("" if none). */
+const char *b40c_last_error_string(void);
+
+/* Library version string. */
+const char *b40c_version(void);
+
+/* Number of CUDA devices visible (0 on a machine without a GPU). */
+int b40c_device_count(int *count);
+
+/* Fills *policy with the tuned default for a strategy. */
+int b40c_bfs_default_policy(int strategy, b40c_bfs_policy *policy);
+
+/* ---- problem (bfs::CsrProblem, csr_problem.cuh:72-756) ---------------------- */
+
+/* CsrProblem::FromHostProblem (csr_problem.cuh:328-540): copies the CSR to the
+ * device (or, with stream_from_host, maps the caller's pinned host arrays
+ * zero-copy: they must stay valid until destroy).  num_gpus other than 1 is
+ * rejected (single-GPU library). */
+int b40c_bfs_problem_create(const int32_t *h_row_offsets, const int32_t *h_column_indices,
+                            int64_t nodes, int64_t edges, int mark_predecessors,
+                            int stream_from_host, int device, b40c_bfs_problem **out);
+
+/* CsrProblem::~CsrProblem (csr_problem.cuh:205-215). */
+int b40c_bfs_problem_destroy(b40c_bfs_problem *problem);
+
+/* Orders the handle's work on a caller stream (a cudaStream_t); NULL restores
+ * the handle's own stream. */
+int b40c_bfs_set_stream(b40c_bfs_problem *problem, void *cuda_stream);
+
+/* CsrProblem::Reset (csr_problem.cuh:547-750): (re)allocates the frontier
+ * queues for frontier_type at queue_sizing x n (vertex) or x m (edge)
+ * elements, and initialises labels to -1 and the visited mask to 0. */
+int b40c_bfs_problem_reset(b40c_bfs_problem *problem, int frontier_type, double queue_sizing);
+
+/* Enact{Fused,Iterative}Search / EnactSearch (enactor_contract_expand.cuh:262,419;
+ * enactor_expand_contract.cuh; enactor_two_phase.cuh:276,421;
+ * enactor_hybrid.cuh:279).  Searches from src; labels become source
+ * distances (src = 0), or predecessors (src = -2) when the problem marks
+ * predecessors; unreached vertices keep -1.  max_grid_size 0 = SMs x
+ * occupancy (EnactorBase::MaxGridSize, enactor_base.cuh:93).  policy NULL =
+ * tuned default.  Asynchronous apart from the iterative mode's per-level
+ * frontier reads; b40c_bfs_stats or b40c_bfs_extract synchronise. */
+int b40c_bfs_enact(b40c_bfs_problem *problem, int strategy, int mode, int32_t src,
+                   int max_grid_size, const b40c_bfs_policy *policy);
+
+/* Same as b40c_bfs_enact with a depth limit: vertices farther than
+ * depth_limit levels from src stay -1 (depth_limit < 0: unlimited). */
+int b40c_bfs_enact_limited(b40c_bfs_problem *problem, int strategy, int mode, int32_t src,
+                           int32_t depth_limit, int max_grid_size, const b40c_bfs_policy *policy);
+
+/* CsrProblem::ExtractResults (csr_problem.cuh:255-322): copies labels[n] to the host. */
+int b40c_bfs_extract(b40c_bfs_problem *problem, int32_t *h_labels);
+
+/* Enactor*::GetStatistics (enactor_contract_expand.cuh:237-250 and peers):
+ * total_queued = sum of the frontier-queue lengths the search processed,
+ * search_depth = number of BFS levels (max distance + 1), avg_duty = mean
+ * fraction of each CTA's lifetime spent on work (0 unless instrumented). */
+int b40c_bfs_stats(b40c_bfs_problem *problem, int64_t *total_queued, int32_t *search_depth,
+                   double *avg_duty);
+
+/* Device time of the last enact in milliseconds (CUDA events on the handle's stream). */
+int b40c_bfs_last_elapsed_ms(b40c_bfs_problem *problem, float *ms);
+
+/* Device times (ms) of the search kernels of the last `count` enacts (oldest
+ * first; at most 256 are kept): each spans from after the source set-up to
+ * the end of the last level, per launch mode.  Synchronises on the newest. */
+int b40c_bfs_recent_search_ms(b40c_bfs_problem *problem, int count, float *out);
+
+/* GraphSlice device pointers (csr_problem.cuh:99-173). */
+int b40c_bfs_device_view_get(b40c_bfs_problem *problem, b40c_bfs_device_view *view);
+
+/* ---- pinned host memory (CsrGraph(pinned), csr_graph.cuh:81-93) ------------ */
+int b40c_host_alloc(void **ptr, size_t bytes, int mapped);
+int b40c_host_free(void *ptr);
+
+/* ---- graph builders (b40c/graph/builder/*.cuh) -----------------------------
+ * Native, multi-threaded builders used by the benchmark and the Python layer.
+ * Arrays are allocated with malloc (or pinned when pinned != 0) and released
+ * with b40c_graph_free.  Results are deterministic for a seed, independent of
+ * the thread count. */
+typedef struct b40c_csr {
+    int64_t nodes;
+    int64_t edges;
+    int32_t *row_offsets;    /* [nodes + 1] */
+    int32_t *column_indices; /* [edges] */
+    int32_t pinned;
+} b40c_csr;
+
+/* BuildGrid2dGraph (grid2d.cuh:54-114): width^2 vertices, neighbour order
+ * -x,+x,-y,+y, then a self-loop. */
+int b40c_build_grid2d(int32_t width, int pinned, b40c_csr *out);
+
+/* BuildGrid3dGraph (grid3d.cuh:54-129): width^3 vertices, neighbour order
+ * -x,+x,-y,+y,-z,+z, then a self-loop. */
+int b40c_build_grid3d(int32_t width, int pinned, b40c_csr *out);
+
+/* BuildRmatGraph (rmat.cuh:128-206): `edges` R-MAT draws over `nodes` (a power
+ * of two) with per-level +-5% parameter noise (VaryParams, rmat.cuh:83-116),
+ * walk starting at u = v = 1 (rmat.cuh:167-169; the id `nodes` wraps to 0),
+ * back-edges when undirected, self-loops and duplicates kept, rows in
+ * generation order (FromCoo's stable sort, csr_graph.cuh:109-152).  With
+ * permute != 0 vertex ids are relabelled by a seeded random permutation. */
+int b40c_build_rmat(int64_t nodes, int64_t edges, int undirected, double a, double b, double c,
+                    uint64_t seed, int permute, int pinned, b40c_csr *out);
+
+/* BuildRandomGraph (random.cuh:54-98): `edges` uniform (u, v) pairs, back-edges when undirected. */
+int b40c_build_random(int64_t nodes, int64_t edges, int undirected, uint64_t seed, int pinned,
+                      b40c_csr *out);
+
+/* BuildRandomRegularishGraph (rr.cuh:53-91): `degree` uniform out-neighbours
+ * per vertex; with symmetrize != 0 every edge also gets its back-edge (the
+ * random.cuh:81-86 construction) and rows keep generation order. */
+int b40c_build_rr(int64_t nodes, int32_t degree, int symmetrize, uint64_t seed, int pinned,
+                  b40c_csr *out);
+
+/* CsrGraph::FromCoo (csr_graph.cuh:109-152): stable by-row CSR of a COO list. */
+int b40c_csr_from_coo(const int32_t *rows, const int32_t *cols, int64_t nodes, int64_t edges,
+                      int pinned, b40c_csr *out);
+
+/* Seeded sample of `count` distinct vertices with nonzero degree (sources). */
+int b40c_sample_sources(const b40c_csr *graph, int32_t count, uint64_t seed, int32_t *out);
+
+void b40c_graph_free(b40c_csr *graph);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* B40C_BFS_H */

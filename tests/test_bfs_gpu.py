@@ -1,0 +1,141 @@
+"""Parity of the CUDA BFS path (through the C ABI) with the CPU oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from back40computing_b200 import (CsrGraph, CsrProblem, BuildGrid2dGraph, BuildGrid3dGraph, BuildRmatGraph,
+                                  BuildRandomRegularishGraph, BuildRandomGraph, search, sample_sources, B40cError)
+from back40computing_b200 import _native as N
+from back40computing_b200.bfs import EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID, ENACTORS
+
+pytestmark = pytest.mark.gpu
+
+MODES = [N.ENACT_FUSED, N.ENACT_ITERATIVE]
+
+
+def _graph(kind, *args, **kw):
+    g = CsrGraph()
+    {"grid2d": BuildGrid2dGraph, "grid3d": BuildGrid3dGraph, "rmat": BuildRmatGraph,
+     "rr": BuildRandomRegularishGraph, "random": BuildRandomGraph}[kind](*args, g, **kw) if kind in (
+        "grid2d", "grid3d") else None
+    if kind == "rmat":
+        BuildRmatGraph(args[0], args[1], g, True, 0.57, 0.19, 0.19, seed=kw.get("seed", 0),
+                       permute=kw.get("permute", True))
+    elif kind == "rr":
+        BuildRandomRegularishGraph(args[0], args[1], g, seed=kw.get("seed", 0), symmetrize=kw.get("sym", True))
+    elif kind == "random":
+        BuildRandomGraph(args[0], args[1], g, kw.get("undirected", True), seed=kw.get("seed", 0))
+    return g
+
+
+def _check_dist(g, problem, src, strategy, mode, **kw):
+    got = search(problem, int(src), strategy=strategy, mode=mode, **kw)
+    want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(src), kw.get("depth_limit", -1))
+    bad = oracle.compare_labels(got, want)
+    assert bad == -1, f"label mismatch at {bad}: got {got[bad]} want {want[bad]}"
+    return depth
+
+
+STRATS = [EXPAND_CONTRACT]
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+@pytest.mark.parametrize("mode", MODES)
+def test_golden_fixtures(golden, strategy, mode):
+    for name, c in golden.items():
+        g = CsrGraph.from_arrays(c["row_offsets"], c["column_indices"])
+        p = CsrProblem.from_graph(g)
+        for k, s in enumerate(c["sources"]):
+            got = search(p, int(s), strategy=strategy, mode=mode)
+            assert oracle.compare_labels(got, c[f"labels{k}"]) == -1, name
+            enactor = ENACTORS[strategy]()
+            enactor._problem = p
+            _, depth, _ = enactor.GetStatistics()
+            assert depth == int(c[f"depth{k}"]), name
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("kind,args", [
+    ("grid2d", (100,)), ("grid3d", (20,)), ("rmat", (1 << 14, 1 << 18)), ("rr", (1 << 14, 8)),
+    ("random", (20000, 60000)),
+])
+def test_distance_parity(kind, args, strategy, mode):
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g)
+    srcs = sample_sources(g, 3, seed=7)
+    for s in srcs:
+        _check_dist(g, p, s, strategy, mode)
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+def test_predecessors_valid(strategy):
+    g = _graph("rmat", 1 << 14, 1 << 18)
+    p = CsrProblem.from_graph(g, mark_predecessors=True)
+    for s in sample_sources(g, 3, seed=1):
+        preds = search(p, int(s), strategy=strategy)
+        dist, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        assert preds[s] == -2
+        assert oracle.check_predecessors(g.row_offsets, g.column_indices, dist, preds) == (-1, 0)
+        assert np.array_equal(preds >= 0, dist > 0)
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+def test_grid2d_1000_corner_full_size(strategy):
+    g = _graph("grid2d", 1000)
+    p = CsrProblem.from_graph(g)
+    got = search(p, 0, strategy=strategy)
+    y, x = np.divmod(np.arange(1_000_000), 1000)
+    assert np.array_equal(got, (y + x).astype(np.int32))
+
+
+def test_depth_limit():
+    g = _graph("grid2d", 64)
+    p = CsrProblem.from_graph(g)
+    for lim in (0, 1, 5, 200):
+        _check_dist(g, p, 0, EXPAND_CONTRACT, N.ENACT_FUSED, depth_limit=lim)
+
+
+def test_isolated_and_edge_cases():
+    # vertex 2 has no edges; vertex 3 only a self-loop; source of degree 0
+    ro = np.array([0, 1, 2, 2, 3], np.int32)
+    ci = np.array([1, 0, 3], np.int32)
+    g = CsrGraph.from_arrays(ro, ci)
+    p = CsrProblem.from_graph(g)
+    for s in range(4):
+        _check_dist(g, p, s, EXPAND_CONTRACT, N.ENACT_FUSED)
+    with pytest.raises(B40cError) as e:
+        search(p, 9)
+    assert e.value.status == N.ERROR_INVALID_VALUE
+
+
+def test_hub_spanning_many_chunks():
+    # star: vertex 0 joined to 100k leaves (both directions): one list spans many chunks
+    n = 100_001
+    rows = np.concatenate([np.zeros(n - 1, np.int32), np.arange(1, n, dtype=np.int32)])
+    cols = np.concatenate([np.arange(1, n, dtype=np.int32), np.zeros(n - 1, np.int32)])
+    g = CsrGraph()
+    g.FromCoo(rows, cols, n)
+    p = CsrProblem.from_graph(g)
+    for mode in MODES:
+        _check_dist(g, p, 0, EXPAND_CONTRACT, mode)
+        _check_dist(g, p, 5, EXPAND_CONTRACT, mode)
+
+
+def test_queue_overflow_status():
+    g = _graph("grid2d", 200)
+    p = CsrProblem.from_graph(g)
+    with pytest.raises(B40cError) as e:
+        search(p, 0, queue_sizing=0.001)
+    assert e.value.status == N.ERROR_INVALID_CONFIGURATION
+
+
+def test_repeated_searches_without_reset():
+    g = _graph("rmat", 1 << 12, 1 << 15)
+    p = CsrProblem.from_graph(g)
+    enactor = ENACTORS[EXPAND_CONTRACT]()
+    N.check(p.Reset(enactor.GetFrontierType(), 1.3))
+    for s in sample_sources(g, 4, seed=3):
+        N.check(enactor.EnactFusedSearch(p, int(s)))
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        assert oracle.compare_labels(p.labels(), want) == -1
