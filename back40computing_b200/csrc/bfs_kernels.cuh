@@ -164,6 +164,92 @@ __device__ __forceinline__ int locate(const int32_t *P, int q, int x, ExpandSmem
     return lo;
 }
 
+// Turns the chunk's discovered vertices (s.out[0, s.out_count)) into entries
+// of the vertex frontier `vout`: reads each one's CSR row, drops degree-0
+// vertices, allocates slots with a CTA scan plus a decoupled look-back over
+// chunk ids, and writes (v, col, P).  The last chunk publishes the totals to
+// *q_out / *e_out and closes P.  All threads must call it.
+template <int B, bool PRED>
+__device__ __forceinline__ void emit_frontier(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int phase,
+                                              const VertexFrontier &vout, int32_t *q_out, int32_t *e_out,
+                                              bool &any_discovered)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int chunk = s.chunk;
+    const int cnt = s.out_count;
+    if (cnt > 0) any_discovered = true;
+    constexpr int PER = kChunkMax / B;
+    const int per = (cnt + B - 1) / B;
+    const int jb = min(tid * per, cnt), je = min(jb + per, cnt);
+    int rv[PER], rc[PER], rd[PER];
+    unsigned my_cnt = 0, my_deg = 0;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        rd[t] = 0;
+        rv[t] = -1;
+        rc[t] = 0;
+        if (jb + t < je) {
+            const int v = s.out[jb + t];
+            const int r0 = ld_ro(p.row_offsets + v);
+            const int r1 = ld_ro(p.row_offsets + v + 1);
+            rv[t] = v;
+            rc[t] = r0;
+            rd[t] = r1 - r0;
+            if (rd[t] > 0) {
+                my_cnt++;
+                my_deg += (unsigned)rd[t];
+            }
+        }
+    }
+    unsigned long long tot;
+    const unsigned long long excl = cta_exclusive_scan<B>(pack(my_cnt, my_deg), s.scan_warp, &tot);
+    const unsigned long long epoch = p.st->epoch + 4ull * (unsigned long long)level + (unsigned)phase;
+    if (warp == 0) {
+        unsigned long long prefix = 0;
+        if (chunk == 0) {
+            if (lane == 0) lookback_publish(&p.slots[0], epoch, kFlagInclusive, tot);
+        } else {
+            if (lane == 0) lookback_publish(&p.slots[chunk], epoch, kFlagAggregate, tot);
+            prefix = lookback_exclusive(p.slots, (unsigned)chunk, epoch, &p.st->error);
+            if (lane == 0 && prefix != ~0ull) lookback_publish(&p.slots[chunk], epoch, kFlagInclusive, prefix + tot);
+        }
+        if (lane == 0) {
+            s.prefix = prefix;
+            if (prefix != ~0ull && chunk == s.nchunks - 1) {
+                const unsigned long long all = prefix + tot;
+                const int qn = (int)(all >> 32);
+                const int en = (int)(all & 0xffffffffu);
+                if (qn > p.vcap) {
+                    atomicOr(&p.st->error, kErrOverflow);
+                } else {
+                    *q_out = qn;
+                    *e_out = en;
+                    vout.P[qn] = en;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const unsigned long long prefix = s.prefix;
+    if (prefix == ~0ull) return;
+    unsigned g = (unsigned)(prefix >> 32) + (unsigned)(excl >> 32);
+    unsigned d = (unsigned)(prefix & 0xffffffffu) + (unsigned)(excl & 0xffffffffu);
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        if (rd[t] > 0) {
+            if ((int)g < p.vcap) {
+                vout.v[g] = rv[t];
+                vout.col[g] = rc[t];
+                vout.P[g] = (int)d;
+            } else {
+                atomicOr(&p.st->error, kErrOverflow);
+            }
+            g++;
+            d += (unsigned)rd[t];
+        }
+    }
+}
+
 // ------------------------------------------------------------------------------------
 // Edge-balanced expansion of one chunk of a vertex frontier.
 //   FUSED_CULL = true  : expand-contract (EC): every gathered neighbour goes
@@ -401,80 +487,8 @@ __device__ __forceinline__ void expand_chunk(const BfsParams &p, const VertexFro
 
     if (!FUSED_CULL) return;
 
-    // ---- allocate the next frontier's slots (scan + decoupled look-back) ----------------
-    const int cnt = s.out_count;
-    if (cnt > 0) any_discovered = true;
-    constexpr int PER = kChunkMax / B;
-    const int per = (cnt + B - 1) / B;
-    const int jb = min(tid * per, cnt), je = min(jb + per, cnt);
-    int rv[PER], rc[PER], rd[PER];
-    unsigned my_cnt = 0, my_deg = 0;
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        rd[t] = 0;
-        rv[t] = -1;
-        rc[t] = 0;
-        if (jb + t < je) {
-            const int v = s.out[jb + t];
-            const int r0 = ld_ro(p.row_offsets + v);
-            const int r1 = ld_ro(p.row_offsets + v + 1);
-            rv[t] = v;
-            rc[t] = r0;
-            rd[t] = r1 - r0;
-            if (rd[t] > 0) {
-                my_cnt++;
-                my_deg += (unsigned)rd[t];
-            }
-        }
-    }
-    unsigned long long tot;
-    const unsigned long long excl = cta_exclusive_scan<B>(pack(my_cnt, my_deg), s.scan_warp, &tot);
-    const unsigned long long epoch = p.st->epoch + 4ull * (unsigned long long)level;
-    if (warp == 0) {
-        unsigned long long prefix = 0;
-        if (chunk == 0) {
-            if (lane == 0) lookback_publish(&p.slots[0], epoch, kFlagInclusive, tot);
-        } else {
-            if (lane == 0) lookback_publish(&p.slots[chunk], epoch, kFlagAggregate, tot);
-            prefix = lookback_exclusive(p.slots, (unsigned)chunk, epoch, &p.st->error);
-            if (lane == 0 && prefix != ~0ull) lookback_publish(&p.slots[chunk], epoch, kFlagInclusive, prefix + tot);
-        }
-        if (lane == 0) {
-            s.prefix = prefix;
-            if (prefix != ~0ull && chunk == s.nchunks - 1) {
-                const unsigned long long all = prefix + tot;
-                const int qn = (int)(all >> 32);
-                const int en = (int)(all & 0xffffffffu);
-                const int nb = (level + 1) & 1;
-                if (qn > p.vcap) {
-                    atomicOr(&p.st->error, kErrOverflow);
-                } else {
-                    p.st->q_len[nb] = qn;
-                    p.st->e_len[nb] = en;
-                    vout.P[qn] = en;
-                }
-            }
-        }
-    }
-    __syncthreads();
-    const unsigned long long prefix = s.prefix;
-    if (prefix == ~0ull) return;
-    unsigned g = (unsigned)(prefix >> 32) + (unsigned)(excl >> 32);
-    unsigned d = (unsigned)(prefix & 0xffffffffu) + (unsigned)(excl & 0xffffffffu);
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        if (rd[t] > 0) {
-            if ((int)g < p.vcap) {
-                vout.v[g] = rv[t];
-                vout.col[g] = rc[t];
-                vout.P[g] = (int)d;
-            } else {
-                atomicOr(&p.st->error, kErrOverflow);
-            }
-            g++;
-            d += (unsigned)rd[t];
-        }
-    }
+    emit_frontier<B, PRED>(p, s, level, 0, vout, &p.st->q_len[(level + 1) & 1], &p.st->e_len[(level + 1) & 1],
+                           any_discovered);
 }
 
 // ------------------------------------------------------------------------------------
@@ -583,6 +597,186 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     } else {
         finish_launch(p, level, 0, limit_hit);
     }
+}
+
+
+// ------------------------------------------------------------------------------------
+// Edge-frontier strategies (contract-expand, two-phase, hybrid)
+// ------------------------------------------------------------------------------------
+
+// Contraction of one chunk of an edge frontier: each item's visited bit is
+// test-and-set; a first visit labels the vertex with the current level (or
+// its predecessor) and the survivors become the vertex frontier vf[0].
+template <int B, bool PRED>
+__device__ __forceinline__ void contract_chunk(const BfsParams &p, ExpandSmem<B, PRED> &s, const EdgeFrontier &in,
+                                               int level, bool &any_discovered)
+{
+    const int tid = threadIdx.x;
+    const int C = s.C, chunk = s.chunk, q = s.q;
+    const int cs = chunk * C, ce = min(cs + C, q);
+    if (tid == 0) s.out_count = 0;
+    __syncthreads();
+    constexpr int U = 4;
+    for (int base = cs; base < ce; base += B * U) {
+        int v[U], u[U];
+        bool valid[U];
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            const int i = base + t * B + tid;
+            valid[t] = i < ce;
+            v[t] = valid[t] ? ld_cg(in.v + i) : -1;
+            u[t] = (PRED && valid[t]) ? ld_cg(in.pred + i) : -1;
+        }
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            bool ok = valid[t];
+            if (p.warp_cull) ok = warp_cull(ok, v[t]);
+            const bool found = ok && discover<PRED>(p, v[t], u[t], level, p.precheck);
+            push_out(found, v[t], s.out, &s.out_count);
+        }
+    }
+    __syncthreads();
+    emit_frontier<B, PRED>(p, s, level, 1, p.vf[0], &p.st->vq_len, &p.st->ve_len, any_discovered);
+}
+
+// Per level: contract the edge frontier into vf[0], then expand vf[0] into
+// the next edge frontier (flattened edge positions, no allocation needed).
+// phase_mask selects the phases of a non-persistent launch; a persistent
+// launch runs both with a grid barrier after each.  With `hybrid`, a
+// persistent launch returns when the edge frontier exceeds
+// gridDim * saturation items (SATURATION_QUIT, enactor_hybrid.cuh:571).
+template <int B, bool PRED>
+__global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ExpandSmem<B, PRED> &s = *reinterpret_cast<ExpandSmem<B, PRED> *>(smem_raw);
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    if (tid == 0) mbar_init(&s.bar, 1);
+    unsigned bar_phase = 0, generation = 0;
+    int max_level_seen = -1;
+    int level = ld_cg(&p.st->cur_level);
+    bool limit_hit = false, saturated = false, completed_level = false, failed = false;
+    __syncthreads();
+    for (int iter = 0; iter < p.max_levels; iter++, level++) {
+        const int in_idx = p.edge_pingpong ? (level & 1) : 0;
+        const int out_idx = p.edge_pingpong ? ((level + 1) & 1) : 0;
+        if (p.phase_mask & 1) {
+            const int pass = 2 * level;
+            if (tid == 0) {
+                s.q = ld_cg(&p.st->q_len[level & 1]);
+                if (blockIdx.x == 0) p.st->chunk_ctr[(pass + 1) % 3] = 0;
+            }
+            __syncthreads();
+            const int q = s.q;
+            if (ld_cg(&p.st->error) != 0) {
+                failed = true;
+                break;
+            }
+            if (q == 0) {
+                if (tid == 0 && blockIdx.x == 0) p.st->vq_len = p.st->ve_len = 0;
+                break;
+            }
+            if (p.hybrid && p.persistent && q > (int)gridDim.x * p.saturation) {
+                saturated = true;
+                break;
+            }
+            if (tid == 0) {
+                s.C = level_chunk(q, p.chunk_edges);
+                s.nchunks = (q + s.C - 1) / s.C;
+                if (s.nchunks > p.max_chunks) {
+                    atomicOr(&p.st->error, kErrOverflow);
+                    s.nchunks = 0;
+                }
+                if (blockIdx.x == 0) atomicAdd(&p.st->total_queued, (unsigned long long)q);
+            }
+            __syncthreads();
+            bool any = false;
+            while (true) {
+                if (tid == 0) s.chunk = (int)atomicAdd(&p.st->chunk_ctr[pass % 3], 1u);
+                __syncthreads();
+                if (s.chunk >= s.nchunks) break;
+                contract_chunk<B, PRED>(p, s, p.ef[in_idx], level, any);
+                __syncthreads();
+            }
+            if (any) max_level_seen = max(max_level_seen, level);
+            if (p.persistent) {
+                if ((int)blockIdx.x == p.skip_arrival_cta) {
+                    if (tid == 0) atomicOr(&p.st->error, kErrInjected);
+                    return;
+                }
+                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) {
+                    failed = true;
+                    break;
+                }
+            }
+        }
+        const int dl = p.st->depth_limit;
+        if (dl >= 0 && level >= dl) {
+            limit_hit = true;
+            if (tid == 0 && blockIdx.x == 0) p.st->q_len[(level + 1) & 1] = 0;
+            break;
+        }
+        if (p.phase_mask & 2) {
+            const int pass = 2 * level + 1;
+            if (tid == 0) {
+                s.q = ld_cg(&p.st->vq_len);
+                s.E = ld_cg(&p.st->ve_len);
+                if (blockIdx.x == 0) p.st->chunk_ctr[(pass + 1) % 3] = 0;
+            }
+            __syncthreads();
+            const int q = s.q, E = s.E;
+            if (E > p.ecap) {
+                if (tid == 0) atomicOr(&p.st->error, kErrOverflow);
+                failed = true;
+                break;
+            }
+            if (tid == 0 && blockIdx.x == 0) p.st->q_len[(level + 1) & 1] = q == 0 ? 0 : E;
+            if (q > 0) {
+                const int stride0 = (q + 256) / 256;
+                for (int t = tid; t <= 256; t += B) s.probe[t] = ld_cg(p.vf[0].P + min(t * stride0, q));
+                if (tid == 0) {
+                    s.C = level_chunk(E, p.chunk_edges);
+                    s.nchunks = (E + s.C - 1) / s.C;
+                    if (s.nchunks > p.max_chunks) {
+                        atomicOr(&p.st->error, kErrOverflow);
+                        s.nchunks = 0;
+                    }
+                }
+                __syncthreads();
+                bool unused = false;
+                while (true) {
+                    if (tid == 0) s.chunk = (int)atomicAdd(&p.st->chunk_ctr[pass % 3], 1u);
+                    __syncthreads();
+                    if (s.chunk >= s.nchunks) break;
+                    expand_chunk<B, PRED, false>(p, p.vf[0], s, level, p.vf[1], p.ef[out_idx], bar_phase, unused);
+                    __syncthreads();
+                }
+            }
+            completed_level = true;
+            if (p.persistent) {
+                if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
+                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) {
+                    failed = true;
+                    break;
+                }
+            }
+        }
+        if (!p.persistent) break;
+    }
+    if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
+    if (p.persistent) {
+        if (tid == 0 && blockIdx.x == 0) {
+            p.st->cur_level = level;
+            if (saturated)
+                p.st->saturated = 1;
+            else
+                p.st->done = 1;
+        }
+    } else if (completed_level || limit_hit) {
+        finish_launch(p, level, 0, limit_hit);
+    }
+    (void)failed;
 }
 
 // Sets up a search: the source's label, visited bit and the level-0

@@ -45,7 +45,9 @@ struct alignas(128) SearchState {
     uint32_t finished;         // CTAs that finished the current non-persistent launch
     int32_t src;               // source vertex (read by the init kernel)
     int32_t depth_limit;       // < 0: unlimited
-    int32_t pad[5];
+    int32_t vq_len;            // edge strategies: contracted vertex frontier length
+    int32_t ve_len;            // edge strategies: its edge total
+    int32_t pad[3];
 };
 
 // Kernel parameter block.
@@ -73,7 +75,10 @@ struct BfsParams {
     int32_t saturation;       // hybrid: leave the fused kernel when items > gridDim * saturation
     int32_t persistent;       // 1: loop over levels with the grid barrier
     int32_t skip_arrival_cta; // test-only fault injection: this CTA never arrives (-1 = off)
-    int32_t pad0;
+    int32_t edge_pingpong;    // edge strategies: 1 = two edge frontiers (EDGE_FRONTIERS), 0 = one (MIXED)
+    int32_t phase_mask;       // edge kernel: 1 = contract, 2 = expand, 3 = both per level (persistent)
+    int32_t hybrid;           // edge kernel: leave the persistent loop when the frontier saturates
+    int32_t pad1;
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
 };
 

@@ -1,0 +1,66 @@
+// Expand-contract enactor (vertex frontiers): one persistent cooperative
+// grid (fused), one launch per level (iterative), or a CUDA graph of the
+// whole search with a conditional WHILE node over levels.
+#include "launch_common.cuh"
+
+namespace b40c {
+namespace rt {
+
+namespace {
+
+template <bool PRED>
+int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol, int32_t depth_limit)
+{
+    int rc;
+    if ((rc = ensure_vf(p, 0, cap_of(p->queue_sizing, p->nodes)))) return rc;
+    if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
+    if ((rc = ensure_slots(p))) return rc;
+    BfsParams k = make_params(p, pol);
+    const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
+    const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
+    int grid = 0;
+    if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
+    if ((rc = begin_enact(p, src, depth_limit))) return rc;
+    if (mode == B40C_ENACT_GRAPH) {
+        if ((rc = mark_search_start(p))) return rc;
+        KernelNode init{init_kernel_ptr<PRED>(true, true), dim3(init_grid(p, true)), dim3(kThreads), 0, k};
+        KernelNode body{kern, dim3(grid), dim3(kThreads), smem, k};
+        if ((rc = run_graph(p, B40C_EXPAND_CONTRACT, init, &body, 1))) return rc;
+        return finish_timing(p);
+    }
+    if ((rc = upload_source(p))) return rc;
+    if ((rc = launch_init<PRED>(p, k, true, p->needs_init))) return rc;
+    if ((rc = mark_search_start(p))) return rc;
+    if (mode == B40C_ENACT_FUSED) {
+        k.persistent = 1;
+        k.max_levels = INT32_MAX;
+        k.skip_arrival_cta = injected_skip_cta();
+        if ((rc = launch_cooperative(p, kern, grid, smem, k, "cooperative launch of the expand-contract kernel")))
+            return rc;
+    } else if (mode == B40C_ENACT_ITERATIVE) {
+        // one launch per level; the host reads the next frontier's size
+        for (int level = 0;; level++) {
+            if ((rc = read_state(p))) return rc;
+            if (p->h_st->error || p->h_st->done) break;
+            const int q = p->h_st->q_len[level & 1], E = p->h_st->e_len[level & 1];
+            if (q == 0) break;
+            const int g = std::max(1, std::min(grid, (E + 255) / 256));
+            if ((rc = launch_plain(p, kern, g, smem, k, "expand-contract level launch"))) return rc;
+        }
+    } else {
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown enact mode %d", mode);
+    }
+    return finish_timing(p);
+}
+
+}  // namespace
+
+int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
+                 int32_t depth_limit)
+{
+    return p->mark_pred ? enact_ec_t<true>(p, mode, src, max_grid, pol, depth_limit)
+                        : enact_ec_t<false>(p, mode, src, max_grid, pol, depth_limit);
+}
+
+}  // namespace rt
+}  // namespace b40c

@@ -1,0 +1,84 @@
+// Launch helpers shared by the enactor translation units.
+#pragma once
+#include "bfs_kernels.cuh"
+#include "problem.h"
+
+namespace b40c {
+namespace rt {
+
+// Grid of the set-up kernel: the full label/mask initialisation is a
+// grid-stride fill, the source-only set-up a single CTA.
+inline int init_grid(b40c_bfs_problem *p, bool full)
+{
+    return full ? std::max(1, std::min<int>(p->sms * 8, (int)((p->nodes + kThreads - 1) / kThreads))) : 1;
+}
+
+template <bool PRED>
+const void *init_kernel_ptr(bool vertex_frontier, bool full)
+{
+    if (vertex_frontier)
+        return full ? (const void *)dev::init_kernel<PRED, true, true> : (const void *)dev::init_kernel<PRED, true, false>;
+    return full ? (const void *)dev::init_kernel<PRED, false, true> : (const void *)dev::init_kernel<PRED, false, false>;
+}
+
+template <bool PRED>
+int launch_init(b40c_bfs_problem *p, const BfsParams &k, bool vertex_frontier, bool full)
+{
+    BfsParams kk = k;
+    void *args[] = {&kk};
+    CUDA_TRY(cudaLaunchKernel(init_kernel_ptr<PRED>(vertex_frontier, full), dim3(init_grid(p, full)), dim3(kThreads),
+                              args, 0, p->stream),
+             "init kernel launch");
+    return B40C_SUCCESS;
+}
+
+// Common start of an enact: uploads (source, depth limit) and records the
+// enact's start event.
+inline int begin_enact(b40c_bfs_problem *p, int32_t src, int32_t depth_limit)
+{
+    p->h_st->src = src;
+    p->h_st->depth_limit = depth_limit;
+    CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
+    return B40C_SUCCESS;
+}
+
+inline int upload_source(b40c_bfs_problem *p)
+{
+    CUDA_TRY(cudaMemcpyAsync(&p->st->src, &p->h_st->src, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
+             "source upload");
+    return B40C_SUCCESS;
+}
+
+inline int mark_search_start(b40c_bfs_problem *p)
+{
+    CUDA_TRY(cudaEventRecord(p->ring_a[p->ring_pos], p->stream), "event record");
+    return B40C_SUCCESS;
+}
+
+inline int launch_cooperative(b40c_bfs_problem *p, const void *kern, int grid, size_t smem, BfsParams &k,
+                              const char *what)
+{
+    void *args[] = {&k};
+    CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream), what);
+    return B40C_SUCCESS;
+}
+
+inline int launch_plain(b40c_bfs_problem *p, const void *kern, int grid, size_t smem, BfsParams &k, const char *what)
+{
+    void *args[] = {&k};
+    CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream), what);
+    return B40C_SUCCESS;
+}
+
+// Test-only fault injection: B40C_TEST_SKIP_ARRIVAL_CTA=<cta> makes that CTA
+// of a persistent launch leave without arriving at the grid barrier, so the
+// other CTAs' bounded waits expire and the search reports
+// B40C_ERROR_LAUNCH_TIMEOUT.
+inline int injected_skip_cta()
+{
+    const char *inj = getenv("B40C_TEST_SKIP_ARRIVAL_CTA");
+    return inj ? atoi(inj) : -1;
+}
+
+}  // namespace rt
+}  // namespace b40c

@@ -1,97 +1,16 @@
-// Host runtime of the BFS library: problem state (CsrProblem), the enactors
-// (per-level launches, persistent grid, CUDA-graph replay) and the C ABI.
-#include <cuda_runtime.h>
-
-#include <algorithm>
-#include <cmath>
-#include <cstdio>
-#include <cstring>
-#include <mutex>
+// Problem allocation, policies and the C ABI of the BFS library.
 #include <vector>
 
-#include "b40c_bfs.h"
 #include "bfs_kernels.cuh"
-#include "bfs_strategies.cuh"
-#include "errors.h"
-
-using namespace b40c;
-using b40c::dev::LookbackSlot;
+#include "problem.h"
 
 #define B40C_VERSION_STRING "b40c-b200 0.1 (sm_100a)"
 
-namespace {
+using namespace b40c;
+using namespace b40c::rt;
 
-constexpr int kThreads = 256;
-
-#define CUDA_TRY(call, what)                                                                             \
-    do {                                                                                                 \
-        cudaError_t _e = (call);                                                                         \
-        if (_e != cudaSuccess) {                                                                         \
-            cudaGetLastError();                                                                          \
-            return b40c::fail((int)_e, "%s failed: %s", what, cudaGetErrorString(_e));                  \
-        }                                                                                                \
-    } while (0)
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev)
-    {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard()
-    {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
-
-}  // namespace
-
-struct b40c_bfs_problem {
-    int device = 0;
-    int64_t nodes = 0, edges = 0;
-    int mark_pred = 0;
-    int stream_from_host = 0;
-    int sms = 0;
-    // CSR
-    int32_t *d_ro = nullptr, *d_ci = nullptr;
-    bool own_csr = true;
-    const void *reg_ro = nullptr, *reg_ci = nullptr;  // host arrays registered for zero-copy
-    // search arrays
-    int32_t *d_labels = nullptr;
-    uint32_t *d_mask = nullptr;
-    int32_t mask_words = 0;
-    // frontiers
-    VertexFrontier vf[2] = {};
-    int64_t vcap[2] = {0, 0};
-    EdgeFrontier ef[2] = {};
-    int64_t ecap[2] = {0, 0};
-    double queue_sizing = 1.3;
-    LookbackSlot *slots = nullptr;
-    int32_t max_slots = 0;
-    SearchState *st = nullptr;
-    SearchState *h_st = nullptr;  // pinned mirror
-    // streams / timing
-    cudaStream_t stream = nullptr, own_stream = nullptr;
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    // ring of event pairs bracketing the search kernels (after source set-up)
-    // of the most recent enacts, for per-launch device times
-    static constexpr int kRing = 256;
-    cudaEvent_t ring_a[kRing] = {}, ring_b[kRing] = {};
-    int ring_pos = 0, ring_count = 0;
-    bool timed = false;
-    bool needs_init = true;  // labels/mask dirty since the last reset
-    // last search
-    int64_t total_queued = 0;
-    int32_t search_depth = 0;
-    double avg_duty = 0.0;
-    bool stats_valid = false;
-    int last_strategy = -1;
-};
-
-namespace {
+namespace b40c {
+namespace rt {
 
 int alloc_dev(void **p, size_t bytes, const char *what)
 {
@@ -161,9 +80,9 @@ int ensure_slots(b40c_bfs_problem *p)
     if (p->slots) cudaFree(p->slots);
     p->slots = nullptr;
     p->max_slots = 0;
-    int rc = alloc_dev((void **)&p->slots, sizeof(LookbackSlot) * need, "look-back slots");
+    int rc = alloc_dev((void **)&p->slots, sizeof(dev::LookbackSlot) * need, "look-back slots");
     if (rc) return rc;
-    CUDA_TRY(cudaMemsetAsync(p->slots, 0, sizeof(LookbackSlot) * need, p->stream), "memset look-back slots");
+    CUDA_TRY(cudaMemsetAsync(p->slots, 0, sizeof(dev::LookbackSlot) * need, p->stream), "memset look-back slots");
     p->max_slots = (int32_t)need;
     return B40C_SUCCESS;
 }
@@ -263,11 +182,8 @@ int check_state_errors(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
-}  // namespace
 
-namespace b40c {
-// Shared helpers for bfs_strategies.cuh users.
-int runtime_persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_policy &pol, int max_grid,
+int persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_policy &pol, int max_grid,
                             size_t smem, int *grid)
 {
     int per_sm = 0;
@@ -280,11 +196,6 @@ int runtime_persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_
     *grid = std::max(g, 1);
     return B40C_SUCCESS;
 }
-}  // namespace b40c
-
-namespace {
-
-// ---- enactors -----------------------------------------------------------------------
 
 int finish_timing(b40c_bfs_problem *p)
 {
@@ -296,69 +207,78 @@ int finish_timing(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
-template <bool PRED>
-int launch_init(b40c_bfs_problem *p, const BfsParams &k, bool vertex_frontier, bool full)
+
+void free_graphs(b40c_bfs_problem *p)
 {
-    const int grid = full ? std::max(1, std::min<int>(p->sms * 8, (int)((p->nodes + kThreads - 1) / kThreads))) : 1;
-    if (vertex_frontier) {
-        if (full) dev::init_kernel<PRED, true, true><<<grid, kThreads, 0, p->stream>>>(k);
-        else dev::init_kernel<PRED, true, false><<<grid, kThreads, 0, p->stream>>>(k);
-    } else {
-        if (full) dev::init_kernel<PRED, false, true><<<grid, kThreads, 0, p->stream>>>(k);
-        else dev::init_kernel<PRED, false, false><<<grid, kThreads, 0, p->stream>>>(k);
+    for (int s = 0; s < 4; s++)
+        if (p->graph_exec[s]) {
+            cudaGraphExecDestroy(p->graph_exec[s]);
+            p->graph_exec[s] = nullptr;
+        }
+}
+
+int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode *body, int n_body)
+{
+    if (!p->graph_exec[slot] || memcmp(&p->graph_params[slot], &body[0].params, sizeof(BfsParams)) != 0 ||
+        p->graph_grid[slot] != (int)body[0].grid.x) {
+        if (p->graph_exec[slot]) {
+            cudaGraphExecDestroy(p->graph_exec[slot]);
+            p->graph_exec[slot] = nullptr;
+        }
+        cudaGraph_t g = nullptr;
+        CUDA_TRY(cudaGraphCreate(&g, 0), "cudaGraphCreate");
+        struct GraphHolder {
+            cudaGraph_t g;
+            ~GraphHolder() { cudaGraphDestroy(g); }
+        } holder{g};
+        cudaGraphNode_t n_copy, n_init, n_loop;
+        CUDA_TRY(cudaGraphAddMemcpyNode1D(&n_copy, g, nullptr, 0, &p->st->src, &p->h_st->src, 2 * sizeof(int32_t),
+                                          cudaMemcpyHostToDevice),
+                 "graph memcpy node");
+        BfsParams init_params = init.params;
+        void *init_args[] = {&init_params};
+        cudaKernelNodeParams kp = {};
+        kp.func = (void *)init.func;
+        kp.gridDim = init.grid;
+        kp.blockDim = init.block;
+        kp.sharedMemBytes = (unsigned)init.smem;
+        kp.kernelParams = init_args;
+        CUDA_TRY(cudaGraphAddKernelNode(&n_init, g, &n_copy, 1, &kp), "graph init node");
+        cudaGraphConditionalHandle handle;
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault),
+                 "cudaGraphConditionalHandleCreate");
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        CUDA_TRY(cudaGraphAddNode(&n_loop, g, &n_init, 1, &cp), "graph WHILE node");
+        cudaGraph_t loop_body = cp.conditional.phGraph_out[0];
+        cudaGraphNode_t prev = nullptr;
+        for (int i = 0; i < n_body; i++) {
+            BfsParams bp = body[i].params;
+            bp.cond_handle = (i == n_body - 1) ? (unsigned long long)handle : 0ull;
+            void *args[] = {&bp};
+            cudaKernelNodeParams kb = {};
+            kb.func = (void *)body[i].func;
+            kb.gridDim = body[i].grid;
+            kb.blockDim = body[i].block;
+            kb.sharedMemBytes = (unsigned)body[i].smem;
+            kb.kernelParams = args;
+            cudaGraphNode_t n;
+            CUDA_TRY(cudaGraphAddKernelNode(&n, loop_body, prev ? &prev : nullptr, prev ? 1 : 0, &kb), "graph body node");
+            prev = n;
+        }
+        CUDA_TRY(cudaGraphInstantiate(&p->graph_exec[slot], g, 0), "cudaGraphInstantiate");
+        p->graph_params[slot] = body[0].params;
+        p->graph_grid[slot] = (int)body[0].grid.x;
     }
-    CUDA_TRY(cudaGetLastError(), "init kernel launch");
+    CUDA_TRY(cudaGraphLaunch(p->graph_exec[slot], p->stream), "cudaGraphLaunch");
     return B40C_SUCCESS;
 }
 
-template <bool PRED>
-int enact_ec(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol, int32_t depth_limit)
-{
-    int rc;
-    if ((rc = ensure_vf(p, 0, cap_of(p->queue_sizing, p->nodes)))) return rc;
-    if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
-    if ((rc = ensure_slots(p))) return rc;
-    BfsParams k = make_params(p, pol);
-    const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
-    const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
-    int grid = 0;
-    if ((rc = runtime_persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
-    p->h_st->src = src;
-    p->h_st->depth_limit = depth_limit;
-    CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
-    CUDA_TRY(cudaMemcpyAsync(&p->st->src, &p->h_st->src, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
-             "source upload");
-    if ((rc = launch_init<PRED>(p, k, true, p->needs_init))) return rc;
-    CUDA_TRY(cudaEventRecord(p->ring_a[p->ring_pos], p->stream), "event record");
-    if (mode == B40C_ENACT_FUSED) {
-        k.persistent = 1;
-        k.max_levels = INT32_MAX;
-        const char *inj = getenv("B40C_TEST_SKIP_ARRIVAL_CTA");
-        if (inj) k.skip_arrival_cta = atoi(inj);
-        void *args[] = {&k};
-        CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream),
-                 "cooperative launch of the expand-contract kernel");
-    } else if (mode == B40C_ENACT_ITERATIVE) {
-        // one launch per level; the host reads the next frontier's size
-        k.persistent = 0;
-        k.max_levels = 1;
-        for (int level = 0;; level++) {
-            if ((rc = read_state(p))) return rc;
-            if (p->h_st->error || p->h_st->done) break;
-            const int q = p->h_st->q_len[level & 1], E = p->h_st->e_len[level & 1];
-            if (q == 0) break;
-            if (depth_limit >= 0 && level >= depth_limit) break;
-            const int g = std::max(1, std::min(grid, (E + 255) / 256));
-            dev::ec_kernel<kThreads, PRED><<<g, kThreads, smem, p->stream>>>(k);
-            CUDA_TRY(cudaGetLastError(), "expand-contract level launch");
-        }
-    } else {
-        return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown enact mode %d", mode);
-    }
-    return finish_timing(p);
-}
-
-}  // namespace
+}  // namespace rt
+}  // namespace b40c
 
 // ---- C ABI -----------------------------------------------------------------------------
 
@@ -512,6 +432,7 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (!p) return B40C_SUCCESS;
     DeviceGuard guard(p->device);
     if (p->stream) cudaStreamSynchronize(p->stream);
+    free_graphs(p);
     if (p->own_csr) {
         if (p->d_ro) cudaFree(p->d_ro);
         if (p->d_ci) cudaFree(p->d_ci);
@@ -588,18 +509,15 @@ int b40c_bfs_enact_limited(b40c_bfs_problem *p, int strategy, int mode, int32_t 
     int rc = resolve_policy(strategy, policy, &pol);
     if (rc) return rc;
     DeviceGuard guard(p->device);
-    p->stats_valid = false;
     p->timed = false;
-    p->last_strategy = strategy;
     switch (strategy) {
     case B40C_EXPAND_CONTRACT:
-        rc = p->mark_pred ? enact_ec<true>(p, mode, src, max_grid_size, pol, depth_limit)
-                          : enact_ec<false>(p, mode, src, max_grid_size, pol, depth_limit);
+        rc = enact_vertex(p, mode, src, max_grid_size, pol, depth_limit);
         break;
     case B40C_CONTRACT_EXPAND:
     case B40C_TWO_PHASE:
     case B40C_HYBRID:
-        rc = b40c::enact_edge_strategy(p, strategy, mode, src, max_grid_size, pol, depth_limit);
+        rc = enact_edge(p, strategy, mode, src, max_grid_size, pol, depth_limit);
         break;
     default:
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown strategy %d", strategy);

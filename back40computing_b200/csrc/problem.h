@@ -1,0 +1,127 @@
+// Host-side state of a BFS problem (the role of bfs::CsrProblem and the
+// enactors' lazily allocated resources) shared by the runtime translation
+// units: problem.cu (C ABI, allocation), enact_vertex.cu (expand-contract),
+// enact_edge.cu (contract-expand, two-phase, hybrid).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "b40c_bfs.h"
+#include "bfs_state.h"
+#include "device_primitives.cuh"
+#include "errors.h"
+
+#define CUDA_TRY(call, what)                                                                             \
+    do {                                                                                                 \
+        cudaError_t _e = (call);                                                                         \
+        if (_e != cudaSuccess) {                                                                         \
+            cudaGetLastError();                                                                          \
+            return b40c::fail((int)_e, "%s failed: %s", what, cudaGetErrorString(_e));                  \
+        }                                                                                                \
+    } while (0)
+
+
+struct b40c_bfs_problem {
+    int device = 0;
+    int64_t nodes = 0, edges = 0;
+    int mark_pred = 0;
+    int stream_from_host = 0;
+    int sms = 0;
+    // CSR
+    int32_t *d_ro = nullptr, *d_ci = nullptr;
+    bool own_csr = true;
+    const void *reg_ro = nullptr, *reg_ci = nullptr;  // host arrays registered for zero-copy
+    // search arrays
+    int32_t *d_labels = nullptr;
+    uint32_t *d_mask = nullptr;
+    int32_t mask_words = 0;
+    // frontiers
+    b40c::VertexFrontier vf[2] = {};
+    int64_t vcap[2] = {0, 0};
+    b40c::EdgeFrontier ef[2] = {};
+    int64_t ecap[2] = {0, 0};
+    double queue_sizing = 1.3;
+    b40c::dev::LookbackSlot *slots = nullptr;
+    int32_t max_slots = 0;
+    b40c::SearchState *st = nullptr;
+    b40c::SearchState *h_st = nullptr;  // pinned mirror
+    // streams / timing
+    cudaStream_t stream = nullptr, own_stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // ring of event pairs bracketing the search kernels (after source set-up)
+    // of the most recent enacts, for per-launch device times
+    static constexpr int kRing = 256;
+    cudaEvent_t ring_a[kRing] = {}, ring_b[kRing] = {};
+    int ring_pos = 0, ring_count = 0;
+    bool timed = false;
+    bool needs_init = true;  // labels/mask dirty since the last reset
+    // CUDA graphs of whole searches (ENACT_GRAPH), one per strategy, rebuilt
+    // when the kernel parameters (buffers, policy) or the grid change
+    cudaGraphExec_t graph_exec[4] = {};
+    b40c::BfsParams graph_params[4] = {};
+    int graph_grid[4] = {};
+};
+
+namespace b40c {
+namespace rt {
+
+constexpr int kThreads = 256;
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int alloc_dev(void **p, size_t bytes, const char *what);
+void free_vf(VertexFrontier &f);
+void free_ef(EdgeFrontier &f);
+int ensure_vf(b40c_bfs_problem *p, int i, int64_t cap);
+int ensure_ef(b40c_bfs_problem *p, int i, int64_t cap);
+int64_t cap_of(double qs, int64_t base);
+int ensure_slots(b40c_bfs_problem *p);
+BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol);
+b40c_bfs_policy default_policy(int strategy);
+int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out);
+int read_state(b40c_bfs_problem *p);
+int check_state_errors(b40c_bfs_problem *p);
+int persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_policy &pol, int max_grid, size_t smem,
+                    int *grid);
+int finish_timing(b40c_bfs_problem *p);
+void free_graphs(b40c_bfs_problem *p);
+
+// One kernel launch of a captured search.
+struct KernelNode {
+    const void *func;
+    dim3 grid, block;
+    size_t smem;
+    BfsParams params;
+};
+// Builds (or reuses) and launches the whole-search graph of `slot`: source
+// upload -> `init` -> conditional WHILE { body[0..n_body) }.  The body's
+// last node sets the loop condition (its params get the handle).
+int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode *body, int n_body);
+
+// enactors
+int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
+                 int32_t depth_limit);
+int enact_edge(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
+               int32_t depth_limit);
+
+}  // namespace rt
+}  // namespace b40c

@@ -10,15 +10,16 @@ from back40computing_b200.bfs import EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE
 
 pytestmark = pytest.mark.gpu
 
-MODES = [N.ENACT_FUSED, N.ENACT_ITERATIVE]
+MODES = [N.ENACT_FUSED, N.ENACT_ITERATIVE, N.ENACT_GRAPH]
 
 
 def _graph(kind, *args, **kw):
     g = CsrGraph()
-    {"grid2d": BuildGrid2dGraph, "grid3d": BuildGrid3dGraph, "rmat": BuildRmatGraph,
-     "rr": BuildRandomRegularishGraph, "random": BuildRandomGraph}[kind](*args, g, **kw) if kind in (
-        "grid2d", "grid3d") else None
-    if kind == "rmat":
+    if kind == "grid2d":
+        BuildGrid2dGraph(args[0], g)
+    elif kind == "grid3d":
+        BuildGrid3dGraph(args[0], g)
+    elif kind == "rmat":
         BuildRmatGraph(args[0], args[1], g, True, 0.57, 0.19, 0.19, seed=kw.get("seed", 0),
                        permute=kw.get("permute", True))
     elif kind == "rr":
@@ -36,7 +37,7 @@ def _check_dist(g, problem, src, strategy, mode, **kw):
     return depth
 
 
-STRATS = [EXPAND_CONTRACT]
+STRATS = [EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID]
 
 
 @pytest.mark.parametrize("strategy", STRATS)
