@@ -25,7 +25,7 @@ ERROR_LAUNCH_TIMEOUT = 702
 ERROR_NOT_SUPPORTED = 801
 
 VERTEX_FRONTIERS, EDGE_FRONTIERS, MIXED_FRONTIERS, MULTI_GPU_FRONTIERS = 0, 1, 2, 3
-EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID = 0, 1, 2, 3
+EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID, DIRECTION_OPTIMIZING = 0, 1, 2, 3, 4
 ENACT_FUSED, ENACT_ITERATIVE, ENACT_GRAPH = 0, 1, 2
 
 
@@ -39,6 +39,9 @@ class Policy(C.Structure):
         ("saturation_quit", C.c_int32),
         ("warp_cull", C.c_int32),
         ("bitmask_precheck", C.c_int32),
+        ("queue_allocation", C.c_int32),
+        ("bottom_up_alpha", C.c_int32),
+        ("bottom_up_beta", C.c_int32),
     ]
 
 
@@ -93,6 +96,7 @@ SIGNATURES: dict[str, tuple] = {
                                          C.POINTER(Policy)]),
     "b40c_bfs_extract": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_stats": (C.c_int, [C.c_void_p, _P_i64, _P_i32, C.POINTER(C.c_double)]),
+    "b40c_bfs_problem_is_symmetric": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_last_elapsed_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "b40c_bfs_recent_search_ms": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),

@@ -28,6 +28,7 @@ EXPAND_CONTRACT = N.EXPAND_CONTRACT
 CONTRACT_EXPAND = N.CONTRACT_EXPAND
 TWO_PHASE = N.TWO_PHASE
 HYBRID = N.HYBRID
+DIRECTION_OPTIMIZING = N.DIRECTION_OPTIMIZING
 
 Policy = N.Policy
 
@@ -110,6 +111,11 @@ class CsrProblem:
         N.check(N.lib().b40c_bfs_recent_search_ms(self.handle, int(count), out), "recent_search_ms")
         return np.array(out[:], dtype=np.float64)
 
+    def is_symmetric(self) -> bool:
+        out = C.c_int32(0)
+        N.check(N.lib().b40c_bfs_problem_is_symmetric(self.handle, C.byref(out)), "is_symmetric")
+        return bool(out.value)
+
     def device_view(self) -> N.DeviceView:
         v = N.DeviceView()
         N.check(N.lib().b40c_bfs_device_view_get(self.handle, C.byref(v)), "device_view")
@@ -190,11 +196,20 @@ class EnactorHybrid(_Enactor):
         return self._enact(problem, src, N.ENACT_FUSED, max_grid_size)
 
 
+class EnactorDirectionOptimizing(_Enactor):
+    """No counterpart in the reference: top-down expand-contract levels plus
+    bottom-up levels while the frontier is large (undirected graphs only; a
+    directed graph runs plain expand-contract).  Same labels as the others."""
+    STRATEGY = DIRECTION_OPTIMIZING
+    FRONTIER = VERTEX_FRONTIERS
+
+
 ENACTORS = {
     EXPAND_CONTRACT: EnactorExpandContract,
     CONTRACT_EXPAND: EnactorContractExpand,
     TWO_PHASE: EnactorTwoPhase,
     HYBRID: EnactorHybrid,
+    DIRECTION_OPTIMIZING: EnactorDirectionOptimizing,
 }
 
 

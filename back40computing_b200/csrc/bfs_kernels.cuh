@@ -10,16 +10,21 @@
 //    layout as the reference's byte mask); discovery is an atomicOr
 //    test-and-set, so every vertex is labelled and enqueued exactly once and
 //    labels never race;
-//  * vertex frontiers carry each entry's degree prefix P, so the next level
-//    splits its flattened edge space into equal chunks (edge-balanced): a
-//    hub's adjacency list is spread over many CTAs;
-//  * inside a chunk, adjacency runs are gathered three ways: CTA-cooperative
-//    (runs >= cta_thresh, bulk-copied into shared memory with cp.async.bulk),
-//    warp-cooperative (runs >= warp_thresh), and scan-based fine-grained
-//    (shorter runs, through a shared-memory slot -> owner map);
-//  * queue slots come from a CTA-wide shuffle scan and a decoupled look-back
-//    over chunk ids (one 64-bit (count, degree-sum) pair per chunk), never
-//    from per-item atomics;
+//  * vertex frontiers carry each entry's degree prefix P and a chunk-first
+//    index cf, so a level's flattened edge space is cut into equal
+//    contiguous ranges, one per CTA (edge-balanced: a hub's adjacency list is
+//    spread over many CTAs), walked in sub-rounds of kChunkMax edges;
+//  * inside a sub-round, adjacency runs are gathered three ways: CTA-
+//    cooperative (the sub-round lies inside one list: one cp.async.bulk
+//    copy into shared memory), warp-cooperative (a warp reads 32 consecutive
+//    positions of a run, one coalesced segment) and scan-based fine-grained
+//    (short runs through a shared-memory position -> owner map);
+//  * discovery is issued in overlapped phases (pre-check loads, atomics, CSR
+//    rows of the winners) so every thread keeps its memory operations in
+//    flight;
+//  * frontier slots come from a CTA-wide shuffle scan plus either a
+//    decoupled look-back over tile ids or one packed 64-bit atomic per tile,
+//    never from per-item atomics;
 //  * one kernel body serves per-level launches, CUDA-graph replays and a
 //    persistent grid with a bounded software barrier between levels.
 #pragma once
@@ -31,35 +36,30 @@
 namespace b40c {
 namespace dev {
 
-constexpr int kChunkMax = 2048;  // edges (EC) or items (CE/contract) per chunk, maximum
-constexpr int kMaxCtaRuns = 8;   // CTA-gathered runs per chunk (cta_thresh >= kChunkMax / 8)
+constexpr int kChunkMax = 2048;   // edges (or edge-frontier items) per sub-round
+constexpr int kChunkGrain = 256;  // CTA ranges start at multiples of this; granularity of the cf index
 
-// ------------------------------------------------------------------------------------
-// Shared-memory layout of the edge-balanced expansion (EC and 2P expand)
-// ------------------------------------------------------------------------------------
 template <int B, bool PRED>
 struct ExpandSmem {
-    int32_t colstart[kChunkMax + 1];  // column index where vertex j's in-chunk run starts
-    int32_t rel[kChunkMax + 2];       // run start relative to the chunk start (k + 1 entries)
-    uint16_t foff[kChunkMax + 1];     // first fine slot of a fine-gathered run
-    int32_t vert[PRED ? kChunkMax + 1 : 1];
-    uint16_t fmap[kChunkMax];         // fine slot -> vertex j
-    int32_t out[kChunkMax];           // discovered vertices of this chunk
-    alignas(16) int32_t stage[kChunkMax + 16];  // bulk-staged CTA runs
-    uint64_t bar;                     // mbarrier for the bulk copies
-    int32_t probe[257];               // per-level cache of P at 256 evenly spaced entries
-    int32_t warp_runs[kChunkMax / 32 + 1];
-    int32_t cta_runs[kMaxCtaRuns];
-    int32_t cta_stage_off[kMaxCtaRuns];
-    int32_t n_warp_runs, n_cta_runs, n_fine, out_count;
-    int32_t i0, k, chunk, flag;
-    int32_t q, E, level, C, nchunks;
+    // per-sub-round run tables; after the gather they hold the sub-round's
+    // output (colstart = row start, rel = degree of each discovered vertex)
+    int32_t colstart[kChunkMax + 2];
+    int32_t rel[kChunkMax + 2];
+    int32_t vert[PRED ? kChunkMax + 2 : 1];
+    uint16_t own[kChunkMax];  // position -> run j owning it
+    int32_t out[kChunkMax];   // discovered vertices of the sub-round
+    alignas(16) int32_t stage[kChunkMax + 16];  // bulk-staged run (sub-round inside one list)
+    uint64_t bar;             // mbarrier of the bulk copy
+    int32_t out_count;
+    int32_t flag;             // a vertex was labelled by this CTA in the current pass
+    int32_t q, E;
+    unsigned long long visited_edges;  // degree sum of the vertices visited up to this pass
+    int32_t prev_bu;                   // the previous level ran bottom-up
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
-    int32_t sfound;
 };
 
-// Packed (count, degree) pair helpers: count in the high 32 bits.
+// Packed (count, degree) pair: count in the high 32 bits.
 __device__ __forceinline__ unsigned long long pack(unsigned cnt, unsigned deg)
 {
     return ((unsigned long long)cnt << 32) | deg;
@@ -92,32 +92,6 @@ __device__ __forceinline__ unsigned long long cta_exclusive_scan(unsigned long l
     return wpre + incl - x;
 }
 
-// Test-and-set of v's visited bit; on discovery writes the label.
-template <bool PRED>
-__device__ __forceinline__ bool discover(const BfsParams &p, int v, int u, int new_level, bool precheck)
-{
-    uint32_t *w = p.mask + (v >> 5);
-    const uint32_t bit = 1u << (v & 31);
-    if (precheck && (ld_mask(w) & bit)) return false;
-    uint32_t old = atomicOr(w, bit);
-    if (old & bit) return false;
-    p.labels[v] = PRED ? u : new_level;
-    return true;
-}
-
-// Warp-aggregated append of `v` (when `found`) to the chunk's output list.
-__device__ __forceinline__ void push_out(bool found, int v, int32_t *out, int32_t *out_count)
-{
-    const unsigned bal = __ballot_sync(0xffffffffu, found);
-    if (bal == 0) return;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(bal) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(out_count, __popc(bal));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (found) out[base + __popc(bal & lanemask_lt())] = v;
-}
-
 // Optional warp culling: among lanes holding the same vertex only the lowest stays valid.
 __device__ __forceinline__ bool warp_cull(bool valid, int v)
 {
@@ -126,387 +100,460 @@ __device__ __forceinline__ bool warp_cull(bool valid, int v)
     return valid && (__ffs(peers) - 1 == lane);
 }
 
-// Finds i0 = the last frontier entry with P[i0] <= x (P strictly increasing,
-// P[0] = 0).  CTA-wide 256-ary search; the first round uses the per-level
-// probe cache.  All threads must call; returns the same value in all threads.
-template <int B, bool PRED>
-__device__ __forceinline__ int locate(const int32_t *P, int q, int x, ExpandSmem<B, PRED> &s)
+// Discovery of up to U gathered neighbours per thread, in overlapped phases
+// (visited-word pre-checks, then atomic test-and-sets, then the CSR rows of
+// the winners) so each thread keeps all of its memory operations in flight.
+// A winner is labelled and, when it has edges, appended to the sub-round's
+// output (s.out = vertex, s.colstart = row start, s.rel = degree; the run
+// tables are consumed by then).  All threads of the CTA call it with
+// CTA-uniform `active`.
+template <int B, bool PRED, int U>
+__device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B, PRED> &s, const int (&v)[U],
+                                               const int (&u)[U], const bool (&valid)[U], const bool (&active)[U],
+                                               int label_value)
 {
-    // probe[t] = P[min(t * stride, q)] for t in [0, 256]
-    const int stride0 = (q + 256) / 256;  // ceil((q+1)/256)
-    int lo, hi;
-    // binary-search the cached probes (257 entries, warp-uniform smem reads)
-    {
-        int a = 0, b = 256;  // probe[a] <= x (probe[0] = P[0] = 0)
-        while (a < b) {
-            int mid = (a + b + 1) >> 1;
-            if (s.probe[mid] <= x) a = mid; else b = mid - 1;
-        }
-        lo = min(a * stride0, q);
-        hi = min(lo + stride0 - 1, q);  // answer in [lo, hi]
+    bool go[U];
+    unsigned word[U];
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        go[t] = valid[t];
+        if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
+        word[t] = 0;
+        if (go[t] && p.precheck) word[t] = ld_mask(p.mask + (v[t] >> 5));
     }
-    while (hi - lo > 0) {
-        const int span = hi - lo;
-        if (span < B) {
-            int idx = lo + 1 + (int)threadIdx.x;
-            bool le = (idx <= hi) && (ld_cg(P + idx) <= x);
-            int c = __syncthreads_count(le);
-            return lo + c;
-        }
-        const int stride = (span + B - 1) / B;
-        int idx = lo + ((int)threadIdx.x + 1) * stride;
-        bool le = (idx <= hi) && (ld_cg(P + min(idx, q)) <= x);
-        int c = __syncthreads_count(le);
-        lo = lo + c * stride;
-        hi = min(lo + stride - 1, hi);
-        if (lo > hi) lo = hi;
+    bool found[U];
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        const unsigned bit = 1u << (v[t] & 31);
+        found[t] = false;
+        if (go[t] && !(word[t] & bit)) found[t] = !(atomicOr(p.mask + (v[t] >> 5), bit) & bit);
     }
-    return lo;
+    int r0[U], r1[U];
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        r0[t] = r1[t] = 0;
+        if (found[t]) {
+            p.labels[v[t]] = PRED ? u[t] : label_value;
+            r0[t] = ld_ro(p.row_offsets + v[t]);
+            r1[t] = ld_ro(p.row_offsets + v[t] + 1);
+        }
+    }
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int t = 0; t < U; t++) {
+        if (!active[t]) continue;
+        if (found[t]) s.flag = 1;  // benign race: every writer stores 1
+        const bool push = found[t] && r1[t] > r0[t];
+        const unsigned bal = __ballot_sync(0xffffffffu, push);
+        if (bal == 0) continue;
+        const int leader = __ffs(bal) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (push) {
+            const int slot = base + __popc(bal & lanemask_lt());
+            s.out[slot] = v[t];
+            s.colstart[slot] = r0[t];
+            s.rel[slot] = r1[t] - r0[t];
+        }
+    }
 }
 
-// Turns the chunk's discovered vertices (s.out[0, s.out_count)) into entries
-// of the vertex frontier `vout`: reads each one's CSR row, drops degree-0
-// vertices, allocates slots with a CTA scan plus a decoupled look-back over
-// chunk ids, and writes (v, col, P).  The last chunk publishes the totals to
-// *q_out / *e_out and closes P.  All threads must call it.
+// Turns the sub-round's output entries (s.out / s.colstart / s.rel over
+// [0, s.out_count): vertex, row start, degree > 0) into entries of the vertex
+// frontier `vout`.  A CTA scan of (count, degree) pairs gives each entry its
+// offset inside the tile; the tile's base comes from a decoupled look-back
+// over tile ids (taken once the tile's aggregate is known, so no tile ever
+// waits for another tile's gather) or, with alloc_lookback = 0, from one
+// packed 64-bit atomicAdd on the pass's output counter.  Each entry gets its
+// slot, its degree prefix P and its kChunkGrain boundaries in vout.cf.  The
+// pass total accumulates in *qe_out.  All threads must call it.
 template <int B, bool PRED>
-__device__ __forceinline__ void emit_frontier(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int phase,
-                                              const VertexFrontier &vout, int32_t *q_out, int32_t *e_out,
-                                              bool &any_discovered)
+__device__ __forceinline__ void emit_frontier(const BfsParams &p, ExpandSmem<B, PRED> &s, int pass,
+                                              const VertexFrontier &vout, unsigned long long *qe_out)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int chunk = s.chunk;
     const int cnt = s.out_count;
-    if (cnt > 0) any_discovered = true;
     constexpr int PER = kChunkMax / B;
     const int per = (cnt + B - 1) / B;
     const int jb = min(tid * per, cnt), je = min(jb + per, cnt);
-    int rv[PER], rc[PER], rd[PER];
-    unsigned my_cnt = 0, my_deg = 0;
+    unsigned my_deg = 0;
 #pragma unroll
-    for (int t = 0; t < PER; t++) {
-        rd[t] = 0;
-        rv[t] = -1;
-        rc[t] = 0;
-        if (jb + t < je) {
-            const int v = s.out[jb + t];
-            const int r0 = ld_ro(p.row_offsets + v);
-            const int r1 = ld_ro(p.row_offsets + v + 1);
-            rv[t] = v;
-            rc[t] = r0;
-            rd[t] = r1 - r0;
-            if (rd[t] > 0) {
-                my_cnt++;
-                my_deg += (unsigned)rd[t];
-            }
-        }
-    }
+    for (int t = 0; t < PER; t++)
+        if (jb + t < je) my_deg += (unsigned)s.rel[jb + t];
     unsigned long long tot;
-    const unsigned long long excl = cta_exclusive_scan<B>(pack(my_cnt, my_deg), s.scan_warp, &tot);
-    const unsigned long long epoch = p.st->epoch + 4ull * (unsigned long long)level + (unsigned)phase;
+    const unsigned long long excl = cta_exclusive_scan<B>(pack((unsigned)(je - jb), my_deg), s.scan_warp, &tot);
+    if (tot == 0) return;  // CTA-uniform: nothing to allocate
     if (warp == 0) {
         unsigned long long prefix = 0;
-        if (chunk == 0) {
-            if (lane == 0) lookback_publish(&p.slots[0], epoch, kFlagInclusive, tot);
+        if (!p.alloc_lookback) {
+            if (lane == 0) prefix = atomicAdd(qe_out, tot);
         } else {
-            if (lane == 0) lookback_publish(&p.slots[chunk], epoch, kFlagAggregate, tot);
-            prefix = lookback_exclusive(p.slots, (unsigned)chunk, epoch, &p.st->error);
-            if (lane == 0 && prefix != ~0ull) lookback_publish(&p.slots[chunk], epoch, kFlagInclusive, prefix + tot);
-        }
-        if (lane == 0) {
-            s.prefix = prefix;
-            if (prefix != ~0ull && chunk == s.nchunks - 1) {
-                const unsigned long long all = prefix + tot;
-                const int qn = (int)(all >> 32);
-                const int en = (int)(all & 0xffffffffu);
-                if (qn > p.vcap) {
-                    atomicOr(&p.st->error, kErrOverflow);
-                } else {
-                    *q_out = qn;
-                    *e_out = en;
-                    vout.P[qn] = en;
-                }
+            const unsigned long long epoch = p.st->epoch + (unsigned long long)pass;
+            int tile = 0;
+            if (lane == 0) tile = (int)atomicAdd(&p.st->tile_ctr[pass % 3], 1u);
+            tile = __shfl_sync(0xffffffffu, tile, 0);
+            if (tile >= p.max_chunks) {
+                if (lane == 0) atomicOr(&p.st->error, kErrOverflow);
+                prefix = ~0ull;
+            } else if (tile == 0) {
+                if (lane == 0) lookback_publish(&p.slots[0], epoch, kFlagInclusive, tot);
+            } else {
+                if (lane == 0) lookback_publish(&p.slots[tile], epoch, kFlagAggregate, tot);
+                prefix = lookback_exclusive(p.slots, (unsigned)tile, epoch, &p.st->error);
+                if (lane == 0 && prefix != ~0ull) lookback_publish(&p.slots[tile], epoch, kFlagInclusive, prefix + tot);
             }
+            if (lane == 0 && prefix != ~0ull) atomicAdd(qe_out, tot);  // pass totals
         }
+        if (lane == 0) s.prefix = prefix;
     }
     __syncthreads();
     const unsigned long long prefix = s.prefix;
     if (prefix == ~0ull) return;
     unsigned g = (unsigned)(prefix >> 32) + (unsigned)(excl >> 32);
     unsigned d = (unsigned)(prefix & 0xffffffffu) + (unsigned)(excl & 0xffffffffu);
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        if (rd[t] > 0) {
-            if ((int)g < p.vcap) {
-                vout.v[g] = rv[t];
-                vout.col[g] = rc[t];
-                vout.P[g] = (int)d;
-            } else {
-                atomicOr(&p.st->error, kErrOverflow);
-            }
-            g++;
-            d += (unsigned)rd[t];
+    for (int j = jb; j < je; j++) {
+        const unsigned deg = (unsigned)s.rel[j];
+        if ((int)g < p.vcap) {
+            vout.v[g] = s.out[j];
+            vout.col[g] = s.colstart[j];
+            vout.P[g] = (int)d;
+            for (unsigned c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) vout.cf[c] = (int)g;
+        } else {
+            atomicOr(&p.st->error, kErrOverflow);
         }
+        g++;
+        d += deg;
+    }
+}
+
+// The CTA's contiguous share [rs, re) of n items, with rs and re multiples of
+// kChunkGrain except re = n for the last CTA.
+__device__ __forceinline__ void cta_range(int n, int &rs, int &re)
+{
+    const long long b = blockIdx.x, G = gridDim.x;
+    rs = (int)((long long)n * b / G / kChunkGrain * kChunkGrain);
+    re = (b == G - 1) ? n : (int)((long long)n * (b + 1) / G / kChunkGrain * kChunkGrain);
+}
+
+// ------------------------------------------------------------------------------------
+// Edge-balanced expansion of the CTA's range of a vertex frontier's flattened
+// edge space, in sub-rounds of kChunkMax positions.
+//   FUSED_CULL = true  : expand-contract (EC): every gathered neighbour goes
+//                        through discovery; discoveries become the next
+//                        vertex frontier (one emit per sub-round).
+//   FUSED_CULL = false : two-phase expand: neighbours are written to the edge
+//                        frontier at their flattened edge position.
+// ------------------------------------------------------------------------------------
+template <int B, bool PRED, bool FUSED_CULL>
+__device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
+                                             int level, int pass, const VertexFrontier &vout,
+                                             const EdgeFrontier &eout, unsigned long long *qe_out,
+                                             unsigned &bar_phase)
+{
+    const int tid = threadIdx.x;
+    const int q = s.q, E = s.E;
+    constexpr int PER = kChunkMax / B;  // sub-round positions per thread
+    int rs, re;
+    cta_range(E, rs, re);
+    if (rs >= re) return;
+    int i_cur = ld_cg(in.cf + rs / kChunkGrain);  // entry owning position rs
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        const int ce = min(cs + kChunkMax, re);
+        const int len = ce - cs;
+        // ---- load the runs of entries i_cur.. that start before ce ----------------
+        if (tid == 0) s.out_count = 0;
+        int k = 0;
+        for (int base = i_cur;; base += B) {
+            const int i = base + tid;
+            bool inside = false;
+            if (i < q) {
+                const int Pi = ld_cg(in.P + i);
+                if (Pi < ce && i - i_cur <= kChunkMax) {
+                    inside = true;
+                    const int j = i - i_cur;
+                    const int start = max(Pi, cs);
+                    s.rel[j] = start - cs;
+                    s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
+                    if (PRED) s.vert[j] = ld_cg(in.v + i);
+                }
+            }
+            const int c = __syncthreads_count(inside);
+            k += c;
+            if (c < B) break;
+        }
+        if (tid == 0) s.rel[k] = len;
+        const int j_last = k - 1;  // its run may continue into the next sub-round
+
+        // ---- CTA-cooperative gather: a sub-round inside one adjacency list is
+        // staged into shared memory with one bulk copy of its aligned body ----------
+        const bool single = (k == 1) && (len >= p.cta_thresh);
+        int b0 = 0, b1 = 0;
+        if (single) {
+            const int c0 = s.colstart[0];
+            b0 = (c0 + 3) & ~3;
+            b1 = (c0 + len) & ~3;
+            if (b1 > b0) {
+                if (tid == 0) {
+                    fence_proxy_async_smem();
+                    mbar_arrive_expect_tx(&s.bar, (unsigned)(b1 - b0) * 4u);
+                    bulk_g2s(s.stage, p.column_indices + b0, (unsigned)(b1 - b0) * 4u, &s.bar);
+                }
+                unsigned spins = 0;
+                bool ok = true;
+                while (!mbar_try_wait(&s.bar, bar_phase)) {
+                    if (++spins > kSpinLimit) {
+                        atomicOr(&p.st->error, kErrBulk);
+                        ok = false;
+                        break;
+                    }
+                }
+                bar_phase ^= 1u;
+                if (!ok) b1 = b0;  // an expired wait leaves the staged words undefined: read global
+            }
+        } else {
+            // ---- owner map: thread t resolves positions [t*PER, t*PER + PER)
+            // (binary search for the first, then a walk over run starts) -----------
+            __syncthreads();
+            const int x0 = tid * PER;
+            if (x0 < len) {
+                int lo = 0, hi = k - 1;  // last j with rel[j] <= x0
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s.rel[mid] <= x0) lo = mid; else hi = mid - 1;
+                }
+                int j = lo;
+                int next = s.rel[j + 1];
+#pragma unroll
+                for (int t = 0; t < PER; t++) {
+                    const int x = x0 + t;
+                    if (x < len) {
+                        while (x >= next) {
+                            j++;
+                            next = s.rel[j + 1];
+                        }
+                        s.own[x] = (uint16_t)j;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+
+        // ---- gather: thread t takes positions t, t + B, ...: a warp reads 32
+        // consecutive positions (one coalesced segment of any run >= 32 long) ------
+        int v[PER], u[PER];
+        bool valid[PER], active[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int x = t * B + tid;
+            active[t] = t * B < len;  // CTA-uniform
+            valid[t] = x < len;
+            v[t] = -1;
+            u[t] = -1;
+            if (valid[t]) {
+                const int j = single ? 0 : s.own[x];
+                const int c = s.colstart[j] + (x - s.rel[j]);
+                v[t] = (c >= b0 && c < b1) ? s.stage[c - b0] : ld_stream(p.column_indices + c);
+                if (PRED) u[t] = s.vert[j];
+            }
+        }
+        i_cur += j_last;
+        if (!FUSED_CULL) {
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                if (valid[t]) {
+                    eout.v[cs + t * B + tid] = v[t];
+                    if (PRED) eout.pred[cs + t * B + tid] = u[t];
+                }
+            }
+            __syncthreads();  // run tables and stage free for the next sub-round
+            continue;
+        }
+        __syncthreads();  // run tables consumed: they now collect the sub-round's output
+        discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level + 1);
+        __syncthreads();
+        emit_frontier<B, PRED>(p, s, pass, vout, qe_out);
+        __syncthreads();
+    }
+}
+
+// Contraction of the CTA's range of an edge frontier (q items), in sub-rounds
+// of kChunkMax items: each item's visited bit is test-and-set; a first visit
+// labels the vertex with the current level (or its predecessor) and the
+// vertices with edges become the vertex frontier vf[0].
+template <int B, bool PRED>
+__device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B, PRED> &s, const EdgeFrontier &in,
+                                               int level, int pass, unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x;
+    const int q = s.q;
+    constexpr int PER = kChunkMax / B;
+    int rs, re;
+    cta_range(q, rs, re);
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        const int ce = min(cs + kChunkMax, re);
+        if (tid == 0) s.out_count = 0;
+        int v[PER], u[PER];
+        bool valid[PER], active[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int i = cs + t * B + tid;
+            active[t] = cs + t * B < ce;
+            valid[t] = i < ce;
+            v[t] = valid[t] ? ld_cg(in.v + i) : -1;
+            u[t] = (PRED && valid[t]) ? ld_cg(in.pred + i) : -1;
+        }
+        __syncthreads();
+        discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level);
+        __syncthreads();
+        emit_frontier<B, PRED>(p, s, pass, p.vf[0], qe_out);
+        __syncthreads();
     }
 }
 
 // ------------------------------------------------------------------------------------
-// Edge-balanced expansion of one chunk of a vertex frontier.
-//   FUSED_CULL = true  : expand-contract (EC): every gathered neighbour goes
-//                        through discover(); discoveries become the next
-//                        vertex frontier (look-back allocated).
-//   FUSED_CULL = false : two-phase expand: neighbours are written to the edge
-//                        frontier at their flattened edge position (no allocation).
+// Bottom-up step (direction-optimizing levels, undirected graphs only)
 // ------------------------------------------------------------------------------------
-template <int B, bool PRED, bool FUSED_CULL>
-__device__ __forceinline__ void expand_chunk(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
-                                             int level, const VertexFrontier &vout, const EdgeFrontier &eout,
-                                             unsigned &bar_phase, bool &any_discovered)
+constexpr int kBottomUpLongList = 256;  // lists longer than this are searched warp-cooperatively
+
+// Level `level` run bottom-up over the CTA's share of vertex ids: every
+// unvisited vertex with edges looks for a neighbour whose visited bit is set
+// in the snapshot taken at the start of the level; on an undirected graph
+// such a neighbour is exactly one level up, so the vertex is labelled
+// level + 1 (or that neighbour, the first one in CSR order).  Discoveries go
+// to next_mask (merged into the visited mask after the level, keeping the
+// snapshot intact) and, through emit_frontier, into the next vertex frontier.
+// A warp handles 32 consecutive vertices (one visited-mask word): each lane
+// scans its short list four neighbours at a time; long lists are then
+// searched by the whole warp, 32 neighbours at a time.
+template <int B, bool PRED>
+__device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
+                                                const VertexFrontier &vout, unsigned long long *qe_out)
 {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    constexpr int NW = B / 32;
-    const int q = s.q, E = s.E, C = s.C, chunk = s.chunk;
-    const int cs = chunk * C;
-    const int ce = min(cs + C, E);
-    const int new_level = level + 1;
-
-    // ---- locate the chunk's vertices and load their runs ---------------------------
-    const int i0 = locate<B, PRED>(in.P, q, cs, s);
-    if (tid == 0) {
-        s.n_warp_runs = 0;
-        s.n_cta_runs = 0;
-        s.out_count = 0;
-    }
-    // load tiles of entries from i0 until P >= ce
-    int k = 0;
-    for (int base = i0;; base += B) {
-        const int i = base + tid;
-        bool inside = false;
-        if (i < q) {
-            const int Pi = ld_cg(in.P + i);
-            if (Pi < ce && i - i0 < kChunkMax) {
-                inside = true;
-                const int j = i - i0;
-                const int start = max(Pi, cs);
-                s.rel[j] = start - cs;
-                s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
-                if (PRED) s.vert[j] = ld_cg(in.v + i);
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr int PER = kChunkMax / B;
+    int rs, re;
+    cta_range(p.nodes, rs, re);
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        if (tid == 0) s.out_count = 0;
+        __syncthreads();
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * B + (tid & ~31);  // multiple of 32: one mask word per warp
+            if (vb >= re) break;                      // warp-uniform
+            const int v = vb + lane;
+            const unsigned vis = ld_cg(p.mask + (vb >> 5));
+            bool todo = v < re && !((vis >> lane) & 1u);
+            int r0 = 0, r1 = 0;
+            if (todo) {
+                r0 = ld_ro(p.row_offsets + v);
+                r1 = ld_ro(p.row_offsets + v + 1);
+                todo = r1 > r0;
             }
-        }
-        const int c = __syncthreads_count(inside);
-        k += c;
-        if (c < B) break;
-    }
-    if (tid == 0) {
-        s.rel[k] = ce - cs;
-        s.k = k;
-    }
-    __syncthreads();
-
-    // ---- classify runs ---------------------------------------------------------------
-    // thread-per-vertex; fine runs get disjoint slot ranges (warp scan + one
-    // shared atomic per warp), warp and CTA runs are listed
-    if (tid == 0) s.n_fine = 0;
-    __syncthreads();
-    for (int jb = 0; jb < k; jb += B) {
-        const int j = jb + tid;
-        int r = 0;
-        bool fine = false;
-        if (j < k) {
-            r = s.rel[j + 1] - s.rel[j];
-            if (r >= p.cta_thresh) {
-                const int slot = atomicAdd(&s.n_cta_runs, 1);
-                if (slot < kMaxCtaRuns) s.cta_runs[slot] = j;
-            } else if (r >= p.warp_thresh) {
-                s.warp_runs[atomicAdd(&s.n_warp_runs, 1)] = j;
-            } else {
-                fine = true;
-            }
-        }
-        int len = fine ? r : 0;
-        int incl = len;
+            if (!__any_sync(0xffffffffu, todo)) continue;
+            const bool longlist = todo && (r1 - r0) > kBottomUpLongList;
+            bool scan = todo && !longlist;
+            int parent = -1;
+            int e = r0;
+            while (__any_sync(0xffffffffu, scan)) {
+                if (scan) {
+                    int nb[4];
+                    unsigned w[4];
 #pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            int y = __shfl_up_sync(0xffffffffu, incl, off);
-            if (lane >= off) incl += y;
-        }
-        int wbase = 0;
-        if (lane == 31 && incl > 0) wbase = atomicAdd(&s.n_fine, incl);
-        wbase = __shfl_sync(0xffffffffu, wbase, 31);
-        if (fine) {
-            const int off = wbase + incl - len;
-            s.foff[j] = (uint16_t)off;
-            for (int x = 0; x < len; x++) s.fmap[off + x] = (uint16_t)j;
-        }
-    }
-    __syncthreads();
-
-    // ---- CTA runs: stage the aligned body of each with one bulk copy -------------------
-    const int n_cta = min(s.n_cta_runs, kMaxCtaRuns);
-    bool bulk_issued = false;
-    if (n_cta > 0) {
-        if (tid == 0) {
-            unsigned total_bytes = 0;
-            int soff = 0;
-            for (int r = 0; r < n_cta; r++) {
-                const int j = s.cta_runs[r];
-                const int c0 = s.colstart[j], len = s.rel[j + 1] - s.rel[j];
-                const int b0 = (c0 + 3) & ~3, b1 = (c0 + len) & ~3;
-                s.cta_stage_off[r] = soff;
-                if (b1 > b0) {
-                    total_bytes += (unsigned)(b1 - b0) * 4u;
-                    soff += b1 - b0;
+                    for (int k = 0; k < 4; k++) nb[k] = (e + k < r1) ? ld_stream(p.column_indices + e + k) : -1;
+#pragma unroll
+                    for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(p.mask + (nb[k] >> 5)) : 0u;
+#pragma unroll
+                    for (int k = 0; k < 4; k++)
+                        if (parent < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent = nb[k];
+                    e += 4;
+                    if (parent >= 0 || e >= r1) scan = false;
                 }
             }
-            if (total_bytes > 0) {
-                fence_proxy_async_smem();
-                mbar_arrive_expect_tx(&s.bar, total_bytes);
-                for (int r = 0; r < n_cta; r++) {
-                    const int j = s.cta_runs[r];
-                    const int c0 = s.colstart[j], len = s.rel[j + 1] - s.rel[j];
-                    const int b0 = (c0 + 3) & ~3, b1 = (c0 + len) & ~3;
-                    if (b1 > b0)
-                        bulk_g2s(&s.stage[s.cta_stage_off[r]], p.column_indices + b0, (unsigned)(b1 - b0) * 4u, &s.bar);
+            unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+            while (lmask) {
+                const int owner = __ffs(lmask) - 1;
+                lmask &= lmask - 1;
+                const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
+                int found_u = -1;
+                for (int eb = lr0; eb < lr1; eb += 32) {
+                    const int ee = eb + lane;
+                    const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
+                    const bool hit = nb >= 0 && ((ld_mask(p.mask + (nb >> 5)) >> (nb & 31)) & 1u);
+                    const unsigned hb = __ballot_sync(0xffffffffu, hit);
+                    if (hb) {
+                        found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
+                        break;
+                    }
                 }
+                if (lane == owner) parent = found_u;
+            }
+            const bool found = parent >= 0;
+            const unsigned fb = __ballot_sync(0xffffffffu, found);
+            if (fb == 0) continue;
+            if (lane == 0) p.next_mask[vb >> 5] = fb;  // this warp owns the whole word
+            if (found) {
+                p.labels[v] = PRED ? parent : level + 1;
                 s.flag = 1;
-            } else {
-                s.flag = 0;
+            }
+            const int leader = __ffs(fb) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&s.out_count, __popc(fb));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (found) {
+                const int slot = base + __popc(fb & lanemask_lt());
+                s.out[slot] = v;
+                s.colstart[slot] = r0;
+                s.rel[slot] = r1 - r0;
             }
         }
         __syncthreads();
-        bulk_issued = s.flag != 0;
+        emit_frontier<B, PRED>(p, s, pass, vout, qe_out);
+        __syncthreads();
     }
+}
 
-    // visit one gathered neighbour (all lanes of the warp call it together)
-    auto visit = [&](bool valid, int v, int u, int epos) {
-        if (FUSED_CULL) {
-            if (p.warp_cull) valid = warp_cull(valid, v);
-            bool found = valid && discover<PRED>(p, v, u, new_level, p.precheck);
-            push_out(found, v, s.out, &s.out_count);
-        } else {
-            if (valid) {
-                eout.v[epos] = v;
-                if (PRED) eout.pred[epos] = u;
-            }
-        }
-    };
-
-    // ---- fine-grained gather (scan-based) ---------------------------------------------
-    {
-        const int F = s.n_fine;
-        constexpr int U = 4;
-        for (int base = 0; base < F; base += B * U) {
-            int v[U], u[U], epos[U];
-            bool valid[U];
-#pragma unroll
-            for (int t = 0; t < U; t++) {
-                const int slot = base + t * B + tid;
-                valid[t] = slot < F;
-                v[t] = -1;
-                u[t] = -1;
-                epos[t] = 0;
-                if (valid[t]) {
-                    const int j = s.fmap[slot];
-                    const int x = slot - (int)s.foff[j];
-                    v[t] = ld_stream(p.column_indices + s.colstart[j] + x);
-                    if (PRED) u[t] = s.vert[j];
-                    epos[t] = cs + s.rel[j] + x;
-                }
-            }
-#pragma unroll
-            for (int t = 0; t < U; t++) visit(valid[t], v[t], u[t], epos[t]);
+// Folds the bottom-up discoveries of the last level into the visited mask
+// and clears next_mask (the CTA's share of words).
+__device__ __forceinline__ void merge_next_mask(const BfsParams &p)
+{
+    const int stride = gridDim.x * blockDim.x;
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < p.mask_words; w += stride) {
+        const unsigned m = ld_cg(p.next_mask + w);
+        if (m) {
+            p.mask[w] |= m;
+            p.next_mask[w] = 0;
         }
     }
+}
 
-    // ---- warp-cooperative gather -------------------------------------------------------
-    {
-        const int nwr = s.n_warp_runs;
-        for (int r = warp; r < nwr; r += NW) {
-            const int j = s.warp_runs[r];
-            const int c0 = s.colstart[j], len = s.rel[j + 1] - s.rel[j];
-            const int u = PRED ? s.vert[j] : -1;
-            const int eb = cs + s.rel[j];
-            constexpr int U = 4;
-            for (int x0 = 0; x0 < len; x0 += 32 * U) {
-                int v[U];
-                bool valid[U];
-#pragma unroll
-                for (int t = 0; t < U; t++) {
-                    const int x = x0 + t * 32 + lane;
-                    valid[t] = x < len;
-                    v[t] = valid[t] ? ld_stream(p.column_indices + c0 + x) : -1;
-                }
-#pragma unroll
-                for (int t = 0; t < U; t++) visit(valid[t], v[t], u, eb + x0 + t * 32 + lane);
-            }
-        }
-    }
-
-    // ---- CTA-cooperative gather from the staged runs -----------------------------------
-    if (n_cta > 0) {
-        bool staged_ok = true;
-        if (bulk_issued) {
-            unsigned spins = 0;
-            while (!mbar_try_wait(&s.bar, bar_phase)) {
-                if (++spins > kSpinLimit) {
-                    atomicOr(&p.st->error, kErrBulk);
-                    staged_ok = false;
-                    break;
-                }
-            }
-            bar_phase ^= 1u;
-        }
-        // an expired wait leaves the staged words undefined: gather nothing from them
-        for (int r = 0; r < (staged_ok ? n_cta : 0); r++) {
-            const int j = s.cta_runs[r];
-            const int c0 = s.colstart[j], len = s.rel[j + 1] - s.rel[j];
-            const int b0 = (c0 + 3) & ~3, b1 = (c0 + len) & ~3;
-            const int soff = s.cta_stage_off[r];
-            const int u = PRED ? s.vert[j] : -1;
-            const int eb = cs + s.rel[j];
-            constexpr int U = 4;
-            for (int x0 = 0; x0 < len; x0 += B * U) {
-                int v[U];
-                bool valid[U];
-#pragma unroll
-                for (int t = 0; t < U; t++) {
-                    const int x = x0 + t * B + tid;
-                    valid[t] = x < len;
-                    v[t] = -1;
-                    if (valid[t]) {
-                        const int c = c0 + x;
-                        v[t] = (c >= b0 && c < b1) ? s.stage[soff + (c - b0)] : ld_stream(p.column_indices + c);
-                    }
-                }
-#pragma unroll
-                for (int t = 0; t < U; t++) visit(valid[t], v[t], u, eb + x0 + t * B + tid);
-            }
-        }
-    }
-    __syncthreads();  // out[] complete; stage and lists free for the next chunk
-
-    if (!FUSED_CULL) return;
-
-    emit_frontier<B, PRED>(p, s, level, 0, vout, &p.st->q_len[(level + 1) & 1], &p.st->e_len[(level + 1) & 1],
-                           any_discovered);
+// Direction of a level from the frontier's size (Beamer, Asanovic and
+// Patterson, SC'12 heuristic): top-down -> bottom-up when the frontier's
+// edges exceed the unvisited edges / alpha, bottom-up -> top-down when the
+// frontier falls under n / beta vertices.
+__device__ __forceinline__ bool choose_bottom_up(const BfsParams &p, bool was_bottom_up, int q, int E,
+                                                 unsigned long long visited_edges)
+{
+    if (!p.direction_opt) return false;
+    const long long unvisited_edges = (long long)p.edges - (long long)visited_edges;
+    if (!was_bottom_up) return (long long)E * p.bu_alpha > unvisited_edges;
+    return (long long)q * p.bu_beta >= (long long)p.nodes;
 }
 
 // ------------------------------------------------------------------------------------
 // Level drivers
 // ------------------------------------------------------------------------------------
 
-// Chunk size for a level: enough chunks for every CTA, at most kChunkMax
-__device__ __forceinline__ int level_chunk(int E, int c_max)
+__device__ __forceinline__ unsigned long long ld_cg64(const unsigned long long *p)
 {
-    int c = (E + (int)gridDim.x - 1) / (int)gridDim.x;
-    c = (c + 31) & ~31;
-    c = max(c, 256);
-    return min(c, c_max);
+    unsigned long long v;
+    asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
+    return v;
 }
 
-// Shared epilogue of a non-persistent launch: the last CTA to finish
-// advances the level and decides whether the search continues.
-__device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int q_next, bool limit_hit)
+// Epilogue of a non-persistent launch that completed a level: the last CTA
+// to finish advances the level and decides whether the search continues
+// (and, inside a captured graph, sets the WHILE node's condition).
+__device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int next_pass, bool limit_hit)
 {
     if (threadIdx.x != 0) return;
     __threadfence();
@@ -515,15 +562,35 @@ __device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int
         __threadfence();
         p.st->finished = 0;
         p.st->cur_level = level + 1;
-        const int qn = ld_cg(&p.st->q_len[(level + 1) & 1]);
+        const int qn = qe_count(ld_cg64(&p.st->qe[next_pass % 3]));
         const bool done = (qn == 0) || limit_hit || (ld_cg(&p.st->error) != 0);
         if (done) p.st->done = 1;
         if (p.cond_handle) cudaGraphSetConditional((cudaGraphConditionalHandle)p.cond_handle, done ? 0u : 1u);
     }
-    (void)q_next;
 }
 
-// Expand-contract (vertex frontier): one level per iteration of the loop.
+// Start of pass `pass`: loads its input size into shared memory and lets
+// block 0 clear the counters two passes ahead.
+template <int B, bool PRED>
+__device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRED> &s, int pass, bool count_queue)
+{
+    if (threadIdx.x == 0) {
+        const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
+        s.q = qe_count(x);
+        s.E = qe_edges(x);
+        s.flag = 0;
+        if (blockIdx.x == 0) {
+            p.st->qe[(pass + 2) % 3] = 0;
+            p.st->tile_ctr[(pass + 1) % 3] = 0;
+            if (count_queue) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
+        }
+        s.visited_edges = ld_cg64(&p.st->visited_edges[pass % 3]) + (unsigned long long)s.E;
+        s.prev_bu = ld_cg(&p.st->dir[pass % 3]);
+    }
+    __syncthreads();
+}
+
+// Expand-contract (vertex frontiers): one level per pass.
 template <int B, bool PRED>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
@@ -533,53 +600,39 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     const int tid = threadIdx.x;
     if (tid == 0) mbar_init(&s.bar, 1);
     unsigned bar_phase = 0, generation = 0;
-    bool any = false;
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
-    bool limit_hit = false;
+    bool limit_hit = false, worked = false;
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
-        if (tid == 0) {
-            s.q = ld_cg(&p.st->q_len[level & 1]);
-            s.E = ld_cg(&p.st->e_len[level & 1]);
-            s.level = level;
-            if (blockIdx.x == 0) p.st->chunk_ctr[(level + 1) % 3] = 0;
-        }
-        __syncthreads();
-        const int q = s.q, E = s.E;
+        const int pass = level;
+        begin_pass<B, PRED>(p, s, pass, true);
+        if (s.q == 0 || ld_cg(&p.st->error) != 0) break;
         const int dl = p.st->depth_limit;
-        if (q == 0 || ld_cg(&p.st->error) != 0) break;
         if (dl >= 0 && level >= dl) {
             limit_hit = true;
-            if (tid == 0 && blockIdx.x == 0) p.st->q_len[(level + 1) & 1] = 0;
             break;
         }
-        const VertexFrontier in = p.vf[level & 1];
-        const VertexFrontier out = p.vf[(level + 1) & 1];
-        // per-level probe cache of P
-        {
-            const int stride0 = (q + 256) / 256;
-            for (int t = tid; t <= 256; t += B) s.probe[t] = ld_cg(in.P + min(t * stride0, q));
+        const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
+        if (tid == 0 && blockIdx.x == 0) {
+            p.st->visited_edges[(pass + 1) % 3] = s.visited_edges;
+            p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
+            if (bu) p.st->merge_pending = 1;
         }
-        if (tid == 0) {
-            s.C = level_chunk(E, p.chunk_edges);
-            s.nchunks = (E + s.C - 1) / s.C;
-            if (s.nchunks > p.max_chunks) {
-                atomicOr(&p.st->error, kErrOverflow);
-                s.nchunks = 0;
-            }
-            if (blockIdx.x == 0) atomicAdd(&p.st->total_queued, (unsigned long long)q);
-        }
+        if (bu)
+            bottom_up_range<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        else
+            expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
+                                        &p.st->qe[(pass + 1) % 3], bar_phase);
         __syncthreads();
-        any = false;
-        while (true) {
-            if (tid == 0) s.chunk = (int)atomicAdd(&p.st->chunk_ctr[level % 3], 1u);
-            __syncthreads();
-            if (s.chunk >= s.nchunks) break;
-            expand_chunk<B, PRED, true>(p, in, s, level, out, p.ef[0], bar_phase, any);
-            __syncthreads();
+        if (bu && p.persistent) {
+            // fold the level's discoveries into the visited mask before the next level
+            if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+            merge_next_mask(p);
+            if (tid == 0 && blockIdx.x == 0) p.st->merge_pending = 0;
         }
-        if (any) max_level_seen = level + 1;
+        worked = true;
+        if (s.flag) max_level_seen = level + 1;
         if (!p.persistent) break;
         if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
         if ((int)blockIdx.x == p.skip_arrival_cta) {
@@ -594,56 +647,16 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             p.st->cur_level = level;
             p.st->done = 1;
         }
-    } else {
-        finish_launch(p, level, 0, limit_hit);
+    } else if (worked || limit_hit) {
+        finish_launch(p, level, level + 1, limit_hit);
     }
 }
 
-
-// ------------------------------------------------------------------------------------
-// Edge-frontier strategies (contract-expand, two-phase, hybrid)
-// ------------------------------------------------------------------------------------
-
-// Contraction of one chunk of an edge frontier: each item's visited bit is
-// test-and-set; a first visit labels the vertex with the current level (or
-// its predecessor) and the survivors become the vertex frontier vf[0].
-template <int B, bool PRED>
-__device__ __forceinline__ void contract_chunk(const BfsParams &p, ExpandSmem<B, PRED> &s, const EdgeFrontier &in,
-                                               int level, bool &any_discovered)
-{
-    const int tid = threadIdx.x;
-    const int C = s.C, chunk = s.chunk, q = s.q;
-    const int cs = chunk * C, ce = min(cs + C, q);
-    if (tid == 0) s.out_count = 0;
-    __syncthreads();
-    constexpr int U = 4;
-    for (int base = cs; base < ce; base += B * U) {
-        int v[U], u[U];
-        bool valid[U];
-#pragma unroll
-        for (int t = 0; t < U; t++) {
-            const int i = base + t * B + tid;
-            valid[t] = i < ce;
-            v[t] = valid[t] ? ld_cg(in.v + i) : -1;
-            u[t] = (PRED && valid[t]) ? ld_cg(in.pred + i) : -1;
-        }
-#pragma unroll
-        for (int t = 0; t < U; t++) {
-            bool ok = valid[t];
-            if (p.warp_cull) ok = warp_cull(ok, v[t]);
-            const bool found = ok && discover<PRED>(p, v[t], u[t], level, p.precheck);
-            push_out(found, v[t], s.out, &s.out_count);
-        }
-    }
-    __syncthreads();
-    emit_frontier<B, PRED>(p, s, level, 1, p.vf[0], &p.st->vq_len, &p.st->ve_len, any_discovered);
-}
-
-// Per level: contract the edge frontier into vf[0], then expand vf[0] into
-// the next edge frontier (flattened edge positions, no allocation needed).
-// phase_mask selects the phases of a non-persistent launch; a persistent
-// launch runs both with a grid barrier after each.  With `hybrid`, a
-// persistent launch returns when the edge frontier exceeds
+// Edge strategies: per level, contract the edge frontier into vf[0] (pass
+// 2L), then expand vf[0] into the next edge frontier at flattened edge
+// positions (pass 2L+1).  phase_mask selects the phases of a non-persistent
+// launch; a persistent launch runs both with a grid barrier after each.
+// With `hybrid`, a persistent launch returns when the edge frontier exceeds
 // gridDim * saturation items (SATURATION_QUIT, enactor_hybrid.cuh:571).
 template <int B, bool PRED>
 __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
@@ -656,110 +669,51 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
     unsigned bar_phase = 0, generation = 0;
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
-    bool limit_hit = false, saturated = false, completed_level = false, failed = false;
+    bool limit_hit = false, saturated = false, completed_level = false;
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
         const int in_idx = p.edge_pingpong ? (level & 1) : 0;
         const int out_idx = p.edge_pingpong ? ((level + 1) & 1) : 0;
         if (p.phase_mask & 1) {
             const int pass = 2 * level;
-            if (tid == 0) {
-                s.q = ld_cg(&p.st->q_len[level & 1]);
-                if (blockIdx.x == 0) p.st->chunk_ctr[(pass + 1) % 3] = 0;
-            }
-            __syncthreads();
-            const int q = s.q;
-            if (ld_cg(&p.st->error) != 0) {
-                failed = true;
-                break;
-            }
-            if (q == 0) {
-                if (tid == 0 && blockIdx.x == 0) p.st->vq_len = p.st->ve_len = 0;
-                break;
-            }
-            if (p.hybrid && p.persistent && q > (int)gridDim.x * p.saturation) {
+            begin_pass<B, PRED>(p, s, pass, true);
+            if (ld_cg(&p.st->error) != 0 || s.q == 0) break;
+            if (p.hybrid && p.persistent && s.q > (int)gridDim.x * p.saturation) {
                 saturated = true;
                 break;
             }
-            if (tid == 0) {
-                s.C = level_chunk(q, p.chunk_edges);
-                s.nchunks = (q + s.C - 1) / s.C;
-                if (s.nchunks > p.max_chunks) {
-                    atomicOr(&p.st->error, kErrOverflow);
-                    s.nchunks = 0;
-                }
-                if (blockIdx.x == 0) atomicAdd(&p.st->total_queued, (unsigned long long)q);
-            }
+            contract_range<B, PRED>(p, s, p.ef[in_idx], level, pass, &p.st->qe[(pass + 1) % 3]);
             __syncthreads();
-            bool any = false;
-            while (true) {
-                if (tid == 0) s.chunk = (int)atomicAdd(&p.st->chunk_ctr[pass % 3], 1u);
-                __syncthreads();
-                if (s.chunk >= s.nchunks) break;
-                contract_chunk<B, PRED>(p, s, p.ef[in_idx], level, any);
-                __syncthreads();
-            }
-            if (any) max_level_seen = max(max_level_seen, level);
+            if (s.flag) max_level_seen = max(max_level_seen, level);
             if (p.persistent) {
                 if ((int)blockIdx.x == p.skip_arrival_cta) {
                     if (tid == 0) atomicOr(&p.st->error, kErrInjected);
                     return;
                 }
-                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) {
-                    failed = true;
-                    break;
-                }
+                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
             }
         }
         const int dl = p.st->depth_limit;
         if (dl >= 0 && level >= dl) {
             limit_hit = true;
-            if (tid == 0 && blockIdx.x == 0) p.st->q_len[(level + 1) & 1] = 0;
             break;
         }
         if (p.phase_mask & 2) {
             const int pass = 2 * level + 1;
-            if (tid == 0) {
-                s.q = ld_cg(&p.st->vq_len);
-                s.E = ld_cg(&p.st->ve_len);
-                if (blockIdx.x == 0) p.st->chunk_ctr[(pass + 1) % 3] = 0;
-            }
-            __syncthreads();
+            begin_pass<B, PRED>(p, s, pass, false);
             const int q = s.q, E = s.E;
             if (E > p.ecap) {
                 if (tid == 0) atomicOr(&p.st->error, kErrOverflow);
-                failed = true;
                 break;
             }
-            if (tid == 0 && blockIdx.x == 0) p.st->q_len[(level + 1) & 1] = q == 0 ? 0 : E;
-            if (q > 0) {
-                const int stride0 = (q + 256) / 256;
-                for (int t = tid; t <= 256; t += B) s.probe[t] = ld_cg(p.vf[0].P + min(t * stride0, q));
-                if (tid == 0) {
-                    s.C = level_chunk(E, p.chunk_edges);
-                    s.nchunks = (E + s.C - 1) / s.C;
-                    if (s.nchunks > p.max_chunks) {
-                        atomicOr(&p.st->error, kErrOverflow);
-                        s.nchunks = 0;
-                    }
-                }
-                __syncthreads();
-                bool unused = false;
-                while (true) {
-                    if (tid == 0) s.chunk = (int)atomicAdd(&p.st->chunk_ctr[pass % 3], 1u);
-                    __syncthreads();
-                    if (s.chunk >= s.nchunks) break;
-                    expand_chunk<B, PRED, false>(p, p.vf[0], s, level, p.vf[1], p.ef[out_idx], bar_phase, unused);
-                    __syncthreads();
-                }
-            }
+            if (tid == 0 && blockIdx.x == 0) p.st->qe[(pass + 1) % 3] = pack((unsigned)(q == 0 ? 0 : E), 0u);
+            if (q > 0)
+                expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr, bar_phase);
+            __syncthreads();
             completed_level = true;
             if (p.persistent) {
                 if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
-                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) {
-                    failed = true;
-                    break;
-                }
+                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
             }
         }
         if (!p.persistent) break;
@@ -774,9 +728,26 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
                 p.st->done = 1;
         }
     } else if (completed_level || limit_hit) {
-        finish_launch(p, level, 0, limit_hit);
+        finish_launch(p, level, 2 * (level + 1), limit_hit);
     }
-    (void)failed;
+}
+
+// Non-persistent launches: folds a bottom-up level's discoveries into the
+// visited mask before the next level's launch.
+template <bool PRED>
+__global__ void merge_kernel(BfsParams p)
+{
+    if (ld_cg(&p.st->merge_pending) == 0) return;
+    merge_next_mask(p);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned t = atomicAdd(&p.st->finished, 1u);
+        if (t == gridDim.x - 1) {
+            p.st->finished = 0;
+            p.st->merge_pending = 0;
+        }
+    }
 }
 
 // Sets up a search: the source's label, visited bit and the level-0
@@ -794,8 +765,10 @@ __global__ void init_kernel(BfsParams p)
     const int src_label = PRED ? -2 : 0;
     if (FULL) {
         for (long long i = t0; i < p.nodes; i += stride) p.labels[i] = (VERTEX_FRONTIER && i == src) ? src_label : -1;
-        for (long long w = t0; w < p.mask_words; w += stride)
+        for (long long w = t0; w < p.mask_words; w += stride) {
             p.mask[w] = (VERTEX_FRONTIER && w == (src >> 5)) ? (1u << (src & 31)) : 0u;
+            if (p.next_mask) p.next_mask[w] = 0u;
+        }
     } else if (VERTEX_FRONTIER && t0 == 0) {
         p.labels[src] = src_label;
         p.mask[src >> 5] = 1u << (src & 31);
@@ -803,7 +776,7 @@ __global__ void init_kernel(BfsParams p)
     if (t0 == 0) {
         SearchState *st = p.st;
         const int r0 = p.row_offsets[src], r1 = p.row_offsets[src + 1];
-        st->chunk_ctr[0] = st->chunk_ctr[1] = st->chunk_ctr[2] = 0;
+        st->tile_ctr[0] = st->tile_ctr[1] = st->tile_ctr[2] = 0;
         st->cur_level = 0;
         st->epoch += 1ull << 24;
         st->barrier = 0;
@@ -813,19 +786,20 @@ __global__ void init_kernel(BfsParams p)
         st->saturated = 0;
         st->total_queued = 0;
         st->finished = 0;
-        st->q_len[1] = st->e_len[1] = 0;
+        st->qe[1] = st->qe[2] = 0;
+        st->dir[0] = st->dir[1] = st->dir[2] = 0;
+        st->merge_pending = 0;
+        st->visited_edges[0] = st->visited_edges[1] = st->visited_edges[2] = 0;
         if (VERTEX_FRONTIER) {
             const int deg = r1 - r0;
-            st->q_len[0] = deg > 0 ? 1 : 0;
-            st->e_len[0] = deg;
+            st->qe[0] = deg > 0 ? pack(1u, (unsigned)deg) : 0ull;
             p.vf[0].v[0] = src;
             p.vf[0].col[0] = r0;
             p.vf[0].P[0] = 0;
-            p.vf[0].P[1] = deg;
+            for (int c = 0; c * kChunkGrain < deg; c++) p.vf[0].cf[c] = 0;
         } else {
             // edge frontier: the source is the only item; its predecessor is -2
-            st->q_len[0] = 1;
-            st->e_len[0] = 0;
+            st->qe[0] = pack(1u, 0u);
             p.ef[0].v[0] = src;
             if (PRED) p.ef[0].pred[0] = -2;
         }

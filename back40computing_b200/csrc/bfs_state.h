@@ -19,6 +19,7 @@ struct VertexFrontier {
     int32_t *v;
     int32_t *col;
     int32_t *P;
+    int32_t *cf;  // chunk-first index: cf[c] = entry owning edge c * kChunkGrain of the flattened edge space
 };
 
 // One edge frontier: neighbour ids (and their predecessors when marking
@@ -31,9 +32,12 @@ struct EdgeFrontier {
 // Rotating/ping-pong counters written by the kernels (the role of the
 // reference's CtaWorkProgress, util/cta_work_progress.cuh:69-223).
 struct alignas(128) SearchState {
-    int32_t q_len[2];          // frontier lengths, indexed by level parity
-    int32_t e_len[2];          // edge totals of vertex frontiers, by level parity
-    uint32_t chunk_ctr[3];     // dynamic chunk counters, by level % 3
+    // Frontier sizes, rotating over passes (a pass is one level of
+    // expand-contract, or one phase of a level of the edge strategies):
+    // pass k reads qe[k % 3] and accumulates its output frontier into
+    // qe[(k + 1) % 3]; each value packs (count << 32 | edge total).
+    unsigned long long qe[3];
+    uint32_t tile_ctr[3];      // look-back tile counters, by pass % 3
     int32_t cur_level;         // next level to process
     unsigned long long epoch;  // look-back epoch base for this search
     unsigned long long barrier;  // grid-barrier arrivals of the current persistent launch
@@ -45,10 +49,19 @@ struct alignas(128) SearchState {
     uint32_t finished;         // CTAs that finished the current non-persistent launch
     int32_t src;               // source vertex (read by the init kernel)
     int32_t depth_limit;       // < 0: unlimited
-    int32_t vq_len;            // edge strategies: contracted vertex frontier length
-    int32_t ve_len;            // edge strategies: its edge total
-    int32_t pad[3];
+    int32_t merge_pending;     // a bottom-up level left discoveries in the next-mask
+    // direction-optimizing bookkeeping, rotating like qe: pass k reads [k % 3]
+    // and block 0 writes [(k + 1) % 3]
+    int32_t dir[3];            // 1: the previous level ran bottom-up
+    unsigned long long visited_edges[3];  // degree sum of the vertices visited before the pass
 };
+
+__host__ __device__ inline int qe_count(unsigned long long x) { return (int)(x >> 32); }
+__host__ __device__ inline int qe_edges(unsigned long long x) { return (int)(x & 0xffffffffull); }
+__host__ __device__ inline int pass_of(int level, int phase, bool edge_strategy)
+{
+    return edge_strategy ? 2 * level + phase : level;
+}
 
 // Kernel parameter block.
 struct BfsParams {
@@ -78,7 +91,12 @@ struct BfsParams {
     int32_t edge_pingpong;    // edge strategies: 1 = two edge frontiers (EDGE_FRONTIERS), 0 = one (MIXED)
     int32_t phase_mask;       // edge kernel: 1 = contract, 2 = expand, 3 = both per level (persistent)
     int32_t hybrid;           // edge kernel: leave the persistent loop when the frontier saturates
-    int32_t pad1;
+    int32_t alloc_lookback;   // 1: frontier slots by decoupled look-back, 0: one atomic per tile
+    int32_t direction_opt;    // 1: levels may run bottom-up (symmetric graphs only)
+    int32_t bu_alpha;         // switch to bottom-up when frontier edges > unvisited edges / alpha
+    int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
+    int32_t pad2;
+    uint32_t *next_mask;      // bottom-up discoveries of the current level (merged into mask after it)
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
 };
 

@@ -74,11 +74,11 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
             while (true) {
                 if ((rc = two_phase_level())) return rc;
                 const SearchState &h = *p->h_st;
-                if (h.error || h.done || h.q_len[h.cur_level & 1] == 0) {
+                if (h.error || h.done || qe_count(h.qe[(2 * h.cur_level) % 3]) == 0) {
                     finished = true;
                     break;
                 }
-                if (h.q_len[h.cur_level & 1] <= threshold) break;
+                if (qe_count(h.qe[(2 * h.cur_level) % 3]) <= threshold) break;
             }
             if (finished) break;
         }
@@ -92,7 +92,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
             return rc;
     } else if (mode == B40C_ENACT_ITERATIVE) {
         if ((rc = read_state(p))) return rc;
-        while (!(p->h_st->error || p->h_st->done || p->h_st->q_len[p->h_st->cur_level & 1] == 0))
+        while (!(p->h_st->error || p->h_st->done || qe_count(p->h_st->qe[(2 * p->h_st->cur_level) % 3]) == 0))
             if ((rc = two_phase_level())) return rc;
     } else {
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "unknown enact mode %d", mode);

@@ -9,14 +9,17 @@ namespace rt {
 namespace {
 
 template <bool PRED>
-int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol, int32_t depth_limit)
+int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
+               int32_t depth_limit, bool direction_opt)
 {
     int rc;
     if ((rc = ensure_vf(p, 0, cap_of(p->queue_sizing, p->nodes)))) return rc;
     if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
     if ((rc = ensure_slots(p))) return rc;
     BfsParams k = make_params(p, pol);
+    k.direction_opt = direction_opt ? 1 : 0;
     const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
+    const void *merge = (const void *)dev::merge_kernel<PRED>;
     const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
@@ -24,8 +27,9 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     if (mode == B40C_ENACT_GRAPH) {
         if ((rc = mark_search_start(p))) return rc;
         KernelNode init{init_kernel_ptr<PRED>(true, true), dim3(init_grid(p, true)), dim3(kThreads), 0, k};
-        KernelNode body{kern, dim3(grid), dim3(kThreads), smem, k};
-        if ((rc = run_graph(p, B40C_EXPAND_CONTRACT, init, &body, 1))) return rc;
+        KernelNode body[2] = {{merge, dim3(grid), dim3(kThreads), 0, k}, {kern, dim3(grid), dim3(kThreads), smem, k}};
+        const int slot = direction_opt ? B40C_HYBRID + 1 : B40C_EXPAND_CONTRACT;
+        if ((rc = run_graph(p, slot, init, direction_opt ? body : body + 1, direction_opt ? 2 : 1))) return rc;
         return finish_timing(p);
     }
     if ((rc = upload_source(p))) return rc;
@@ -42,9 +46,13 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
         for (int level = 0;; level++) {
             if ((rc = read_state(p))) return rc;
             if (p->h_st->error || p->h_st->done) break;
-            const int q = p->h_st->q_len[level & 1], E = p->h_st->e_len[level & 1];
+            const int q = qe_count(p->h_st->qe[level % 3]), E = qe_edges(p->h_st->qe[level % 3]);
             if (q == 0) break;
-            const int g = std::max(1, std::min(grid, (E + 255) / 256));
+            int g = std::max(1, std::min(grid, (E + 255) / 256));
+            if (direction_opt) {
+                if ((rc = launch_plain(p, merge, grid, 0, k, "merge launch"))) return rc;
+                g = grid;  // a bottom-up level spans every vertex
+            }
             if ((rc = launch_plain(p, kern, g, smem, k, "expand-contract level launch"))) return rc;
         }
     } else {
@@ -56,10 +64,10 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
 }  // namespace
 
 int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
-                 int32_t depth_limit)
+                 int32_t depth_limit, bool direction_optimizing)
 {
-    return p->mark_pred ? enact_ec_t<true>(p, mode, src, max_grid, pol, depth_limit)
-                        : enact_ec_t<false>(p, mode, src, max_grid, pol, depth_limit);
+    return p->mark_pred ? enact_ec_t<true>(p, mode, src, max_grid, pol, depth_limit, direction_optimizing)
+                        : enact_ec_t<false>(p, mode, src, max_grid, pol, depth_limit, direction_optimizing);
 }
 
 }  // namespace rt

@@ -40,7 +40,9 @@ struct b40c_bfs_problem {
     // search arrays
     int32_t *d_labels = nullptr;
     uint32_t *d_mask = nullptr;
+    uint32_t *d_next = nullptr;  // bottom-up discoveries of a level (direction-optimizing), kept zero between levels
     int32_t mask_words = 0;
+    int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
     // frontiers
     b40c::VertexFrontier vf[2] = {};
     int64_t vcap[2] = {0, 0};
@@ -63,9 +65,9 @@ struct b40c_bfs_problem {
     bool needs_init = true;  // labels/mask dirty since the last reset
     // CUDA graphs of whole searches (ENACT_GRAPH), one per strategy, rebuilt
     // when the kernel parameters (buffers, policy) or the grid change
-    cudaGraphExec_t graph_exec[4] = {};
-    b40c::BfsParams graph_params[4] = {};
-    int graph_grid[4] = {};
+    cudaGraphExec_t graph_exec[5] = {};
+    b40c::BfsParams graph_params[5] = {};
+    int graph_grid[5] = {};
 };
 
 namespace b40c {
@@ -119,7 +121,8 @@ int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode 
 
 // enactors
 int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
-                 int32_t depth_limit);
+                 int32_t depth_limit, bool direction_optimizing);
+int check_symmetric(b40c_bfs_problem *p);
 int enact_edge(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                int32_t depth_limit);
 

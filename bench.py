@@ -264,7 +264,9 @@ def main():
     srcs = sources_for(g, fixed, args.sources)
     deg = np.diff(g.row_offsets).astype(np.int64)
     problem = CsrProblem.from_graph(g, device=local)
-    stream = torch.cuda.current_stream()
+    # a dedicated (non-default) stream shared by the library and the timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     problem.set_stream(stream.cuda_stream)
     enactor = ENACTORS[args.strategy]()
     N.check(problem.Reset(enactor.GetFrontierType(), 1.3), "Reset")

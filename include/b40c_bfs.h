@@ -57,7 +57,10 @@ enum {
     B40C_EXPAND_CONTRACT = 0, /* EnactorExpandContract   (enactor_expand_contract.cuh:59) */
     B40C_CONTRACT_EXPAND = 1, /* EnactorContractExpand   (enactor_contract_expand.cuh:61) */
     B40C_TWO_PHASE = 2,       /* EnactorTwoPhase         (enactor_two_phase.cuh:68) */
-    B40C_HYBRID = 3           /* EnactorHybrid           (enactor_hybrid.cuh:64) */
+    B40C_HYBRID = 3,          /* EnactorHybrid           (enactor_hybrid.cuh:64) */
+    B40C_DIRECTION_OPTIMIZING = 4 /* no counterpart in the reference: expand-contract top-down levels plus
+                                     bottom-up levels while the frontier is large (undirected graphs;
+                                     the same labels; plain expand-contract on a directed graph) */
 };
 
 /* How the levels of one search are launched. */
@@ -81,6 +84,12 @@ typedef struct b40c_bfs_policy {
                                       -1: do not (default) */
     int32_t bitmask_precheck;      /* 1: read the visited word before the atomic test-and-set (default),
                                       -1: go straight to the atomic */
+    int32_t queue_allocation;      /* frontier-slot allocation per tile of output: 1 = decoupled look-back
+                                      over tile ids, 2 = one packed 64-bit atomicAdd; 0 = default */
+    int32_t bottom_up_alpha;       /* direction-optimizing: go bottom-up when frontier edges exceed
+                                      unvisited edges / alpha */
+    int32_t bottom_up_beta;        /* direction-optimizing: return top-down when the frontier holds fewer
+                                      than nodes / beta vertices */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
@@ -159,6 +168,12 @@ int b40c_bfs_extract(b40c_bfs_problem *problem, int32_t *h_labels);
  * fraction of each CTA's lifetime spent on work (0 unless instrumented). */
 int b40c_bfs_stats(b40c_bfs_problem *problem, int64_t *total_queued, int32_t *search_depth,
                    double *avg_duty);
+
+/* Whether the CSR is symmetric (every edge u->v has a matching v->u, as a
+ * multiset), tested on the device by comparing order-independent 64-bit
+ * hash sums of the edges and of their reversals; cached per problem.
+ * Direction-optimizing searches run bottom-up levels only on symmetric graphs. */
+int b40c_bfs_problem_is_symmetric(b40c_bfs_problem *problem, int *symmetric);
 
 /* Device time of the last enact in milliseconds (CUDA events on the handle's stream). */
 int b40c_bfs_last_elapsed_ms(b40c_bfs_problem *problem, float *ms);

@@ -6,7 +6,7 @@ import oracle
 from back40computing_b200 import (CsrGraph, CsrProblem, BuildGrid2dGraph, BuildGrid3dGraph, BuildRmatGraph,
                                   BuildRandomRegularishGraph, BuildRandomGraph, search, sample_sources, B40cError)
 from back40computing_b200 import _native as N
-from back40computing_b200.bfs import EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID, ENACTORS
+from back40computing_b200.bfs import EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID, DIRECTION_OPTIMIZING, ENACTORS
 
 pytestmark = pytest.mark.gpu
 
@@ -37,7 +37,7 @@ def _check_dist(g, problem, src, strategy, mode, **kw):
     return depth
 
 
-STRATS = [EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID]
+STRATS = [EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID, DIRECTION_OPTIMIZING]
 
 
 @pytest.mark.parametrize("strategy", STRATS)
@@ -140,3 +140,51 @@ def test_repeated_searches_without_reset():
         N.check(enactor.EnactFusedSearch(p, int(s)))
         want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
         assert oracle.compare_labels(p.labels(), want) == -1
+
+
+def test_symmetry_detection():
+    g = _graph("rmat", 1 << 12, 1 << 15)
+    assert CsrProblem.from_graph(g).is_symmetric()
+    d = CsrGraph()
+    BuildRandomRegularishGraph(4096, 8, d, seed=1, symmetrize=False)
+    assert not CsrProblem.from_graph(d).is_symmetric()
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_direction_optimizing_goes_bottom_up_and_matches(mode):
+    """On R-MAT the large levels run bottom-up: labels and predecessor trees still
+    agree with the oracle, also with alpha/beta forcing bottom-up early and long."""
+    g = _graph("rmat", 1 << 16, 1 << 20)
+    for pred in (False, True):
+        p = CsrProblem.from_graph(g, mark_predecessors=pred)
+        for alpha, beta in ((0, 0), (1, 1000), (1000, 1)):
+            pol = N.Policy()
+            pol.bottom_up_alpha, pol.bottom_up_beta = alpha, beta
+            for s in sample_sources(g, 2, seed=5):
+                got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, mode=mode, policy=pol)
+                dist, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+                if pred:
+                    assert oracle.check_predecessors(g.row_offsets, g.column_indices, dist, got) == (-1, 0)
+                else:
+                    assert oracle.compare_labels(got, dist) == -1
+
+
+def test_direction_optimizing_directed_graph_falls_back():
+    d = CsrGraph()
+    BuildRandomRegularishGraph(20000, 6, d, seed=2, symmetrize=False)
+    p = CsrProblem.from_graph(d)
+    for s in (0, 7):
+        _check_dist(d, p, s, DIRECTION_OPTIMIZING, N.ENACT_FUSED)
+
+
+@pytest.mark.parametrize("qa", [1, 2])
+def test_queue_allocation_modes(qa):
+    g = _graph("rmat", 1 << 14, 1 << 18)
+    p = CsrProblem.from_graph(g)
+    pol = N.Policy()
+    pol.queue_allocation = qa
+    for strategy in (EXPAND_CONTRACT, TWO_PHASE):
+        for s in sample_sources(g, 2, seed=9):
+            got = search(p, int(s), strategy=strategy, policy=pol)
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            assert oracle.compare_labels(got, want) == -1
