@@ -42,6 +42,7 @@ class Policy(C.Structure):
         ("queue_allocation", C.c_int32),
         ("bottom_up_alpha", C.c_int32),
         ("bottom_up_beta", C.c_int32),
+        ("small_frontier_edges", C.c_int32),
     ]
 
 
@@ -56,6 +57,16 @@ class DeviceView(C.Structure):
         ("edges", C.c_int64),
         ("device", C.c_int32),
         ("mark_predecessors", C.c_int32),
+    ]
+
+
+class LevelRecord(C.Structure):
+    _fields_ = [
+        ("vertices", C.c_int32),
+        ("edges", C.c_int32),
+        ("bottom_up", C.c_int32),
+        ("pass_", C.c_int32),
+        ("t_ns", C.c_uint64),
     ]
 
 
@@ -97,6 +108,8 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_bfs_extract": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_stats": (C.c_int, [C.c_void_p, _P_i64, _P_i32, C.POINTER(C.c_double)]),
     "b40c_bfs_problem_is_symmetric": (C.c_int, [C.c_void_p, _P_i32]),
+    "b40c_bfs_set_instrument": (C.c_int, [C.c_void_p, C.c_int]),
+    "b40c_bfs_level_records": (C.c_int, [C.c_void_p, C.POINTER(LevelRecord), C.c_int, _P_i32]),
     "b40c_bfs_last_elapsed_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "b40c_bfs_recent_search_ms": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),

@@ -111,6 +111,20 @@ class CsrProblem:
         N.check(N.lib().b40c_bfs_recent_search_ms(self.handle, int(count), out), "recent_search_ms")
         return np.array(out[:], dtype=np.float64)
 
+    def set_instrument(self, on: bool = True) -> None:
+        N.check(N.lib().b40c_bfs_set_instrument(self.handle, int(bool(on))), "set_instrument")
+
+    def level_records(self, max_records: int = 1 << 16) -> list[dict]:
+        """Per-pass records of the last instrumented search (with durations)."""
+        buf = (N.LevelRecord * (max_records + 1))()
+        cnt = C.c_int32(0)
+        N.check(N.lib().b40c_bfs_level_records(self.handle, buf, max_records + 1, C.byref(cnt)), "level_records")
+        recs = [dict(vertices=r.vertices, edges=r.edges, bottom_up=bool(r.bottom_up), pass_=r.pass_,
+                     t_ns=int(r.t_ns)) for r in buf[:cnt.value]]
+        for a, b in zip(recs, recs[1:]):
+            a["ns"] = b["t_ns"] - a["t_ns"]
+        return [r for r in recs if r["pass_"] >= 0]
+
     def is_symmetric(self) -> bool:
         out = C.c_int32(0)
         N.check(N.lib().b40c_bfs_problem_is_symmetric(self.handle, C.byref(out)), "is_symmetric")

@@ -227,11 +227,11 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, ExpandSmem<B, 
     }
 }
 
-// The CTA's contiguous share [rs, re) of n items, with rs and re multiples of
-// kChunkGrain except re = n for the last CTA.
-__device__ __forceinline__ void cta_range(int n, int &rs, int &re)
+// Share `part` of `parts` of n items: [rs, re), with rs and re multiples of
+// kChunkGrain except re = n for the last share.
+__device__ __forceinline__ void cta_range(int n, int part, int parts, int &rs, int &re)
 {
-    const long long b = blockIdx.x, G = gridDim.x;
+    const long long b = part, G = parts;
     rs = (int)((long long)n * b / G / kChunkGrain * kChunkGrain);
     re = (b == G - 1) ? n : (int)((long long)n * (b + 1) / G / kChunkGrain * kChunkGrain);
 }
@@ -249,13 +249,13 @@ template <int B, bool PRED, bool FUSED_CULL>
 __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
                                              int level, int pass, const VertexFrontier &vout,
                                              const EdgeFrontier &eout, unsigned long long *qe_out,
-                                             unsigned &bar_phase)
+                                             unsigned &bar_phase, int part, int parts)
 {
     const int tid = threadIdx.x;
     const int q = s.q, E = s.E;
     constexpr int PER = kChunkMax / B;  // sub-round positions per thread
     int rs, re;
-    cta_range(E, rs, re);
+    cta_range(E, part, parts, rs, re);
     if (rs >= re) return;
     int i_cur = ld_cg(in.cf + rs / kChunkGrain);  // entry owning position rs
     for (int cs = rs; cs < re; cs += kChunkMax) {
@@ -389,7 +389,7 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
     const int q = s.q;
     constexpr int PER = kChunkMax / B;
     int rs, re;
-    cta_range(q, rs, re);
+    cta_range(q, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
         const int ce = min(cs + kChunkMax, re);
         if (tid == 0) s.out_count = 0;
@@ -423,57 +423,96 @@ constexpr int kBottomUpLongList = 256;  // lists longer than this are searched w
 // level + 1 (or that neighbour, the first one in CSR order).  Discoveries go
 // to next_mask (merged into the visited mask after the level, keeping the
 // snapshot intact) and, through emit_frontier, into the next vertex frontier.
-// A warp handles 32 consecutive vertices (one visited-mask word): each lane
-// scans its short list four neighbours at a time; long lists are then
-// searched by the whole warp, 32 neighbours at a time.
+// A warp handles blocks of 32 consecutive vertices (one visited-mask word);
+// each thread first issues, for all of its PER vertices at once, the
+// vertices' own visited words, their rows and their first kBottomUpProbe
+// neighbours' visited bits; vertices still without a parent then scan on
+// (short lists one lane each, four neighbours at a time; long lists by the
+// whole warp, 32 neighbours at a time).
+constexpr int kBottomUpProbe = 2;
+
 template <int B, bool PRED>
 __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
                                                 const VertexFrontier &vout, unsigned long long *qe_out)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr int PER = kChunkMax / B;
+    constexpr int K = kBottomUpProbe;
     int rs, re;
-    cta_range(p.nodes, rs, re);
+    cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
         if (tid == 0) s.out_count = 0;
-        __syncthreads();
+        // ---- own visited words (the snapshot is read coherently: ld.cg) ----------
+        unsigned word[PER];
+#pragma unroll
         for (int t = 0; t < PER; t++) {
-            const int vb = cs + t * B + (tid & ~31);  // multiple of 32: one mask word per warp
-            if (vb >= re) break;                      // warp-uniform
-            const int v = vb + lane;
-            const unsigned vis = ld_cg(p.mask + (vb >> 5));
-            bool todo = v < re && !((vis >> lane) & 1u);
-            int r0 = 0, r1 = 0;
-            if (todo) {
-                r0 = ld_ro(p.row_offsets + v);
-                r1 = ld_ro(p.row_offsets + v + 1);
-                todo = r1 > r0;
+            const int vb = cs + t * B + (tid & ~31);
+            word[t] = vb < re ? ld_cg(p.mask + (vb >> 5)) : 0xffffffffu;
+        }
+        int r0[PER], r1[PER];
+        bool todo[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int v = cs + t * B + tid;
+            todo[t] = v < re && !((word[t] >> lane) & 1u);
+            r0[t] = r1[t] = 0;
+            if (todo[t]) {
+                r0[t] = ld_ro(p.row_offsets + v);
+                r1[t] = ld_ro(p.row_offsets + v + 1);
             }
-            if (!__any_sync(0xffffffffu, todo)) continue;
-            const bool longlist = todo && (r1 - r0) > kBottomUpLongList;
-            bool scan = todo && !longlist;
-            int parent = -1;
-            int e = r0;
+        }
+        // ---- first K neighbours of every candidate -----------------------------------
+        int parent[PER];
+        {
+            int nb[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                todo[t] = todo[t] && r1[t] > r0[t];
+#pragma unroll
+                for (int k = 0; k < K; k++) nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+            }
+            unsigned w[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++)
+#pragma unroll
+                for (int k = 0; k < K; k++) w[t][k] = nb[t][k] >= 0 ? ld_mask(p.mask + (nb[t][k] >> 5)) : 0u;
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                parent[t] = -1;
+#pragma unroll
+                for (int k = K - 1; k >= 0; k--)
+                    if (nb[t][k] >= 0 && ((w[t][k] >> (nb[t][k] & 31)) & 1u)) parent[t] = nb[t][k];
+            }
+        }
+        // ---- continue the scan for candidates still without a parent ---------------
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
+            if (!__any_sync(0xffffffffu, more)) continue;
+            const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
+            bool scan = more && !longlist;
+            int e = r0[t] + K;
             while (__any_sync(0xffffffffu, scan)) {
                 if (scan) {
                     int nb[4];
                     unsigned w[4];
 #pragma unroll
-                    for (int k = 0; k < 4; k++) nb[k] = (e + k < r1) ? ld_stream(p.column_indices + e + k) : -1;
+                    for (int k = 0; k < 4; k++) nb[k] = (e + k < r1[t]) ? ld_stream(p.column_indices + e + k) : -1;
 #pragma unroll
                     for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(p.mask + (nb[k] >> 5)) : 0u;
 #pragma unroll
                     for (int k = 0; k < 4; k++)
-                        if (parent < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent = nb[k];
+                        if (parent[t] < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent[t] = nb[k];
                     e += 4;
-                    if (parent >= 0 || e >= r1) scan = false;
+                    if (parent[t] >= 0 || e >= r1[t]) scan = false;
                 }
             }
             unsigned lmask = __ballot_sync(0xffffffffu, longlist);
             while (lmask) {
                 const int owner = __ffs(lmask) - 1;
                 lmask &= lmask - 1;
-                const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
+                const int lr0 = __shfl_sync(0xffffffffu, r0[t], owner) + K;
+                const int lr1 = __shfl_sync(0xffffffffu, r1[t], owner);
                 int found_u = -1;
                 for (int eb = lr0; eb < lr1; eb += 32) {
                     const int ee = eb + lane;
@@ -485,14 +524,21 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                         break;
                     }
                 }
-                if (lane == owner) parent = found_u;
+                if (lane == owner) parent[t] = found_u;
             }
-            const bool found = parent >= 0;
+        }
+        // ---- label, mark and append the discoveries --------------------------------
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * B + (tid & ~31);
+            if (vb >= re) continue;  // warp-uniform
+            const int v = vb + lane;
+            const bool found = parent[t] >= 0;
             const unsigned fb = __ballot_sync(0xffffffffu, found);
             if (fb == 0) continue;
             if (lane == 0) p.next_mask[vb >> 5] = fb;  // this warp owns the whole word
             if (found) {
-                p.labels[v] = PRED ? parent : level + 1;
+                p.labels[v] = PRED ? parent[t] : level + 1;
                 s.flag = 1;
             }
             const int leader = __ffs(fb) - 1;
@@ -502,8 +548,8 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             if (found) {
                 const int slot = base + __popc(fb & lanemask_lt());
                 s.out[slot] = v;
-                s.colstart[slot] = r0;
-                s.rel[slot] = r1 - r0;
+                s.colstart[slot] = r0[t];
+                s.rel[slot] = r1[t] - r0[t];
             }
         }
         __syncthreads();
@@ -543,12 +589,47 @@ __device__ __forceinline__ bool choose_bottom_up(const BfsParams &p, bool was_bo
 // Level drivers
 // ------------------------------------------------------------------------------------
 
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 __device__ __forceinline__ unsigned long long ld_cg64(const unsigned long long *p)
 {
     unsigned long long v;
     asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
     return v;
 }
+
+// Per-CTA busy time (lifetime minus grid-barrier waits), accumulated into
+// p.duty when the search is instrumented: avg duty = busy / lifetime.
+struct DutyClock {
+    const BfsParams &p;
+    unsigned long long t0 = 0, waited = 0;
+    __device__ explicit DutyClock(const BfsParams &params) : p(params)
+    {
+        if (p.duty && threadIdx.x == 0) t0 = globaltimer_ns();
+    }
+    __device__ bool barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word, int *s_flag)
+    {
+        unsigned long long a = 0;
+        if (p.duty && threadIdx.x == 0) a = globaltimer_ns();
+        const bool ok = grid_barrier(counter, generation, error_word, s_flag);
+        if (p.duty && threadIdx.x == 0) waited += globaltimer_ns() - a;
+        return ok;
+    }
+    __device__ void finish()
+    {
+        if (p.duty && threadIdx.x == 0) {
+            const unsigned long long t1 = globaltimer_ns(), life = t1 - t0;
+            atomicAdd(&p.duty[0], life - min(waited, life));
+            atomicAdd(&p.duty[1], life);
+            atomicMax(&p.duty[2], t1);
+        }
+    }
+};
 
 // Epilogue of a non-persistent launch that completed a level: the last CTA
 // to finish advances the level and decides whether the search continues
@@ -586,11 +667,37 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
         }
         s.visited_edges = ld_cg64(&p.st->visited_edges[pass % 3]) + (unsigned long long)s.E;
         s.prev_bu = ld_cg(&p.st->dir[pass % 3]);
+        if (p.levels && blockIdx.x == 0 && pass < kMaxLevelRecords) {
+            LevelRecord r;
+            r.vertices = s.q;
+            r.edges = s.E;
+            r.bottom_up = 0;
+            r.pass = pass;
+            r.t_ns = globaltimer_ns();
+            p.levels[pass] = r;
+        }
     }
     __syncthreads();
 }
 
-// Expand-contract (vertex frontiers): one level per pass.
+// Direction bookkeeping of pass `pass` (block 0): the visited-edge total
+// and whether the level ran bottom-up, for the next pass.
+__device__ __forceinline__ void record_direction(const BfsParams &p, unsigned long long visited_edges, int pass,
+                                                 bool bu)
+{
+    p.st->visited_edges[(pass + 1) % 3] = visited_edges;
+    p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
+    if (bu) p.st->merge_pending = 1;
+    if (bu && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
+}
+
+constexpr int kSoloLevelCap = 4096;  // small levels CTA 0 runs alone before the grid resynchronises
+
+// Expand-contract (vertex frontiers): one level per pass.  With
+// direction_opt, levels with a large frontier run bottom-up.  In a
+// persistent launch, a run of levels whose frontiers have at most
+// p.small_edges edges is processed by CTA 0 alone, separated by CTA-level
+// barriers only, while the other CTAs wait at the grid barrier.
 template <int B, bool PRED>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
@@ -603,9 +710,10 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, worked = false;
+    DutyClock duty(p);
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
-        const int pass = level;
+        int pass = level;
         begin_pass<B, PRED>(p, s, pass, true);
         if (s.q == 0 || ld_cg(&p.st->error) != 0) break;
         const int dl = p.st->depth_limit;
@@ -613,21 +721,46 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             limit_hit = true;
             break;
         }
-        const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
-        if (tid == 0 && blockIdx.x == 0) {
-            p.st->visited_edges[(pass + 1) % 3] = s.visited_edges;
-            p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
-            if (bu) p.st->merge_pending = 1;
+        if (p.persistent && s.E <= p.small_edges) {
+            // ---- small frontiers: CTA 0 alone, level after level ----------------------
+            if (blockIdx.x == 0) {
+                for (int solo = 0;; solo++) {
+                    if (tid == 0) record_direction(p, s.visited_edges, pass, false);
+                    expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
+                                                &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
+                    __syncthreads();
+                    if (s.flag) max_level_seen = level + 1;
+                    level++;
+                    pass = level;
+                    if (tid == 0) {
+                        const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
+                        s.q = qe_count(x);
+                        s.E = qe_edges(x);
+                    }
+                    __syncthreads();
+                    const bool stop = s.q == 0 || s.E > p.small_edges || (dl >= 0 && level >= dl) ||
+                                      solo + 1 >= kSoloLevelCap || ld_cg(&p.st->error) != 0;
+                    if (stop) break;
+                    begin_pass<B, PRED>(p, s, pass, true);
+                }
+                if (tid == 0) p.st->cur_level = level;
+            }
+            worked = true;
+            if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+            level = ld_cg(&p.st->cur_level) - 1;  // the loop increment brings it back
+            continue;
         }
+        const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
+        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu);
         if (bu)
             bottom_up_range<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         else
             expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
-                                        &p.st->qe[(pass + 1) % 3], bar_phase);
+                                        &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);
         __syncthreads();
         if (bu && p.persistent) {
             // fold the level's discoveries into the visited mask before the next level
-            if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+            if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
             merge_next_mask(p);
             if (tid == 0 && blockIdx.x == 0) p.st->merge_pending = 0;
         }
@@ -639,9 +772,10 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             if (tid == 0) atomicOr(&p.st->error, kErrInjected);
             return;  // never arrives: the others' bounded waits must expire
         }
-        if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
+    duty.finish();
     if (p.persistent) {
         if (tid == 0 && blockIdx.x == 0) {
             p.st->cur_level = level;
@@ -670,6 +804,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, saturated = false, completed_level = false;
+    DutyClock duty(p);
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
         const int in_idx = p.edge_pingpong ? (level & 1) : 0;
@@ -690,7 +825,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
                     if (tid == 0) atomicOr(&p.st->error, kErrInjected);
                     return;
                 }
-                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+                if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
             }
         }
         const int dl = p.st->depth_limit;
@@ -708,17 +843,19 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
             }
             if (tid == 0 && blockIdx.x == 0) p.st->qe[(pass + 1) % 3] = pack((unsigned)(q == 0 ? 0 : E), 0u);
             if (q > 0)
-                expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr, bar_phase);
+                expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr, bar_phase,
+                                             blockIdx.x, gridDim.x);
             __syncthreads();
             completed_level = true;
             if (p.persistent) {
                 if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
-                if (!grid_barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+                if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
             }
         }
         if (!p.persistent) break;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
+    duty.finish();
     if (p.persistent) {
         if (tid == 0 && blockIdx.x == 0) {
             p.st->cur_level = level;

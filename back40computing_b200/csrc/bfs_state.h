@@ -63,6 +63,18 @@ __host__ __device__ inline int pass_of(int level, int phase, bool edge_strategy)
     return edge_strategy ? 2 * level + phase : level;
 }
 
+// Per-level record written when a search is instrumented (the role of the
+// reference's KernelRuntimeStats, util/kernel_runtime_stats.cuh:45-126, and of
+// its driver's per-level histogram, test/bfs/test_bfs.cu:264-337).
+struct LevelRecord {
+    int32_t vertices;          // frontier entries (vertex frontier) or items (edge frontier) of the pass
+    int32_t edges;             // edges of the vertex frontier (0 for edge-frontier passes)
+    int32_t bottom_up;         // 1 when the level ran bottom-up
+    int32_t pass;
+    unsigned long long t_ns;   // %globaltimer when block 0 started the pass
+};
+constexpr int kMaxLevelRecords = 1 << 16;
+
 // Kernel parameter block.
 struct BfsParams {
     const int32_t *row_offsets;
@@ -95,8 +107,10 @@ struct BfsParams {
     int32_t direction_opt;    // 1: levels may run bottom-up (symmetric graphs only)
     int32_t bu_alpha;         // switch to bottom-up when frontier edges > unvisited edges / alpha
     int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
-    int32_t pad2;
+    int32_t small_edges;      // persistent launches: frontiers with at most this many edges run on CTA 0 alone
     uint32_t *next_mask;      // bottom-up discoveries of the current level (merged into mask after it)
+    LevelRecord *levels;      // per-pass records when instrumented, else null
+    unsigned long long *duty; // [0] sum over CTAs of busy ns, [1] sum of lifetime ns (instrumented)
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
 };
 

@@ -29,6 +29,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     if ((rc = begin_enact(p, src, depth_limit))) return rc;
+    if ((rc = begin_instrumented(p))) return rc;
 
     BfsParams kc = k, kx = k;  // one-phase launches: contract, expand
     kc.phase_mask = 1;

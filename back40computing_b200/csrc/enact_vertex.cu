@@ -24,6 +24,7 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     if ((rc = begin_enact(p, src, depth_limit))) return rc;
+    if ((rc = begin_instrumented(p))) return rc;
     if (mode == B40C_ENACT_GRAPH) {
         if ((rc = mark_search_start(p))) return rc;
         KernelNode init{init_kernel_ptr<PRED>(true, true), dim3(init_grid(p, true)), dim3(kThreads), 0, k};

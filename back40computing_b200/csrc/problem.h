@@ -43,6 +43,10 @@ struct b40c_bfs_problem {
     uint32_t *d_next = nullptr;  // bottom-up discoveries of a level (direction-optimizing), kept zero between levels
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
+    // instrumentation (per-pass records, CTA duty)
+    bool instrument = false;
+    b40c::LevelRecord *d_levels = nullptr;
+    unsigned long long *d_duty = nullptr;
     // frontiers
     b40c::VertexFrontier vf[2] = {};
     int64_t vcap[2] = {0, 0};
@@ -105,6 +109,7 @@ int check_state_errors(b40c_bfs_problem *p);
 int persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_policy &pol, int max_grid, size_t smem,
                     int *grid);
 int finish_timing(b40c_bfs_problem *p);
+int begin_instrumented(b40c_bfs_problem *p);
 void free_graphs(b40c_bfs_problem *p);
 
 // One kernel launch of a captured search.

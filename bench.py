@@ -34,6 +34,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "BFS GTEPS on 1 B200 (plain vs 64-source batched); served p50/p99 latency"
+STRATEGY_NAMES = ["expand-contract", "contract-expand", "two-phase", "hybrid", "direction-optimizing"]
 
 CONFIGS = {
     "rmat22": dict(kind="rmat", scale=22, ef=16,
@@ -53,7 +54,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="rmat22")
-    ap.add_argument("--strategy", type=int, default=0, help="0 EC, 1 CE, 2 two-phase, 3 hybrid")
+    ap.add_argument("--strategy", type=int, default=4,
+                    help="0 expand-contract, 1 contract-expand, 2 two-phase, 3 hybrid, 4 direction-optimizing")
     ap.add_argument("--mode", type=int, default=0, help="0 fused (persistent), 1 per-level launches, 2 CUDA graph")
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -337,6 +339,15 @@ def main():
     e2e = {"value": float(ec.sum()) * args.steps / e2e_s / 1e9, "unit": "GTEPS",
            "h2d_bytes_per_step": 8 * len(srcs), "d2h_bytes_per_step": 4 * g.nodes * len(srcs)}
 
+    # the same searches through the reference-faithful top-down strategy, for comparison
+    topdown = None
+    if args.strategy == 4 and rank == 0:
+        td = ENACTORS[0]()
+        for s in srcs:
+            N.check(td._enact(problem, int(s), args.mode, 0))
+        tk = problem.recent_search_ms(len(srcs))
+        topdown = {"gteps": float(ec.sum() / (tk.sum() * 1e-3) / 1e9), "kernel_ms_per_search": float(tk.mean())}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g, srcs, deg, args.cpu_seconds)
@@ -348,7 +359,8 @@ def main():
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
             "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
                        "vertices": g.nodes, "edges": g.edges, "searches_per_step": len(srcs),
-                       "strategy": ["expand-contract", "contract-expand", "two-phase", "hybrid"][args.strategy],
+                       "strategy": STRATEGY_NAMES[args.strategy],
+                       "topdown_expand_contract": topdown,
                        "mode": ["fused persistent", "per-level launches", "cuda graph"][args.mode],
                        "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6),
                        "parallelism": f"replicas x{world}"},

@@ -90,6 +90,9 @@ typedef struct b40c_bfs_policy {
                                       unvisited edges / alpha */
     int32_t bottom_up_beta;        /* direction-optimizing: return top-down when the frontier holds fewer
                                       than nodes / beta vertices */
+    int32_t small_frontier_edges;  /* fused searches: runs of levels whose frontier has at most this many
+                                      edges are processed by one CTA alone (CTA-level barriers only);
+                                      -1 disables */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
@@ -174,6 +177,25 @@ int b40c_bfs_stats(b40c_bfs_problem *problem, int64_t *total_queued, int32_t *se
  * hash sums of the edges and of their reversals; cached per problem.
  * Direction-optimizing searches run bottom-up levels only on symmetric graphs. */
 int b40c_bfs_problem_is_symmetric(b40c_bfs_problem *problem, int *symmetric);
+
+/* Instrumentation (the reference's INSTRUMENT template flag,
+ * kernel_runtime_stats.cuh:45-126, and its driver's per-level histogram,
+ * test_bfs.cu:264-337).  When on, each search records one entry per pass
+ * (a level; edge strategies: contract and expand phases of a level) and the
+ * CTAs' busy time, which b40c_bfs_stats reports as avg_duty. */
+typedef struct b40c_level_record {
+    int32_t vertices;  /* frontier entries (or edge-frontier items) processed by the pass */
+    int32_t edges;     /* edges of the vertex frontier (0 for edge-frontier passes) */
+    int32_t bottom_up; /* 1 when the level ran bottom-up */
+    int32_t pass;      /* pass index; -1 marks the closing record */
+    uint64_t t_ns;     /* device global timer when the pass started (closing record: search end) */
+} b40c_level_record;
+
+int b40c_bfs_set_instrument(b40c_bfs_problem *problem, int on);
+
+/* Copies the last instrumented search's records (at most max_records) plus a
+ * closing record; *count receives the number written. */
+int b40c_bfs_level_records(b40c_bfs_problem *problem, b40c_level_record *out, int max_records, int *count);
 
 /* Device time of the last enact in milliseconds (CUDA events on the handle's stream). */
 int b40c_bfs_last_elapsed_ms(b40c_bfs_problem *problem, float *ms);

@@ -188,3 +188,34 @@ def test_queue_allocation_modes(qa):
             got = search(p, int(s), strategy=strategy, policy=pol)
             want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
             assert oracle.compare_labels(got, want) == -1
+
+
+@pytest.mark.parametrize("small", [-1, 256, 1 << 30])
+@pytest.mark.parametrize("strategy", [EXPAND_CONTRACT, DIRECTION_OPTIMIZING])
+def test_small_frontier_path(small, strategy):
+    """Runs of small levels on one CTA (or never, or always) give the same labels."""
+    pol = N.Policy()
+    pol.small_frontier_edges = small
+    for kind, args in (("grid2d", (70,)), ("rmat", (1 << 13, 1 << 16)), ("grid3d", (12,))):
+        g = _graph(kind, *args)
+        p = CsrProblem.from_graph(g)
+        for s in sample_sources(g, 2, seed=4):
+            got = search(p, int(s), strategy=strategy, policy=pol)
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            assert oracle.compare_labels(got, want) == -1
+
+
+def test_instrumentation_records_levels():
+    g = _graph("grid2d", 40)
+    p = CsrProblem.from_graph(g)
+    p.set_instrument(True)
+    got = search(p, 0)
+    recs = p.level_records()
+    assert len(recs) == int(got.max()) + 2  # one per level plus the empty last frontier
+    hist = oracle.level_histogram(got)
+    # a level's frontier is the vertices at that distance (all have edges on a lattice)
+    assert [r["vertices"] for r in recs[:-1]] == [int(c) for c in hist]
+    enactor = ENACTORS[EXPAND_CONTRACT]()
+    enactor._problem = p
+    _, depth, duty = enactor.GetStatistics()
+    assert depth == int(got.max()) + 1 and 0.0 < duty <= 1.0
