@@ -424,7 +424,11 @@ int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t no
         cudaGetLastError();
         return b40c::fail(B40C_ERROR_NO_DEVICE, "no CUDA device available");
     }
-    if (device < 0 || device >= ndev) return b40c::fail(B40C_ERROR_INVALID_VALUE, "invalid device %d", device);
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no current CUDA device");
+    }
+    if (device >= ndev) return b40c::fail(B40C_ERROR_INVALID_VALUE, "invalid device %d", device);
     DeviceGuard guard(device);
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");

@@ -1,0 +1,85 @@
+/*
+ * Direction-optimizing enactor (no counterpart in the reference): expand-contract
+ * top-down levels, bottom-up levels while the frontier is large, on
+ * undirected (symmetric) graphs; plain expand-contract otherwise.  Same labels.
+ */
+#pragma once
+#include "enactor_base.cuh"
+
+namespace b40c {
+namespace graph {
+namespace bfs {
+
+template <bool INSTRUMENT>
+class EnactorDirectionOptimizing : public EnactorBase {
+  public:
+    EnactorDirectionOptimizing(bool DEBUG = false) : EnactorBase(VERTEX_FRONTIERS, B40C_DIRECTION_OPTIMIZING, INSTRUMENT, DEBUG) {}
+
+    /* one persistent grid, bounded software barrier between levels */
+    template <typename CsrProblem>
+    cudaError_t EnactFusedSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_FUSED, max_grid_size, (const b40c_bfs_policy *)0);
+    }
+
+    /* same, with an explicit runtime kernel policy (in place of the reference's
+     * compile-time KernelPolicy template argument) */
+    template <typename CsrProblem>
+    cudaError_t EnactFusedSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, const b40c_bfs_policy &policy,
+                        int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_FUSED, max_grid_size, &policy);
+    }
+
+    /* one launch (or phase pair) per level */
+    template <typename CsrProblem>
+    cudaError_t EnactIterativeSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_ITERATIVE, max_grid_size, (const b40c_bfs_policy *)0);
+    }
+
+    /* same, with an explicit runtime kernel policy (in place of the reference's
+     * compile-time KernelPolicy template argument) */
+    template <typename CsrProblem>
+    cudaError_t EnactIterativeSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, const b40c_bfs_policy &policy,
+                        int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_ITERATIVE, max_grid_size, &policy);
+    }
+
+    /* the strategy's default schedule */
+    template <typename CsrProblem>
+    cudaError_t EnactSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_FUSED, max_grid_size, (const b40c_bfs_policy *)0);
+    }
+
+    /* same, with an explicit runtime kernel policy (in place of the reference's
+     * compile-time KernelPolicy template argument) */
+    template <typename CsrProblem>
+    cudaError_t EnactSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, const b40c_bfs_policy &policy,
+                        int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_FUSED, max_grid_size, &policy);
+    }
+
+    /* the whole search replayed as one CUDA graph */
+    template <typename CsrProblem>
+    cudaError_t EnactGraphSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_GRAPH, max_grid_size, (const b40c_bfs_policy *)0);
+    }
+
+    /* same, with an explicit runtime kernel policy (in place of the reference's
+     * compile-time KernelPolicy template argument) */
+    template <typename CsrProblem>
+    cudaError_t EnactGraphSearch(CsrProblem &csr_problem, typename CsrProblem::VertexId src, const b40c_bfs_policy &policy,
+                        int max_grid_size = 0)
+    {
+        return this->Enact(csr_problem, src, B40C_ENACT_GRAPH, max_grid_size, &policy);
+    }
+};
+
+}  // namespace bfs
+}  // namespace graph
+}  // namespace b40c

@@ -128,8 +128,9 @@ int b40c_bfs_default_policy(int strategy, b40c_bfs_policy *policy);
 
 /* CsrProblem::FromHostProblem (csr_problem.cuh:328-540): copies the CSR to the
  * device (or, with stream_from_host, maps the caller's pinned host arrays
- * zero-copy: they must stay valid until destroy).  num_gpus other than 1 is
- * rejected (single-GPU library). */
+ * zero-copy: they must stay valid until destroy).  device < 0 selects the
+ * calling thread's current CUDA device.  num_gpus other than 1 is
+ * rejected by the C++ layer (single-GPU library). */
 int b40c_bfs_problem_create(const int32_t *h_row_offsets, const int32_t *h_column_indices,
                             int64_t nodes, int64_t edges, int mark_predecessors,
                             int stream_from_host, int device, b40c_bfs_problem **out);
@@ -212,7 +213,7 @@ int b40c_bfs_device_view_get(b40c_bfs_problem *problem, b40c_bfs_device_view *vi
 int b40c_host_alloc(void **ptr, size_t bytes, int mapped);
 int b40c_host_free(void *ptr);
 
-/* ---- graph builders (b40c/graph/builder/*.cuh) -----------------------------
+/* ---- graph builders (the b40c/graph/builder headers) ---------------------------
  * Native, multi-threaded builders used by the benchmark and the Python layer.
  * Arrays are allocated with malloc (or pinned when pinned != 0) and released
  * with b40c_graph_free.  Results are deterministic for a seed, independent of
