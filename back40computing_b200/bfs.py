@@ -125,6 +125,21 @@ class CsrProblem:
             a["ns"] = b["t_ns"] - a["t_ns"]
         return [r for r in recs if r["pass_"] >= 0]
 
+    # ---- batched multi-source searches ------------------------------------------------
+    def msbfs(self, sources, depth_limits=None, policy: N.Policy | None = None, max_grid_size: int = 0) -> None:
+        """Searches up to 64 sources together (asynchronous); see labels_of()."""
+        src = np.ascontiguousarray(sources, dtype=np.int32)
+        lim = None if depth_limits is None else np.ascontiguousarray(depth_limits, dtype=np.int32)
+        pol = C.byref(policy) if policy is not None else None
+        N.check(N.lib().b40c_msbfs_enact(self.handle, N.i32p(src), N.i32p(lim) if lim is not None else None,
+                                         int(src.size), int(max_grid_size), pol), "msbfs")
+
+    def labels_of(self, slot: int) -> np.ndarray:
+        """Labels of source `slot` of the last batch."""
+        out = np.empty(self.nodes, dtype=np.int32)
+        N.check(N.lib().b40c_msbfs_extract(self.handle, int(slot), N.i32p(out)), "msbfs_extract")
+        return out
+
     def is_symmetric(self) -> bool:
         out = C.c_int32(0)
         N.check(N.lib().b40c_bfs_problem_is_symmetric(self.handle, C.byref(out)), "is_symmetric")

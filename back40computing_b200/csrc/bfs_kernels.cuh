@@ -168,9 +168,9 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
 // packed 64-bit atomicAdd on the pass's output counter.  Each entry gets its
 // slot, its degree prefix P and its kChunkGrain boundaries in vout.cf.  The
 // pass total accumulates in *qe_out.  All threads must call it.
-template <int B, bool PRED>
-__device__ __forceinline__ void emit_frontier(const BfsParams &p, ExpandSmem<B, PRED> &s, int pass,
-                                              const VertexFrontier &vout, unsigned long long *qe_out)
+template <int B, typename Smem>
+__device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int pass, const VertexFrontier &vout,
+                                              unsigned long long *qe_out)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cnt = s.out_count;
@@ -372,7 +372,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         __syncthreads();  // run tables consumed: they now collect the sub-round's output
         discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level + 1);
         __syncthreads();
-        emit_frontier<B, PRED>(p, s, pass, vout, qe_out);
+        emit_frontier<B>(p, s, pass, vout, qe_out);
         __syncthreads();
     }
 }
@@ -406,7 +406,7 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
         __syncthreads();
         discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level);
         __syncthreads();
-        emit_frontier<B, PRED>(p, s, pass, p.vf[0], qe_out);
+        emit_frontier<B>(p, s, pass, p.vf[0], qe_out);
         __syncthreads();
     }
 }
@@ -553,7 +553,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             }
         }
         __syncthreads();
-        emit_frontier<B, PRED>(p, s, pass, vout, qe_out);
+        emit_frontier<B>(p, s, pass, vout, qe_out);
         __syncthreads();
     }
 }

@@ -1,0 +1,413 @@
+// Batched multi-source BFS (up to 64 sources per launch) for sm_100a.
+//
+// No counterpart in the reference (its BFS searches one source at a time);
+// the traversal arithmetic per source is the same as a single-source search:
+// labels[s][v] = distance of v from source s (-1 unreached).
+//
+// Per vertex the search keeps a 64-bit visited mask V[v] (bit s: source s
+// reached v) and, for the current and next level, 64-bit frontier masks
+// F[cur][v] / F[next][v].  Two level kinds:
+//  * push (sparse frontiers): the frontier queue is expanded with the same
+//    edge-balanced per-CTA ranges as the single-source kernels, so each
+//    adjacency list is read once per level for all sources together; for a
+//    gathered edge u -> w:
+//        new = F[cur][u] & active & ~V[w]    (active: sources under their depth limit)
+//        set = new & ~atomicOr(&V[w], new)   (the bits this edge is first to set)
+//        labels[s][w] = level + 1 for s in set
+//        if atomicOr(&F[next][w], set) was 0: w joins the next frontier queue;
+//  * pull (dense frontiers, symmetric graphs only): every vertex still missing
+//    some active source ORs its neighbours' F[cur] masks (no atomics; a warp
+//    stores source s's labels of 32 consecutive vertices at once).
+// After each level F[cur] is cleared over the level's queue (two grid
+// barriers per level).
+#pragma once
+#include "bfs_kernels.cuh"
+
+namespace b40c {
+namespace dev {
+
+struct MsParams {
+    unsigned long long *visited;     // V[n]
+    unsigned long long *fmask[2];    // F[2][n]
+    int32_t *labels;                 // [k][n], source-major
+    const int32_t *depth_limit;      // [k]; < 0 unlimited
+    int32_t k;
+    int32_t pull_ok;                 // 1: the graph is symmetric, dense levels may pull
+};
+
+template <int B>
+struct MsSmem {
+    int32_t colstart[kChunkMax + 2];
+    int32_t rel[kChunkMax + 2];
+    unsigned long long fm[kChunkMax + 2];  // frontier mask of run j's vertex
+    uint16_t own[kChunkMax];
+    int32_t out[kChunkMax];
+    int32_t limits[64];
+    int32_t out_count;
+    int32_t flag;
+    int32_t q, E;
+    unsigned long long active;
+    unsigned long long scan_warp[B / 32];
+    unsigned long long prefix;
+};
+
+// Push level: expansion of the CTA's share of the level's frontier queue.
+template <int B>
+__device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
+                                                const VertexFrontier &in, const VertexFrontier &vout,
+                                                unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int q = s.q, E = s.E;
+    constexpr int PER = kChunkMax / B;
+    const unsigned long long *fcur = m.fmask[level & 1];
+    unsigned long long *fnext = m.fmask[(level + 1) & 1];
+    const long long n = p.nodes;
+    int rs, re;
+    cta_range(E, blockIdx.x, gridDim.x, rs, re);
+    if (rs >= re) return;
+    int i_cur = ld_cg(in.cf + rs / kChunkGrain);
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        const int ce = min(cs + kChunkMax, re);
+        const int len = ce - cs;
+        if (tid == 0) s.out_count = 0;
+        int k = 0;
+        for (int base = i_cur;; base += B) {
+            const int i = base + tid;
+            bool inside = false;
+            if (i < q) {
+                const int Pi = ld_cg(in.P + i);
+                if (Pi < ce && i - i_cur <= kChunkMax) {
+                    inside = true;
+                    const int j = i - i_cur;
+                    const int start = max(Pi, cs);
+                    s.rel[j] = start - cs;
+                    s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
+                    s.fm[j] = ld_cg64(fcur + ld_cg(in.v + i)) & s.active;
+                }
+            }
+            const int c = __syncthreads_count(inside);
+            k += c;
+            if (c < B) break;
+        }
+        if (tid == 0) s.rel[k] = len;
+        __syncthreads();
+        {
+            const int x0 = tid * PER;
+            if (x0 < len) {
+                int lo = 0, hi = k - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s.rel[mid] <= x0) lo = mid; else hi = mid - 1;
+                }
+                int j = lo;
+                int next = s.rel[j + 1];
+#pragma unroll
+                for (int t = 0; t < PER; t++) {
+                    const int x = x0 + t;
+                    if (x < len) {
+                        while (x >= next) {
+                            j++;
+                            next = s.rel[j + 1];
+                        }
+                        s.own[x] = (uint16_t)j;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        int w[PER];
+        unsigned long long f[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int x = t * B + tid;
+            w[t] = -1;
+            f[t] = 0;
+            if (x < len) {
+                const int j = s.own[x];
+                f[t] = s.fm[j];
+                if (f[t]) w[t] = ld_stream(p.column_indices + s.colstart[j] + (x - s.rel[j]));
+            }
+        }
+        i_cur += k - 1;
+        __syncthreads();  // run tables consumed: they now collect the sub-round's output
+        unsigned long long nw[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) nw[t] = (w[t] >= 0) ? (f[t] & ~ld_cg64(m.visited + w[t])) : 0ull;
+        unsigned long long set[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) set[t] = nw[t] ? (nw[t] & ~atomicOr(m.visited + w[t], nw[t])) : 0ull;
+        bool first[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            first[t] = false;
+            if (set[t]) {
+                unsigned long long bits = set[t];
+                while (bits) {
+                    const int src = __ffsll((long long)bits) - 1;
+                    bits &= bits - 1;
+                    m.labels[(long long)src * n + w[t]] = level + 1;
+                }
+                first[t] = atomicOr(fnext + w[t], set[t]) == 0ull;
+            }
+        }
+        int r0[PER], r1[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            r0[t] = r1[t] = 0;
+            if (first[t]) {
+                r0[t] = ld_ro(p.row_offsets + w[t]);
+                r1[t] = ld_ro(p.row_offsets + w[t] + 1);
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            if (t * B >= len) continue;  // CTA-uniform
+            if (set[t]) s.flag = 1;
+            const bool push = first[t] && r1[t] > r0[t];
+            const unsigned bal = __ballot_sync(0xffffffffu, push);
+            if (bal == 0) continue;
+            const int leader = __ffs(bal) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (push) {
+                const int slot = base + __popc(bal & lanemask_lt());
+                s.out[slot] = w[t];
+                s.colstart[slot] = r0[t];
+                s.rel[slot] = r1[t] - r0[t];
+            }
+        }
+        __syncthreads();
+        emit_frontier<B>(p, s, level, vout, qe_out);
+        __syncthreads();
+    }
+}
+
+// Pull level (symmetric graphs): one thread per vertex, eight neighbours per
+// step, stopping once every missing source is found; lists longer than
+// kPullLongList are searched by the whole warp afterwards.  Only v's own
+// thread writes V[v] and F[next][v].
+constexpr int kPullLongList = 256;
+
+template <int B>
+__device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
+                                              const VertexFrontier &vout, unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr int PER = kChunkMax / B;
+    constexpr int U = 8;
+    const unsigned long long *fcur = m.fmask[level & 1];
+    unsigned long long *fnext = m.fmask[(level + 1) & 1];
+    const unsigned long long active = s.active;
+    const long long n = p.nodes;
+    int rs, re;
+    cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        if (tid == 0) s.out_count = 0;
+        __syncthreads();
+#pragma unroll 1
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * B + (tid & ~31);
+            if (vb >= re) break;  // warp-uniform
+            const int v = vb + lane;
+            const bool inr = v < re;
+            unsigned long long vold = 0, missing = 0;
+            int r0 = 0, r1 = 0;
+            if (inr) {
+                vold = ld_cg64(m.visited + v);
+                missing = active & ~vold;
+                if (missing) {
+                    r0 = ld_ro(p.row_offsets + v);
+                    r1 = ld_ro(p.row_offsets + v + 1);
+                }
+            }
+            const bool longlist = missing && (r1 - r0) > kPullLongList;
+            unsigned long long acc = 0;
+            if (missing && !longlist) {
+                for (int e = r0; e < r1 && acc != missing; e += U) {
+                    int nb[U];
+#pragma unroll
+                    for (int k = 0; k < U; k++) nb[k] = (e + k < r1) ? ld_stream(p.column_indices + e + k) : -1;
+                    unsigned long long fm[U];
+#pragma unroll
+                    for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_cg64(fcur + nb[k]) : 0ull;
+#pragma unroll
+                    for (int k = 0; k < U; k++) acc |= fm[k] & missing;
+                }
+            }
+            unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+            while (lmask) {
+                const int owner = __ffs(lmask) - 1;
+                lmask &= lmask - 1;
+                const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
+                const unsigned long long miss = __shfl_sync(0xffffffffu, missing, owner);
+                unsigned long long a = 0;
+                for (int eb = lr0; eb < lr1; eb += 32) {
+                    const int ee = eb + lane;
+                    if (ee < lr1) a |= ld_cg64(fcur + ld_stream(p.column_indices + ee)) & miss;
+                    for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
+                    if (a == miss) break;
+                }
+                if (lane == owner) acc = a;
+            }
+            const bool found = acc != 0;
+            if (found) {
+                m.visited[v] = vold | acc;
+                fnext[v] = acc;
+                s.flag = 1;
+            }
+            // labels, source by source: one coalesced store per warp
+            const unsigned long long wor_lo = __reduce_or_sync(0xffffffffu, (unsigned)(acc & 0xffffffffull));
+            const unsigned long long wor_hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc >> 32));
+            unsigned long long wor = wor_lo | (wor_hi << 32);
+            while (wor) {
+                const int src = __ffsll((long long)wor) - 1;
+                wor &= wor - 1;
+                if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1;
+            }
+            const bool push = found && r1 > r0;
+            const unsigned bal = __ballot_sync(0xffffffffu, push);
+            if (bal) {
+                const int leader = __ffs(bal) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (push) {
+                    const int slot = base + __popc(bal & lanemask_lt());
+                    s.out[slot] = v;
+                    s.colstart[slot] = r0;
+                    s.rel[slot] = r1 - r0;
+                }
+            }
+        }
+        __syncthreads();
+        emit_frontier<B>(p, s, level, vout, qe_out);
+        __syncthreads();
+    }
+}
+
+// Whole batched search in one persistent cooperative grid.
+template <int B>
+__global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    MsSmem<B> &s = *reinterpret_cast<MsSmem<B> *>(smem_raw);
+    __shared__ int s_ok;
+    const int tid = threadIdx.x;
+    if (tid < 64) s.limits[tid] = tid < m.k ? m.depth_limit[tid] : 0;
+    unsigned generation = 0;
+    int max_level_seen = -1;
+    DutyClock duty(p);
+    __syncthreads();
+    for (int level = 0;; level++) {
+        const int pass = level;
+        if (tid == 0) {
+            const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
+            s.q = qe_count(x);
+            s.E = qe_edges(x);
+            s.flag = 0;
+            unsigned long long act = 0;
+            for (int src = 0; src < m.k; src++)
+                if (s.limits[src] < 0 || level < s.limits[src]) act |= 1ull << src;
+            s.active = act;
+            if (blockIdx.x == 0) {
+                p.st->qe[(pass + 2) % 3] = 0;
+                p.st->tile_ctr[(pass + 1) % 3] = 0;
+                atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
+                if (p.levels && pass < kMaxLevelRecords) {
+                    LevelRecord r;
+                    r.vertices = s.q;
+                    r.edges = s.E;
+                    r.bottom_up = 0;
+                    r.pass = pass;
+                    r.t_ns = globaltimer_ns();
+                    p.levels[pass] = r;
+                }
+            }
+        }
+        __syncthreads();
+        if (s.q == 0 || s.active == 0 || ld_cg(&p.st->error) != 0) break;
+        // pull when the frontier's edges are a large share of the graph (symmetric graphs)
+        const bool pull = m.pull_ok && (long long)s.E * p.bu_alpha > (long long)p.edges;
+        if (tid == 0 && blockIdx.x == 0 && pull && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
+        if (pull)
+            ms_pull_range<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        else
+            ms_expand_range<B>(p, m, s, level, p.vf[level & 1], p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        __syncthreads();
+        if (s.flag) max_level_seen = level + 1;
+        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+        // clear this level's frontier masks (the queue lists every vertex with edges that has one)
+        {
+            const VertexFrontier in = p.vf[level & 1];
+            unsigned long long *fcur = m.fmask[level & 1];
+            for (int i = blockIdx.x * B + tid; i < s.q; i += gridDim.x * B) fcur[ld_cg(in.v + i)] = 0ull;
+        }
+        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+    }
+    if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
+    duty.finish();
+    if (tid == 0 && blockIdx.x == 0) p.st->done = 1;
+}
+
+// Batch set-up: labels <- -1, masks <- 0 (grid-stride) and the search state.
+template <int DUMMY = 0>
+__global__ void msbfs_init_kernel(BfsParams p, MsParams m)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)m.k * p.nodes;
+    for (long long i = t0; i < total; i += stride) m.labels[i] = -1;
+    for (long long v = t0; v < p.nodes; v += stride) {
+        m.visited[v] = 0;
+        m.fmask[0][v] = 0;
+        m.fmask[1][v] = 0;
+    }
+    if (t0 == 0) {
+        SearchState *st = p.st;
+        st->tile_ctr[0] = st->tile_ctr[1] = st->tile_ctr[2] = 0;
+        st->epoch += 1ull << 24;
+        st->cur_level = 0;
+        st->barrier = 0;
+        st->error = 0;
+        st->max_level = 0;
+        st->done = 0;
+        st->total_queued = 0;
+        st->finished = 0;
+        st->qe[1] = st->qe[2] = 0;
+    }
+}
+
+// Second set-up step (after the fill): the sources' labels and masks and the
+// level-0 frontier queue of the distinct source vertices (sources[] distinct,
+// with their combined source masks in src_masks[]); one thread.
+template <int DUMMY = 0>
+__global__ void msbfs_seed_kernel(BfsParams p, MsParams m, const int32_t *sources, const unsigned long long *src_masks,
+                                  int32_t n_distinct)
+{
+    if (threadIdx.x == 0) {
+        int g = 0, d = 0;
+        for (int i = 0; i < n_distinct; i++) {
+            const int v = sources[i];
+            const unsigned long long mask = src_masks[i];
+            m.visited[v] = mask;
+            m.fmask[0][v] = mask;
+            for (int s = 0; s < m.k; s++)
+                if ((mask >> s) & 1ull) m.labels[(long long)s * p.nodes + v] = 0;
+            const int r0 = p.row_offsets[v], deg = p.row_offsets[v + 1] - r0;
+            if (deg > 0) {
+                p.vf[0].v[g] = v;
+                p.vf[0].col[g] = r0;
+                p.vf[0].P[g] = d;
+                for (int c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) p.vf[0].cf[c] = g;
+                g++;
+                d += deg;
+            }
+        }
+        p.st->qe[0] = pack((unsigned)g, (unsigned)d);
+    }
+}
+
+}  // namespace dev
+}  // namespace b40c

@@ -538,6 +538,7 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->d_labels) cudaFree(p->d_labels);
     if (p->d_mask) cudaFree(p->d_mask);
     if (p->d_next) cudaFree(p->d_next);
+    free_batch(p);
     if (p->d_levels) cudaFree(p->d_levels);
     if (p->d_duty) cudaFree(p->d_duty);
     for (int i = 0; i < 2; i++) {

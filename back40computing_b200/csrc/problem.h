@@ -43,6 +43,14 @@ struct b40c_bfs_problem {
     uint32_t *d_next = nullptr;  // bottom-up discoveries of a level (direction-optimizing), kept zero between levels
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
+    // batched multi-source searches (allocated on first use)
+    unsigned long long *d_ms_visited = nullptr, *d_ms_fmask[2] = {nullptr, nullptr};
+    int32_t *d_ms_labels = nullptr;
+    int32_t ms_labels_k = 0;       // sources the label array is sized for
+    int32_t *d_ms_src = nullptr;   // [0, 64) distinct sources, [64, 128) depth limits
+    unsigned long long *d_ms_src_masks = nullptr;
+    int32_t *h_ms_stage = nullptr; // pinned staging of sources / limits / masks
+    int32_t ms_k = 0;              // sources of the last batch
     // instrumentation (per-pass records, CTA duty)
     bool instrument = false;
     b40c::LevelRecord *d_levels = nullptr;
@@ -128,6 +136,7 @@ int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode 
 int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                  int32_t depth_limit, bool direction_optimizing);
 int check_symmetric(b40c_bfs_problem *p);
+void free_batch(b40c_bfs_problem *p);
 int enact_edge(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                int32_t depth_limit);
 

@@ -209,6 +209,25 @@ int b40c_bfs_recent_search_ms(b40c_bfs_problem *problem, int count, float *out);
 /* GraphSlice device pointers (csr_problem.cuh:99-173). */
 int b40c_bfs_device_view_get(b40c_bfs_problem *problem, b40c_bfs_device_view *view);
 
+/* ---- batched multi-source search (no counterpart in the reference) ----------
+ * Up to 64 sources searched together: one pass over each level's adjacency
+ * lists serves every source (64-bit per-vertex visited / frontier masks;
+ * dense levels of a symmetric graph pull instead of push).  The labels of
+ * slot s are what a single-source search from sources[s] with
+ * depth_limits[s] produces (distances; -1 unreached or beyond the limit).
+ * depth_limits may be NULL (unlimited).  Duplicate sources are allowed.  One
+ * persistent cooperative grid, asynchronous like b40c_bfs_enact (the call
+ * itself waits for the previous batch's uploads); b40c_bfs_stats reports the
+ * deepest search as search_depth. */
+int b40c_msbfs_enact(b40c_bfs_problem *problem, const int32_t *sources, const int32_t *depth_limits, int k,
+                     int max_grid_size, const b40c_bfs_policy *policy);
+
+/* Copies slot `slot`'s labels of the last batch to the host. */
+int b40c_msbfs_extract(b40c_bfs_problem *problem, int slot, int32_t *h_labels);
+
+/* Device array int32[k][nodes] of the last batch's labels (valid until the next batch). */
+int b40c_msbfs_device_labels(b40c_bfs_problem *problem, void **d_labels, int32_t *k);
+
 /* ---- pinned host memory (CsrGraph(pinned), csr_graph.cuh:81-93) ------------ */
 int b40c_host_alloc(void **ptr, size_t bytes, int mapped);
 int b40c_host_free(void *ptr);

@@ -219,3 +219,73 @@ def test_instrumentation_records_levels():
     enactor._problem = p
     _, depth, duty = enactor.GetStatistics()
     assert depth == int(got.max()) + 1 and 0.0 < duty <= 1.0
+
+
+# ---- batched multi-source searches ------------------------------------------------------
+
+@pytest.mark.parametrize("kind,args", [("rmat", (1 << 14, 1 << 18)), ("rr", (1 << 14, 8)), ("grid2d", (90,)),
+                                       ("random", (20000, 60000))])
+def test_batched_matches_single_source(kind, args):
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g)
+    srcs = sample_sources(g, 64, seed=11)
+    p.msbfs(srcs)
+    for slot in (0, 1, 17, 63):
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+
+
+def test_batched_depth_limits_duplicates_and_small_batches():
+    g = _graph("rmat", 1 << 13, 1 << 17)
+    p = CsrProblem.from_graph(g)
+    base = sample_sources(g, 5, seed=2)
+    srcs = np.array([base[0], base[1], base[0], base[2], base[3], base[1], base[4]], np.int32)  # duplicates
+    limits = np.array([-1, 2, 3, 0, -1, -1, 1], np.int32)
+    p.msbfs(srcs, limits)
+    for slot in range(srcs.size):
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]), int(limits[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+    p.msbfs(srcs[:1])
+    want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[0]))
+    assert oracle.compare_labels(p.labels_of(0), want) == -1
+    with pytest.raises(B40cError):
+        p.labels_of(1)
+    with pytest.raises(B40cError):
+        p.msbfs(np.zeros(65, np.int32))
+
+
+def test_batched_directed_graph_push_only():
+    d = CsrGraph()
+    BuildRandomRegularishGraph(30000, 6, d, seed=3, symmetrize=False)
+    p = CsrProblem.from_graph(d)
+    srcs = np.arange(0, 64 * 400, 400, dtype=np.int32)
+    p.msbfs(srcs)
+    for slot in (0, 33, 63):
+        want, _ = oracle.bfs(d.row_offsets, d.column_indices, int(srcs[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+
+
+@pytest.mark.parametrize("alpha", [1, 1000])
+def test_batched_pull_threshold_extremes(alpha):
+    """alpha = 1: only very dense levels pull; alpha = 1000: nearly every level pulls."""
+    g = _graph("rmat", 1 << 14, 1 << 18)
+    p = CsrProblem.from_graph(g)
+    pol = N.Policy()
+    pol.bottom_up_alpha = alpha
+    srcs = sample_sources(g, 64, seed=21)
+    lim = np.where(np.arange(64) % 5 == 0, 3, -1).astype(np.int32)
+    p.msbfs(srcs, lim, policy=pol)
+    for slot in (0, 5, 31, 62):
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]), int(lim[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+
+
+def test_batch_then_single_source_on_same_problem():
+    g = _graph("rmat", 1 << 13, 1 << 16)
+    p = CsrProblem.from_graph(g)
+    srcs = sample_sources(g, 8, seed=30)
+    p.msbfs(srcs)
+    got = search(p, int(srcs[2]), strategy=DIRECTION_OPTIMIZING)
+    want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[2]))
+    assert oracle.compare_labels(got, want) == -1
+    assert oracle.compare_labels(p.labels_of(2), want) == -1
