@@ -710,6 +710,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, worked = false;
+    int solo_phase = 0;  // small-frontier phases so far (the same count in every CTA)
     DutyClock duty(p);
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
@@ -743,11 +744,13 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                     if (stop) break;
                     begin_pass<B, PRED>(p, s, pass, true);
                 }
-                if (tid == 0) p.st->cur_level = level;
+                if (tid == 0) p.st->solo_resume[solo_phase & 1] = level;
             }
             worked = true;
             if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
-            level = ld_cg(&p.st->cur_level) - 1;  // the loop increment brings it back
+            // not st->cur_level: CTA 0 may already have moved it on by the time a slow CTA reads
+            level = ld_cg(&p.st->solo_resume[solo_phase & 1]) - 1;  // the loop increment brings it back
+            solo_phase++;
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);

@@ -54,6 +54,10 @@ struct alignas(128) SearchState {
     // and block 0 writes [(k + 1) % 3]
     int32_t dir[3];            // 1: the previous level ran bottom-up
     unsigned long long visited_edges[3];  // degree sum of the vertices visited before the pass
+    // level at which a persistent launch resumes after a small-frontier phase of
+    // CTA 0, by phase parity (a slot is rewritten only two phases later, after
+    // every CTA has read it)
+    int32_t solo_resume[2];
 };
 
 __host__ __device__ inline int qe_count(unsigned long long x) { return (int)(x >> 32); }
