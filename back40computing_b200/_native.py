@@ -116,6 +116,8 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_msbfs_enact": (C.c_int, [C.c_void_p, _P_i32, _P_i32, C.c_int, C.c_int, C.POINTER(Policy)]),
     "b40c_msbfs_extract": (C.c_int, [C.c_void_p, C.c_int, _P_i32]),
     "b40c_msbfs_device_labels": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), _P_i32]),
+    "b40c_bfs_search_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_void_p,
+                                          C.c_void_p]),
     "b40c_host_alloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_size_t, C.c_int]),
     "b40c_host_free": (C.c_int, [C.c_void_p]),
     "b40c_build_grid2d": (C.c_int, [C.c_int32, C.c_int, C.POINTER(Csr)]),

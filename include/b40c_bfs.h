@@ -228,6 +228,28 @@ int b40c_msbfs_extract(b40c_bfs_problem *problem, int slot, int32_t *h_labels);
 /* Device array int32[k][nodes] of the last batch's labels (valid until the next batch). */
 int b40c_msbfs_device_labels(b40c_bfs_problem *problem, void **d_labels, int32_t *k);
 
+/* ---- search without allocation ----------------------------------------------
+ * No counterpart in the reference.  A single-source distance search for
+ * callers that cannot allocate device memory when they search -- code living
+ * inside another allocator's pool or a fixed memory budget, a device whose
+ * memory is already spoken for, or a latency-critical path where cudaMalloc /
+ * cudaFree would stall.  The caller passes the CSR (d_row_offsets[nodes + 1],
+ * d_column_indices[edges]) and the output d_labels[nodes], all device
+ * pointers it owns; the visited mask, frontier queues and search state live
+ * in a fixed scratch array built into the library (about 6.3 MB held on every
+ * device that loads it, until the process exits).  Limits: at most 262,144
+ * vertices and 4,194,304 edges; larger graphs are rejected with
+ * B40C_ERROR_INVALID_VALUE (use b40c_bfs_problem_create).  The first call on
+ * a device sets that device up (looks up the scratch's device address and
+ * the kernel's launch shape), so make it before any stream capture.  Every
+ * call shares the one scratch array: calls whose work overlaps on the GPU
+ * (different streams or threads at once) race and must be serialised by the
+ * caller.  Runs on cuda_stream (NULL: the legacy default stream) on the
+ * current device and returns when the search has finished; labels are the
+ * same as b40c_bfs_enact's expand-contract distances. */
+int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32_t *d_column_indices, int64_t nodes,
+                            int64_t edges, int32_t src, int32_t *d_labels, void *cuda_stream);
+
 /* ---- pinned host memory (CsrGraph(pinned), csr_graph.cuh:81-93) ------------ */
 int b40c_host_alloc(void **ptr, size_t bytes, int mapped);
 int b40c_host_free(void *ptr);
