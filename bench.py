@@ -44,6 +44,10 @@ CONFIGS = {
                        workload="plain single-source BFS, 2D 5-point lattice 1000x1000, source 0"),
     "grid3d256": dict(kind="grid3d", width=256,
                       workload="high-diameter BFS, 3D 7-point lattice 256^3, source = centre"),
+    "rmat20": dict(kind="rmat", scale=20, ef=16,
+                   workload="plain single-source BFS, R-MAT scale 20 edge factor 16 (small case for profiling)"),
+    "random21": dict(kind="rr", scale=21, degree=16,
+                     workload="batched BFS, 2^21 vertices x 16 uniform out-neighbours symmetrised, 64 sources"),
 }
 
 
@@ -60,6 +64,8 @@ def parse():
     ap.add_argument("--sources", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound on the CPU-baseline sample")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched (random 2^21) and lattice (grid2d-1000, grid3d-256) measurements")
     return ap.parse_args()
 
 
@@ -70,6 +76,10 @@ def build_graph(cfg_name):
     if cfg["kind"] == "rmat":
         n = 1 << cfg["scale"]
         BuildRmatGraph(n, cfg["ef"] * n, g, True, 0.57, 0.19, 0.19, seed=0, permute=True)
+        return g, None
+    if cfg["kind"] == "rr":
+        from back40computing_b200 import BuildRandomRegularishGraph
+        BuildRandomRegularishGraph(1 << cfg["scale"], cfg["degree"], g, seed=0, symmetrize=True)
         return g, None
     if cfg["kind"] == "grid2d":
         BuildGrid2dGraph(cfg["width"], g)
@@ -160,12 +170,12 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic(cfg_name):
+def profiled_traffic(cfg_name, strategy):
     """DRAM bytes per search of the dominant kernel from the committed ncu summary, if any."""
-    path = os.path.join(ROOT, "profiles", f"traffic_{cfg_name}.json")
+    path = os.path.join(ROOT, "profiles", "ec_kernel_traffic.json")
     try:
         with open(path) as f:
-            return json.load(f)
+            return json.load(f).get(f"{cfg_name}/{strategy}")
     except (OSError, ValueError):
         return None
 
@@ -242,6 +252,72 @@ def run_reference(args, rank):
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def batched_extra(steps, warmup):
+    """64-source batched search on the random 2^21 x 16 symmetrised graph against 64
+    one-at-a-time plain searches (direction-optimizing and expand-contract) on the
+    same GPU; labels of two slots are checked against the oracle."""
+    import oracle
+    from back40computing_b200 import CsrProblem, sample_sources
+    from back40computing_b200 import _native as N
+    from back40computing_b200.bfs import ENACTORS
+    g, _ = build_graph("random21")
+    deg = np.diff(g.row_offsets).astype(np.int64)
+    srcs = sample_sources(g, 64, seed=0)
+    p = CsrProblem.from_graph(g)
+    p.msbfs(srcs)
+    ec = []
+    for slot in range(64):
+        lab = p.labels_of(slot)
+        ec.append(visited(deg, lab)[1])
+        if slot in (0, 37):
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
+            if oracle.compare_labels(lab, want) != -1:
+                raise SystemExit("batched parity failure against the oracle")
+    for _ in range(warmup):
+        p.msbfs(srcs)
+    for _ in range(steps):
+        p.msbfs(srcs)
+    batch_ms = float(p.recent_search_ms(steps).mean())
+    seq = {}
+    for st in (4, 0):
+        e = ENACTORS[st]()
+        N.check(p.Reset(e.GetFrontierType(), 1.3))
+        for s in srcs:
+            N.check(e._enact(p, int(s), 0, 0))
+        seq[STRATEGY_NAMES[st]] = float(p.recent_search_ms(64).sum())
+    total = float(sum(ec))
+    best_seq = min(seq.values())
+    out = {"workload": CONFIGS["random21"]["workload"], "batch_ms": batch_ms,
+           "gteps": total / (batch_ms * 1e-3) / 1e9, "queries_per_s": 64 / (batch_ms * 1e-3),
+           "sequential_ms": seq, "speedup_vs_best_sequential": best_seq / batch_ms}
+    p.Destroy()
+    return out
+
+
+def lattice_extra():
+    """grid2d-1000 from the corner and grid3d-256 from the centre: the persistent grid,
+    the whole-search CUDA graph and per-level launches."""
+    from back40computing_b200 import CsrProblem
+    from back40computing_b200 import _native as N
+    from back40computing_b200.bfs import ENACTORS
+    out = {}
+    for name in ("grid2d1000", "grid3d256"):
+        g, srcs = build_graph(name)
+        ec = int(g.edges)  # lattices are connected: every edge is reached
+        p = CsrProblem.from_graph(g)
+        e = ENACTORS[0]()
+        N.check(p.Reset(e.GetFrontierType(), 1.3))
+        res = {}
+        for mode, mname in ((0, "fused persistent"), (2, "cuda graph"), (1, "per-level launches")):
+            for _ in range(2):
+                N.check(e._enact(p, int(srcs[0]), mode, 0))
+            ms = float(p.recent_search_ms(1)[0])
+            res[mname] = {"ms": ms, "gteps": ec / (ms * 1e-3) / 1e9}
+        out[name] = res
+        p.Destroy()
+    return out
 
 
 def main():
@@ -348,10 +424,15 @@ def main():
         tk = problem.recent_search_ms(len(srcs))
         topdown = {"gteps": float(ec.sum() / (tk.sum() * 1e-3) / 1e9), "kernel_ms_per_search": float(tk.mean())}
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["batched"] = batched_extra(max(args.steps, 3), args.warmup)
+        extras["lattices"] = lattice_extra()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(g, srcs, deg, args.cpu_seconds)
-    traffic = profiled_traffic(args.config)
+    traffic = profiled_traffic(args.config, STRATEGY_NAMES[args.strategy])
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
@@ -372,6 +453,7 @@ def main():
             "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": 2 * len(srcs) * args.steps,
             "clocks": clk,
+            **extras,
             "edges_per_search": float(ec.mean()), "search_gteps_mean": float((ec / 1e9).mean()
                                                                               / (kernel_ms.mean() * 1e-3)),
         }
