@@ -32,19 +32,24 @@ int launch_init(b40c_bfs_problem *p, const BfsParams &k, bool vertex_frontier, b
     return B40C_SUCCESS;
 }
 
-// Common start of an enact: uploads (source, depth limit) and records the
-// enact's start event.
+// Common start of an enact: stores (source, depth limit) in this enact's
+// pinned ring slot and records the enact's start event.  The slot was last
+// used kRing enacts ago; its search (and so its upload) must have finished
+// before the pair is overwritten.
 inline int begin_enact(b40c_bfs_problem *p, int32_t src, int32_t depth_limit)
 {
-    p->h_st->src = src;
-    p->h_st->depth_limit = depth_limit;
+    const int slot = p->ring_pos;
+    if (p->ring_count == b40c_bfs_problem::kRing)
+        CUDA_TRY(cudaEventSynchronize(p->ring_b[slot]), "source slot reuse wait");
+    p->h_src_ring[2 * slot] = src;
+    p->h_src_ring[2 * slot + 1] = depth_limit;
     CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
     return B40C_SUCCESS;
 }
 
 inline int upload_source(b40c_bfs_problem *p)
 {
-    CUDA_TRY(cudaMemcpyAsync(&p->st->src, &p->h_st->src, 2 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
+    CUDA_TRY(cudaMemcpyAsync(&p->st->src, source_slot(p), 2 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
              "source upload");
     return B40C_SUCCESS;
 }

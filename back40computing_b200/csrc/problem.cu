@@ -296,31 +296,31 @@ int begin_instrumented(b40c_bfs_problem *p)
 
 void free_graphs(b40c_bfs_problem *p)
 {
-    for (int s = 0; s < 5; s++)
-        if (p->graph_exec[s]) {
-            cudaGraphExecDestroy(p->graph_exec[s]);
-            p->graph_exec[s] = nullptr;
-        }
+    for (int s = 0; s < 5; s++) {
+        if (p->graph_exec[s]) cudaGraphExecDestroy(p->graph_exec[s]);
+        if (p->graph_def[s]) cudaGraphDestroy(p->graph_def[s]);
+        p->graph_exec[s] = nullptr;
+        p->graph_def[s] = nullptr;
+        p->graph_copy_node[s] = nullptr;
+    }
 }
 
 int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode *body, int n_body)
 {
     if (!p->graph_exec[slot] || memcmp(&p->graph_params[slot], &body[0].params, sizeof(BfsParams)) != 0 ||
         p->graph_grid[slot] != (int)body[0].grid.x) {
-        if (p->graph_exec[slot]) {
-            cudaGraphExecDestroy(p->graph_exec[slot]);
-            p->graph_exec[slot] = nullptr;
-        }
+        if (p->graph_exec[slot]) cudaGraphExecDestroy(p->graph_exec[slot]);
+        if (p->graph_def[slot]) cudaGraphDestroy(p->graph_def[slot]);
+        p->graph_exec[slot] = nullptr;
+        p->graph_def[slot] = nullptr;
         cudaGraph_t g = nullptr;
         CUDA_TRY(cudaGraphCreate(&g, 0), "cudaGraphCreate");
-        struct GraphHolder {
-            cudaGraph_t g;
-            ~GraphHolder() { cudaGraphDestroy(g); }
-        } holder{g};
+        p->graph_def[slot] = g;  // owned by the handle from here on (free_graphs)
         cudaGraphNode_t n_copy, n_init, n_loop;
-        CUDA_TRY(cudaGraphAddMemcpyNode1D(&n_copy, g, nullptr, 0, &p->st->src, &p->h_st->src, 2 * sizeof(int32_t),
+        CUDA_TRY(cudaGraphAddMemcpyNode1D(&n_copy, g, nullptr, 0, &p->st->src, source_slot(p), 2 * sizeof(int32_t),
                                           cudaMemcpyHostToDevice),
                  "graph memcpy node");
+        p->graph_copy_node[slot] = n_copy;
         BfsParams init_params = init.params;
         void *init_args[] = {&init_params};
         cudaKernelNodeParams kp = {};
@@ -358,6 +358,11 @@ int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode 
         CUDA_TRY(cudaGraphInstantiate(&p->graph_exec[slot], g, 0), "cudaGraphInstantiate");
         p->graph_params[slot] = body[0].params;
         p->graph_grid[slot] = (int)body[0].grid.x;
+    } else {
+        // this launch's source pair lives in its own ring slot
+        CUDA_TRY(cudaGraphExecMemcpyNodeSetParams1D(p->graph_exec[slot], p->graph_copy_node[slot], &p->st->src,
+                                                    source_slot(p), 2 * sizeof(int32_t), cudaMemcpyHostToDevice),
+                 "graph source re-point");
     }
     CUDA_TRY(cudaGraphLaunch(p->graph_exec[slot], p->stream), "cudaGraphLaunch");
     return B40C_SUCCESS;
@@ -513,6 +518,11 @@ int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t no
         return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "state allocation failed"));
     }
     memset(p->h_st, 0, sizeof(SearchState));
+    if (cudaMallocHost((void **)&p->h_src_ring, 2 * sizeof(int32_t) * b40c_bfs_problem::kRing) != cudaSuccess) {
+        cudaGetLastError();
+        p->h_src_ring = nullptr;
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "pinned source ring allocation failed"));
+    }
     if ((rc = ensure_slots(p))) return bail(rc);
     if (cudaStreamSynchronize(p->stream) != cudaSuccess) {
         cudaError_t e = cudaGetLastError();
@@ -548,6 +558,7 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->slots) cudaFree(p->slots);
     if (p->st) cudaFree(p->st);
     if (p->h_st) cudaFreeHost(p->h_st);
+    if (p->h_src_ring) cudaFreeHost(p->h_src_ring);
     if (p->ev0) cudaEventDestroy(p->ev0);
     if (p->ev1) cudaEventDestroy(p->ev1);
     for (int i = 0; i < b40c_bfs_problem::kRing; i++) {

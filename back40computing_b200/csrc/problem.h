@@ -65,6 +65,10 @@ struct b40c_bfs_problem {
     int32_t max_slots = 0;
     b40c::SearchState *st = nullptr;
     b40c::SearchState *h_st = nullptr;  // pinned mirror
+    // pinned (source, depth limit) of each enact, one pair per timing-ring slot:
+    // an enact's upload reads its own pair, so enacts queued back to back
+    // never see a later call's source
+    int32_t *h_src_ring = nullptr;
     // streams / timing
     cudaStream_t stream = nullptr, own_stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -78,6 +82,8 @@ struct b40c_bfs_problem {
     // CUDA graphs of whole searches (ENACT_GRAPH), one per strategy, rebuilt
     // when the kernel parameters (buffers, policy) or the grid change
     cudaGraphExec_t graph_exec[5] = {};
+    cudaGraph_t graph_def[5] = {};           // kept for re-pointing the source copy per launch
+    cudaGraphNode_t graph_copy_node[5] = {};  // the source-upload memcpy node of each graph
     b40c::BfsParams graph_params[5] = {};
     int graph_grid[5] = {};
 };
@@ -101,6 +107,9 @@ struct DeviceGuard {
         if (prev >= 0 && cur != prev) cudaSetDevice(prev);
     }
 };
+
+// The pinned (source, depth limit) pair of the enact being issued.
+inline const int32_t *source_slot(const b40c_bfs_problem *p) { return p->h_src_ring + 2 * p->ring_pos; }
 
 int alloc_dev(void **p, size_t bytes, const char *what);
 void free_vf(VertexFrontier &f);

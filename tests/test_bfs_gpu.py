@@ -289,3 +289,50 @@ def test_batch_then_single_source_on_same_problem():
     want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[2]))
     assert oracle.compare_labels(got, want) == -1
     assert oracle.compare_labels(p.labels_of(2), want) == -1
+
+
+@pytest.mark.parametrize("strategy", [EXPAND_CONTRACT, DIRECTION_OPTIMIZING, CONTRACT_EXPAND])
+@pytest.mark.parametrize("mode", [N.ENACT_FUSED, N.ENACT_GRAPH])
+def test_queued_enacts_keep_their_sources(strategy, mode):
+    """Enacts are asynchronous: three searches queued back to back (a long path
+    search, the same long search, then a search from an isolated vertex) must
+    each run from their own source, even though the host returns long before
+    the GPU reaches the second one."""
+    L = 6000
+    ro = np.zeros(L + 2, np.int32)
+    deg = np.full(L, 2, np.int32)
+    deg[0] = deg[-1] = 1
+    ro[1:L + 1] = np.cumsum(deg)
+    ro[L + 1] = ro[L]
+    ci = np.empty(ro[L], np.int32)
+    for v in range(L):
+        nb = [u for u in (v - 1, v + 1) if 0 <= u < L]
+        ci[ro[v]:ro[v] + len(nb)] = nb
+    g = CsrGraph.from_arrays(ro, ci)
+    p = CsrProblem.from_graph(g)
+    e = ENACTORS[strategy]()
+    N.check(p.Reset(e.GetFrontierType(), 1.3))
+    N.check(e._enact(p, 0, mode, 0))  # warm-up (graph build, symmetry check)
+    p.labels()
+    for s in (0, 0, L):
+        N.check(e._enact(p, s, mode, 0))
+    t = p.recent_search_ms(3)
+    got = p.labels()
+    want = np.full(L + 1, -1, np.int32)
+    want[L] = 0
+    assert oracle.compare_labels(got, want) == -1
+    assert t[1] > 5 * t[2], f"second queued search ran short ({t}): it did not search from its own source"
+    assert t[1] > 0.5 * t[0], t
+
+
+def test_many_queued_enacts_wrap_the_source_ring():
+    """More queued enacts than the per-handle ring of source slots (256)."""
+    g = _graph("rmat", 1 << 12, 1 << 15)
+    p = CsrProblem.from_graph(g)
+    e = ENACTORS[DIRECTION_OPTIMIZING]()
+    N.check(p.Reset(e.GetFrontierType(), 1.3))
+    srcs = sample_sources(g, 7, seed=3)
+    for i in range(300):
+        N.check(e._enact(p, int(srcs[i % 7]), N.ENACT_FUSED, 0))
+    want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[299 % 7]))
+    assert oracle.compare_labels(p.labels(), want) == -1
