@@ -80,6 +80,51 @@ class Csr(C.Structure):
     ]
 
 
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("memory_budget_bytes", C.c_int64),
+        ("max_batch", C.c_int32),
+        ("single_strategy", C.c_int32),
+        ("max_in_flight", C.c_int32),
+        ("reserved", C.c_int32 * 5),
+    ]
+
+
+class ServerResult(C.Structure):
+    _fields_ = [
+        ("ticket", C.c_int64),
+        ("graph", C.c_int32),
+        ("source", C.c_int32),
+        ("depth_limit", C.c_int32),
+        ("status", C.c_int32),
+        ("search_depth", C.c_int32),
+        ("batch_size", C.c_int32),
+        ("arrival_ns", C.c_int64),
+        ("launch_ns", C.c_int64),
+        ("finish_ns", C.c_int64),
+    ]
+
+
+SERVER_RESULT_DTYPE = np.dtype([("ticket", "<i8"), ("graph", "<i4"), ("source", "<i4"), ("depth_limit", "<i4"),
+                                ("status", "<i4"), ("search_depth", "<i4"), ("batch_size", "<i4"),
+                                ("arrival_ns", "<i8"), ("launch_ns", "<i8"), ("finish_ns", "<i8")])
+
+
+class ServerCounters(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_int64),
+        ("completed", C.c_int64),
+        ("failed", C.c_int64),
+        ("batches", C.c_int64),
+        ("batched_queries", C.c_int64),
+        ("single_queries", C.c_int64),
+        ("memory_used_bytes", C.c_int64),
+        ("memory_budget_bytes", C.c_int64),
+        ("graphs", C.c_int32),
+        ("reserved", C.c_int32 * 3),
+    ]
+
+
 class B40cError(RuntimeError):
     """A non-zero status from the library; ``.status`` is the cudaError_t value."""
 
@@ -91,7 +136,7 @@ class B40cError(RuntimeError):
 _P_i32 = C.POINTER(C.c_int32)
 _P_i64 = C.POINTER(C.c_int64)
 
-# name -> (restype, argtypes); every symbol declared in include/b40c_bfs.h
+# name -> (restype, argtypes); every symbol declared in include/b40c_bfs.h and include/b40c_server.h
 SIGNATURES: dict[str, tuple] = {
     "b40c_last_error_string": (C.c_char_p, []),
     "b40c_version": (C.c_char_p, []),
@@ -115,6 +160,8 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
     "b40c_msbfs_enact": (C.c_int, [C.c_void_p, _P_i32, _P_i32, C.c_int, C.c_int, C.POINTER(Policy)]),
     "b40c_msbfs_extract": (C.c_int, [C.c_void_p, C.c_int, _P_i32]),
+    "b40c_msbfs_stats": (C.c_int, [C.c_void_p, _P_i32]),
+    "b40c_bfs_problem_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "b40c_msbfs_device_labels": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), _P_i32]),
     "b40c_bfs_search_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_int32, C.c_void_p,
                                           C.c_void_p]),
@@ -129,6 +176,21 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_csr_from_coo": (C.c_int, [_P_i32, _P_i32, C.c_int64, C.c_int64, C.c_int, C.POINTER(Csr)]),
     "b40c_sample_sources": (C.c_int, [C.POINTER(Csr), C.c_int32, C.c_uint64, _P_i32]),
     "b40c_graph_free": (None, [C.POINTER(Csr)]),
+    # include/b40c_server.h
+    "b40c_server_create": (C.c_int, [C.c_int, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "b40c_server_destroy": (C.c_int, [C.c_void_p]),
+    "b40c_server_add_graph": (C.c_int, [C.c_void_p, _P_i32, _P_i32, C.c_int64, C.c_int64, _P_i32]),
+    "b40c_server_remove_graph": (C.c_int, [C.c_void_p, C.c_int32]),
+    "b40c_server_graph_info": (C.c_int, [C.c_void_p, C.c_int32, _P_i64, _P_i32]),
+    "b40c_server_plan_bytes": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, _P_i64]),
+    "b40c_server_now_ns": (C.c_int, [C.c_void_p, _P_i64]),
+    "b40c_server_submit": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, _P_i64]),
+    "b40c_server_submit_many": (C.c_int, [C.c_void_p, C.c_int64, _P_i32, _P_i32, _P_i32, _P_i64, _P_i64]),
+    "b40c_server_result_get": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ServerResult)]),
+    "b40c_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.POINTER(ServerResult)]),
+    "b40c_server_drain": (C.c_int, [C.c_void_p]),
+    "b40c_server_results": (C.c_int, [C.c_void_p, C.c_int64, C.c_int64, C.c_void_p]),
+    "b40c_server_counters_get": (C.c_int, [C.c_void_p, C.POINTER(ServerCounters)]),
 }
 
 _lib = None

@@ -50,6 +50,7 @@ class CsrProblem:
         self.num_gpus = 0
         self._h = C.c_void_p(None)
         self._keep = None  # host arrays kept alive for stream-from-host
+        self._ms_k = 0     # sources of the last batch
 
     # csr_problem.cuh:328-540
     def FromHostProblem(self, stream_from_host: bool, nodes: int, edges: int, column_indices, row_offsets,
@@ -133,12 +134,19 @@ class CsrProblem:
         pol = C.byref(policy) if policy is not None else None
         N.check(N.lib().b40c_msbfs_enact(self.handle, N.i32p(src), N.i32p(lim) if lim is not None else None,
                                          int(src.size), int(max_grid_size), pol), "msbfs")
+        self._ms_k = int(src.size)
 
     def labels_of(self, slot: int) -> np.ndarray:
         """Labels of source `slot` of the last batch."""
         out = np.empty(self.nodes, dtype=np.int32)
         N.check(N.lib().b40c_msbfs_extract(self.handle, int(slot), N.i32p(out)), "msbfs_extract")
         return out
+
+    def msbfs_depths(self) -> np.ndarray:
+        """Search depth (max label + 1) of every slot of the last batch."""
+        out = np.empty(64, dtype=np.int32)
+        N.check(N.lib().b40c_msbfs_stats(self.handle, N.i32p(out)), "msbfs_stats")
+        return out[:self._ms_k]
 
     def is_symmetric(self) -> bool:
         out = C.c_int32(0)

@@ -17,18 +17,14 @@ void free_batch(b40c_bfs_problem *p)
         if (p->d_ms_fmask[i]) cudaFree(p->d_ms_fmask[i]);
     if (p->d_ms_labels) cudaFree(p->d_ms_labels);
     if (p->d_ms_src) cudaFree(p->d_ms_src);
-    if (p->d_ms_src_masks) cudaFree(p->d_ms_src_masks);
-    if (p->h_ms_stage) cudaFreeHost(p->h_ms_stage);
+    if (p->d_ms_depth) cudaFree(p->d_ms_depth);
     p->d_ms_visited = nullptr;
     p->d_ms_fmask[0] = p->d_ms_fmask[1] = nullptr;
     p->d_ms_labels = nullptr;
     p->d_ms_src = nullptr;
-    p->d_ms_src_masks = nullptr;
-    p->h_ms_stage = nullptr;
+    p->d_ms_depth = nullptr;
     p->ms_labels_k = 0;
 }
-
-namespace {
 
 int ensure_batch(b40c_bfs_problem *p, int k)
 {
@@ -39,14 +35,8 @@ int ensure_batch(b40c_bfs_problem *p, int k)
         for (int i = 0; i < 2; i++)
             if ((rc = alloc_dev((void **)&p->d_ms_fmask[i], sizeof(unsigned long long) * n, "batch frontier masks")))
                 return rc;
-        if ((rc = alloc_dev((void **)&p->d_ms_src, sizeof(int32_t) * 128, "batch sources"))) return rc;
-        if ((rc = alloc_dev((void **)&p->d_ms_src_masks, sizeof(unsigned long long) * 64, "batch masks"))) return rc;
-        if (cudaMallocHost((void **)&p->h_ms_stage, 128 * sizeof(int32_t) + 64 * sizeof(unsigned long long)) !=
-            cudaSuccess) {
-            cudaGetLastError();
-            p->h_ms_stage = nullptr;
-            return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "pinned batch staging failed");
-        }
+        if ((rc = alloc_dev((void **)&p->d_ms_src, sizeof(int32_t) * 64, "batch depth limits"))) return rc;
+        if ((rc = alloc_dev((void **)&p->d_ms_depth, sizeof(int32_t) * 64, "batch search depths"))) return rc;
     }
     if (p->ms_labels_k < k) {
         if (p->d_ms_labels) cudaFree(p->d_ms_labels);
@@ -67,9 +57,9 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     if ((rc = ensure_slots(p))) return rc;
     if ((rc = ensure_batch(p, k))) return rc;
     if ((rc = check_symmetric(p))) return rc;
-    // the previous batch's staging buffer may still be read by an in-flight copy
-    CUDA_TRY(cudaStreamSynchronize(p->stream), "stream synchronize");
-    // distinct source vertices with their combined source masks
+    // distinct source vertices with their combined source masks; they travel
+    // to the device as kernel arguments, so nothing on the host is reused
+    // while an earlier batch is still queued
     std::vector<std::pair<int32_t, unsigned long long>> ds;
     for (int s = 0; s < k; s++) ds.push_back({sources[s], 1ull << s});
     std::sort(ds.begin(), ds.end());
@@ -80,14 +70,13 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
         else
             ds[nd++] = ds[i];
     }
-    int32_t *h_src = p->h_ms_stage;
-    int32_t *h_lim = p->h_ms_stage + 64;
-    unsigned long long *h_mask = (unsigned long long *)(p->h_ms_stage + 128);
+    dev::MsSeed seed{};
     for (int i = 0; i < nd; i++) {
-        h_src[i] = ds[i].first;
-        h_mask[i] = ds[i].second;
+        seed.src[i] = ds[i].first;
+        seed.mask[i] = ds[i].second;
     }
-    for (int s = 0; s < k; s++) h_lim[s] = limits ? limits[s] : -1;
+    for (int s = 0; s < k; s++) seed.limit[s] = limits ? limits[s] : -1;
+    seed.n_distinct = nd;
 
     BfsParams bp = make_params(p, pol);
     dev::MsParams m{};
@@ -95,7 +84,8 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     m.fmask[0] = p->d_ms_fmask[0];
     m.fmask[1] = p->d_ms_fmask[1];
     m.labels = p->d_ms_labels;
-    m.depth_limit = p->d_ms_src + 64;
+    m.depth_limit = p->d_ms_src;
+    m.depth = p->d_ms_depth;
     m.k = k;
     m.pull_ok = p->symmetric == 1 ? 1 : 0;
     const void *kern = (const void *)dev::msbfs_kernel<kThreads>;
@@ -104,15 +94,10 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
     if ((rc = begin_instrumented(p))) return rc;
-    CUDA_TRY(cudaMemcpyAsync(p->d_ms_src, h_src, 128 * sizeof(int32_t), cudaMemcpyHostToDevice, p->stream),
-             "batch source upload");
-    CUDA_TRY(cudaMemcpyAsync(p->d_ms_src_masks, h_mask, 64 * sizeof(unsigned long long), cudaMemcpyHostToDevice,
-                             p->stream),
-             "batch mask upload");
     const int init_blocks = std::max(1, std::min<int>(p->sms * 8, (int)(((long long)p->nodes * k + 255) / 256)));
     dev::msbfs_init_kernel<<<init_blocks, kThreads, 0, p->stream>>>(bp, m);
     CUDA_TRY(cudaGetLastError(), "batch init launch");
-    dev::msbfs_seed_kernel<<<1, 32, 0, p->stream>>>(bp, m, p->d_ms_src, p->d_ms_src_masks, nd);
+    dev::msbfs_seed_kernel<<<1, 32, 0, p->stream>>>(bp, m, p->d_ms_src, seed);
     CUDA_TRY(cudaGetLastError(), "batch seed launch");
     if ((rc = mark_search_start(p))) return rc;
     void *args[] = {&bp, &m};
@@ -123,7 +108,6 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     return finish_timing(p);
 }
 
-}  // namespace
 }  // namespace rt
 }  // namespace b40c
 
@@ -161,6 +145,22 @@ int b40c_msbfs_extract(b40c_bfs_problem *p, int slot, int32_t *h_labels)
                              cudaMemcpyDeviceToHost, p->stream),
              "batch label copy");
     CUDA_TRY(cudaStreamSynchronize(p->stream), "batch label copy synchronize");
+    return B40C_SUCCESS;
+}
+
+int b40c_msbfs_stats(b40c_bfs_problem *p, int32_t *search_depths)
+{
+    b40c::clear_error();
+    if (!p || !search_depths) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    if (p->ms_k < 1) return b40c::fail(B40C_ERROR_NOT_READY, "no batch has run");
+    DeviceGuard guard(p->device);
+    int rc = read_state(p);
+    if (rc) return rc;
+    if ((rc = check_state_errors(p))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(search_depths, p->d_ms_depth, sizeof(int32_t) * p->ms_k, cudaMemcpyDeviceToHost,
+                             p->stream),
+             "batch depth copy");
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "batch depth copy synchronize");
     return B40C_SUCCESS;
 }
 

@@ -31,6 +31,7 @@ struct MsParams {
     unsigned long long *fmask[2];    // F[2][n]
     int32_t *labels;                 // [k][n], source-major
     const int32_t *depth_limit;      // [k]; < 0 unlimited
+    int32_t *depth;                  // [k]; search depth of each source (max label + 1)
     int32_t k;
     int32_t pull_ok;                 // 1: the graph is symmetric, dense levels may pull
 };
@@ -47,6 +48,7 @@ struct MsSmem {
     int32_t flag;
     int32_t q, E;
     unsigned long long active;
+    unsigned long long found;        // sources that reached a vertex this level
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -55,7 +57,7 @@ struct MsSmem {
 template <int B>
 __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
                                                 const VertexFrontier &in, const VertexFrontier &vout,
-                                                unsigned long long *qe_out)
+                                                unsigned long long *qe_out, unsigned long long &found)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     const int q = s.q, E = s.E;
@@ -141,6 +143,7 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
 #pragma unroll
         for (int t = 0; t < PER; t++) {
             first[t] = false;
+            found |= set[t];
             if (set[t]) {
                 unsigned long long bits = set[t];
                 while (bits) {
@@ -192,7 +195,8 @@ constexpr int kPullLongList = 256;
 
 template <int B>
 __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
-                                              const VertexFrontier &vout, unsigned long long *qe_out)
+                                              const VertexFrontier &vout, unsigned long long *qe_out,
+                                              unsigned long long &found)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr int PER = kChunkMax / B;
@@ -251,8 +255,8 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
                 }
                 if (lane == owner) acc = a;
             }
-            const bool found = acc != 0;
-            if (found) {
+            found |= acc;
+            if (acc) {
                 m.visited[v] = vold | acc;
                 fnext[v] = acc;
                 s.flag = 1;
@@ -266,7 +270,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
                 wor &= wor - 1;
                 if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1;
             }
-            const bool push = found && r1 > r0;
+            const bool push = acc && r1 > r0;
             const unsigned bal = __ballot_sync(0xffffffffu, push);
             if (bal) {
                 const int leader = __ffs(bal) - 1;
@@ -307,6 +311,7 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             s.q = qe_count(x);
             s.E = qe_edges(x);
             s.flag = 0;
+            s.found = 0;
             unsigned long long act = 0;
             for (int src = 0; src < m.k; src++)
                 if (s.limits[src] < 0 || level < s.limits[src]) act |= 1ull << src;
@@ -331,12 +336,28 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
         // pull when the frontier's edges are a large share of the graph (symmetric graphs)
         const bool pull = m.pull_ok && (long long)s.E * p.bu_alpha > (long long)p.edges;
         if (tid == 0 && blockIdx.x == 0 && pull && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
+        unsigned long long found = 0;
         if (pull)
-            ms_pull_range<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+            ms_pull_range<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], found);
         else
-            ms_expand_range<B>(p, m, s, level, p.vf[level & 1], p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+            ms_expand_range<B>(p, m, s, level, p.vf[level & 1], p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3],
+                               found);
+        {
+            const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)(found & 0xffffffffull));
+            const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(found >> 32));
+            if ((tid & 31) == 0 && (lo | hi)) atomicOr(&s.found, ((unsigned long long)hi << 32) | lo);
+        }
         __syncthreads();
         if (s.flag) max_level_seen = level + 1;
+        if (tid == 0) {
+            // sources that labelled a vertex level + 1 have search depth >= level + 2
+            unsigned long long bits = s.found;
+            while (bits) {
+                const int src = __ffsll((long long)bits) - 1;
+                bits &= bits - 1;
+                atomicMax(m.depth + src, level + 2);
+            }
+        }
         if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
         // clear this level's frontier masks (the queue lists every vertex with edges that has one)
         {
@@ -379,18 +400,29 @@ __global__ void msbfs_init_kernel(BfsParams p, MsParams m)
     }
 }
 
-// Second set-up step (after the fill): the sources' labels and masks and the
-// level-0 frontier queue of the distinct source vertices (sources[] distinct,
-// with their combined source masks in src_masks[]); one thread.
+// The batch's sources, passed by value to the seed kernel (no host staging).
+struct MsSeed {
+    int32_t src[64];               // distinct source vertices
+    unsigned long long mask[64];   // combined source mask of each distinct vertex
+    int32_t limit[64];             // depth limit of each source slot (< 0 unlimited)
+    int32_t n_distinct;
+};
+
+// Second set-up step (after the fill): the depth limits, the sources' labels,
+// masks and search depths, and the level-0 frontier queue of the distinct
+// source vertices; one thread.
 template <int DUMMY = 0>
-__global__ void msbfs_seed_kernel(BfsParams p, MsParams m, const int32_t *sources, const unsigned long long *src_masks,
-                                  int32_t n_distinct)
+__global__ void msbfs_seed_kernel(BfsParams p, MsParams m, int32_t *limits_out, MsSeed seed)
 {
     if (threadIdx.x == 0) {
+        for (int s = 0; s < m.k; s++) {
+            limits_out[s] = seed.limit[s];
+            m.depth[s] = 1;
+        }
         int g = 0, d = 0;
-        for (int i = 0; i < n_distinct; i++) {
-            const int v = sources[i];
-            const unsigned long long mask = src_masks[i];
+        for (int i = 0; i < seed.n_distinct; i++) {
+            const int v = seed.src[i];
+            const unsigned long long mask = seed.mask[i];
             m.visited[v] = mask;
             m.fmask[0][v] = mask;
             for (int s = 0; s < m.k; s++)

@@ -186,6 +186,50 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     return B40C_SUCCESS;
 }
 
+// Device bytes a handle holds right now (the sizes its allocations asked
+// for; alloc_dev asks for at least 16 bytes).
+int64_t device_bytes(const b40c_bfs_problem *p)
+{
+    auto a = [](int64_t b) { return std::max<int64_t>(b, 16); };
+    const int64_t n = p->nodes, m = p->edges;
+    int64_t t = 0;
+    if (p->own_csr && p->d_ro) t += a(4 * (n + 1)) + a(4 * std::max<int64_t>(m, 1));
+    if (p->d_labels) t += a(4 * n);
+    const int64_t mask = a(4 * ((int64_t)(p->mask_words + 63) / 64 * 64));
+    if (p->d_mask) t += mask;
+    if (p->d_next) t += mask;
+    if (p->st) t += a(sizeof(SearchState));
+    if (p->slots) t += a((int64_t)sizeof(dev::LookbackSlot) * p->max_slots);
+    const int64_t cf_len = (std::max<int64_t>(m, 1) + dev::kChunkGrain - 1) / dev::kChunkGrain + 2;
+    for (int i = 0; i < 2; i++) {
+        if (p->vcap[i]) t += 2 * a(4 * p->vcap[i]) + a(4 * (p->vcap[i] + 1)) + a(4 * cf_len);
+        if (p->ecap[i]) t += a(4 * p->ecap[i]) * (p->ef[i].pred ? 2 : 1);
+    }
+    if (p->d_ms_visited) t += 3 * a(8 * n) + 2 * a(4 * 64);
+    if (p->d_ms_labels) t += a(4 * n * (int64_t)p->ms_labels_k);
+    if (p->d_levels) t += a((int64_t)sizeof(LevelRecord) * kMaxLevelRecords);
+    if (p->d_duty) t += a(4 * sizeof(unsigned long long));
+    return t;
+}
+
+// What a handle built from a host CSR (copied to the device) holds after a
+// batched search of width k and a single-source vertex-frontier search with
+// queue sizing qs: device_bytes() of that handle, computed without one.
+int64_t planned_bytes(int64_t n, int64_t m, int k, double qs)
+{
+    auto a = [](int64_t b) { return std::max<int64_t>(b, 16); };
+    const int64_t mask_words = (n + 31) / 32;
+    const int64_t mask = a(4 * ((mask_words + 63) / 64 * 64));
+    const int64_t slots = (std::max(m, n) + 255) / 256 + 4096;
+    const int64_t cap = std::max<int64_t>(cap_of(qs, n), 1);
+    const int64_t cf_len = (std::max<int64_t>(m, 1) + dev::kChunkGrain - 1) / dev::kChunkGrain + 2;
+    int64_t t = a(4 * (n + 1)) + a(4 * std::max<int64_t>(m, 1));
+    t += a(4 * n) + 2 * mask + a(sizeof(SearchState)) + a((int64_t)sizeof(dev::LookbackSlot) * slots);
+    t += 2 * (2 * a(4 * cap) + a(4 * (cap + 1)) + a(4 * cf_len));
+    if (k > 0) t += 3 * a(8 * n) + 2 * a(4 * 64) + a(4 * n * (int64_t)k);
+    return t;
+}
+
 // Reads the device state into the pinned mirror (synchronous).
 int read_state(b40c_bfs_problem *p)
 {
@@ -568,6 +612,14 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->own_stream) cudaStreamDestroy(p->own_stream);
     cudaGetLastError();
     delete p;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_problem_device_bytes(b40c_bfs_problem *p, int64_t *bytes)
+{
+    b40c::clear_error();
+    if (!p || !bytes) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    *bytes = device_bytes(p);
     return B40C_SUCCESS;
 }
 

@@ -47,9 +47,8 @@ struct b40c_bfs_problem {
     unsigned long long *d_ms_visited = nullptr, *d_ms_fmask[2] = {nullptr, nullptr};
     int32_t *d_ms_labels = nullptr;
     int32_t ms_labels_k = 0;       // sources the label array is sized for
-    int32_t *d_ms_src = nullptr;   // [0, 64) distinct sources, [64, 128) depth limits
-    unsigned long long *d_ms_src_masks = nullptr;
-    int32_t *h_ms_stage = nullptr; // pinned staging of sources / limits / masks
+    int32_t *d_ms_src = nullptr;   // [64] depth limit of each source slot
+    int32_t *d_ms_depth = nullptr; // [64] search depth of each source slot
     int32_t ms_k = 0;              // sources of the last batch
     // instrumentation (per-pass records, CTA duty)
     bool instrument = false;
@@ -117,6 +116,8 @@ void free_ef(EdgeFrontier &f);
 int ensure_vf(b40c_bfs_problem *p, int i, int64_t cap);
 int ensure_ef(b40c_bfs_problem *p, int i, int64_t cap);
 int64_t cap_of(double qs, int64_t base);
+int64_t device_bytes(const b40c_bfs_problem *p);
+int64_t planned_bytes(int64_t n, int64_t m, int k, double qs);
 int ensure_slots(b40c_bfs_problem *p);
 BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol);
 b40c_bfs_policy default_policy(int strategy);
@@ -146,6 +147,10 @@ int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const
                  int32_t depth_limit, bool direction_optimizing);
 int check_symmetric(b40c_bfs_problem *p);
 void free_batch(b40c_bfs_problem *p);
+int ensure_batch(b40c_bfs_problem *p, int k);
+// Queues a batched search of k <= 64 sources on p->stream (asynchronous).
+int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limits, int k, int max_grid,
+                const b40c_bfs_policy &pol);
 int enact_edge(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                int32_t depth_limit);
 

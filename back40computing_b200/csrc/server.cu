@@ -1,0 +1,645 @@
+// BFS query server: resident graphs, continuous batching, a device-memory
+// budget (include/b40c_server.h).
+//
+// One dispatcher thread owns all GPU work of a server.  Its loop:
+//   1. queries whose arrival time has come move from the arrival heap to their
+//      graph's FIFO;
+//   2. finished batches are retired in issue order (one CUDA stream, so they
+//      finish in that order): results, latencies, labels already copied;
+//   3. while fewer than max_in_flight batches are queued and some graph with
+//      waiting queries has no batch in flight, the graph whose oldest waiting
+//      query arrived first gets a batch of up to its width: the batched kernel
+//      for two or more queries, the plain search for one;
+//   4. it spins (yielding) while batches are in flight, otherwise sleeps until
+//      the next arrival or a submit.
+// Queries for a graph that already has a batch in flight wait and gather into
+// its next batch: that is the continuous batching.
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <queue>
+#include <thread>
+#include <vector>
+
+#include "b40c_server.h"
+#include "problem.h"
+
+extern "C" int b40c_bfs_enact_limited(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int32_t depth_limit,
+                                      int max_grid_size, const b40c_bfs_policy *policy);
+extern "C" int b40c_msbfs_enact(b40c_bfs_problem *p, const int32_t *sources, const int32_t *depth_limits, int k,
+                                int max_grid_size, const b40c_bfs_policy *policy);
+extern "C" int b40c_bfs_problem_create(const int32_t *row_offsets, const int32_t *column_indices, int64_t nodes,
+                                       int64_t edges, int mark_predecessors, int stream_from_host, int device,
+                                       b40c_bfs_problem **out);
+extern "C" int b40c_bfs_problem_destroy(b40c_bfs_problem *p);
+
+namespace b40c {
+namespace server {
+
+constexpr double kQueueSizing = 1.3;
+
+struct Query {
+    int64_t ticket;
+    int32_t graph, source, depth_limit;
+    int32_t *h_labels;
+    int64_t arrival_ns;
+};
+
+struct LaterArrival {
+    bool operator()(const Query &a, const Query &b) const
+    {
+        return a.arrival_ns != b.arrival_ns ? a.arrival_ns > b.arrival_ns : a.ticket > b.ticket;
+    }
+};
+
+struct Graph {
+    b40c_bfs_problem *p = nullptr;
+    int64_t nodes = 0, edges = 0;
+    int32_t width = 0;        // batch width admitted
+    int64_t bytes = 0;        // device bytes charged to the budget
+    bool busy = false;        // a batch of this graph is in flight
+    bool removed = false;
+    int64_t pending = 0;      // queries submitted and not yet finished
+    std::deque<Query> ready;  // arrived, waiting for a batch
+};
+
+// Page-locked landing area of one in-flight batch.
+struct Landing {
+    int32_t depth[64];
+    uint32_t error;
+    int32_t max_level;
+};
+
+struct Batch {
+    int graph;
+    std::vector<Query> queries;
+    bool single;
+    int slot;
+    int64_t launch_ns;
+};
+
+}  // namespace server
+}  // namespace b40c
+
+using namespace b40c;
+using namespace b40c::server;
+
+struct b40c_server {
+    int device = 0;
+    int32_t max_batch = 64, single_strategy = B40C_DIRECTION_OPTIMIZING, max_in_flight = 2;
+    int64_t budget = 0, used = 0;
+    cudaStream_t stream = nullptr;
+    std::chrono::steady_clock::time_point t0;
+    std::vector<Graph *> graphs;
+    std::mutex mu;
+    std::mutex admin;  // serialises add_graph / remove_graph (admission reads then charges the budget)
+    std::condition_variable cv_work, cv_done;
+    std::priority_queue<Query, std::vector<Query>, LaterArrival> arrivals;
+    std::vector<b40c_server_result> results;  // by ticket
+    std::deque<Batch> in_flight;
+    Landing *landing = nullptr;               // [max_in_flight], page-locked
+    cudaEvent_t *done_ev = nullptr;           // [max_in_flight]
+    std::vector<int> free_slots;
+    int64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_queries = 0, single_queries = 0;
+    bool stop = false;
+    int thread_error = 0;
+    std::thread worker;
+
+    int64_t now() const
+    {
+        return std::chrono::duration_cast<std::chrono::nanoseconds>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+// Marks every query of a batch finished (called with the lock held).
+void finish_batch(b40c_server *s, Batch &b, int status, int64_t finish_ns)
+{
+    Graph &g = *s->graphs[b.graph];
+    const Landing &l = s->landing[b.slot];
+    for (size_t i = 0; i < b.queries.size(); i++) {
+        const Query &q = b.queries[i];
+        b40c_server_result &r = s->results[q.ticket];
+        r.status = status;
+        r.search_depth = status ? 0 : (b.single ? l.max_level + 1 : l.depth[i]);
+        r.batch_size = (int32_t)b.queries.size();
+        r.launch_ns = b.launch_ns;
+        r.finish_ns = finish_ns;
+        g.pending--;
+        s->completed++;
+        if (status) s->failed++;
+    }
+    g.busy = false;
+    s->free_slots.push_back(b.slot);
+}
+
+// Issues one batch on the server stream (lock held; the calls only queue work).
+int issue(b40c_server *s, Batch &b)
+{
+    Graph &g = *s->graphs[b.graph];
+    b40c_bfs_problem *p = g.p;
+    Landing *l = s->landing + b.slot;
+    const int k = (int)b.queries.size();
+    int rc;
+    if (b.single) {
+        const Query &q = b.queries[0];
+        rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, q.source, q.depth_limit, 0, nullptr);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(&l->max_level, &p->st->max_level, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream),
+                 "depth copy");
+        if (q.h_labels)
+            CUDA_TRY(cudaMemcpyAsync(q.h_labels, p->d_labels, sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost,
+                                     s->stream),
+                     "label copy");
+    } else {
+        int32_t src[64], lim[64];
+        for (int i = 0; i < k; i++) {
+            src[i] = b.queries[i].source;
+            lim[i] = b.queries[i].depth_limit;
+        }
+        rc = b40c_msbfs_enact(p, src, lim, k, 0, nullptr);
+        if (rc) return rc;
+        CUDA_TRY(cudaMemcpyAsync(l->depth, p->d_ms_depth, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s->stream),
+                 "depth copy");
+        for (int i = 0; i < k; i++)
+            if (b.queries[i].h_labels)
+                CUDA_TRY(cudaMemcpyAsync(b.queries[i].h_labels, p->d_ms_labels + (size_t)i * (size_t)g.nodes,
+                                         sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, s->stream),
+                         "label copy");
+    }
+    CUDA_TRY(cudaMemcpyAsync(&l->error, &p->st->error, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream),
+             "error word copy");
+    CUDA_TRY(cudaEventRecord(s->done_ev[b.slot], s->stream), "event record");
+    return B40C_SUCCESS;
+}
+
+// The graph whose oldest waiting query arrived first among graphs without a
+// batch in flight, or -1.
+int next_graph(b40c_server *s)
+{
+    int best = -1;
+    int64_t best_t = 0;
+    for (size_t i = 0; i < s->graphs.size(); i++) {
+        Graph *g = s->graphs[i];
+        if (!g || g->removed || g->busy || g->ready.empty()) continue;
+        const Query &q = g->ready.front();
+        if (best < 0 || q.arrival_ns < best_t || (q.arrival_ns == best_t && q.ticket < s->graphs[best]->ready.front().ticket)) {
+            best = (int)i;
+            best_t = q.arrival_ns;
+        }
+    }
+    return best;
+}
+
+void dispatcher(b40c_server *s)
+{
+    if (cudaSetDevice(s->device) != cudaSuccess) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->thread_error = B40C_ERROR_NO_DEVICE;
+    }
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        int64_t t = s->now();
+        // 1. arrivals that are due
+        while (!s->arrivals.empty() && s->arrivals.top().arrival_ns <= t) {
+            Query q = s->arrivals.top();
+            s->arrivals.pop();
+            s->graphs[q.graph]->ready.push_back(q);
+        }
+        // 2. retire finished batches in issue order
+        bool retired = false;
+        while (!s->in_flight.empty()) {
+            Batch &b = s->in_flight.front();
+            const cudaError_t e = cudaEventQuery(s->done_ev[b.slot]);
+            if (e == cudaErrorNotReady) break;
+            int status = B40C_SUCCESS;
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                status = (int)e;
+            } else {
+                const uint32_t w = s->landing[b.slot].error;
+                if (w & dev::kErrOverflow)
+                    status = B40C_ERROR_INVALID_CONFIGURATION;
+                else if (w)
+                    status = B40C_ERROR_LAUNCH_TIMEOUT;
+            }
+            finish_batch(s, b, status, s->now());
+            s->in_flight.pop_front();
+            retired = true;
+        }
+        // a dispatcher without a device fails what is waiting instead of issuing it
+        if (s->thread_error) {
+            for (size_t gi = 0; gi < s->graphs.size(); gi++) {
+                Graph *g = s->graphs[gi];
+                while (g && !g->ready.empty()) {
+                    b40c_server_result &r = s->results[g->ready.front().ticket];
+                    r.status = s->thread_error;
+                    r.finish_ns = s->now();
+                    g->ready.pop_front();
+                    g->pending--;
+                    s->completed++;
+                    s->failed++;
+                    retired = true;
+                }
+            }
+        }
+        if (retired) s->cv_done.notify_all();
+        // 3. issue batches
+        while ((int)s->in_flight.size() < s->max_in_flight && !s->free_slots.empty() && !s->thread_error) {
+            const int gi = next_graph(s);
+            if (gi < 0) break;
+            Graph &g = *s->graphs[gi];
+            Batch b;
+            b.graph = gi;
+            b.slot = s->free_slots.back();
+            s->free_slots.pop_back();
+            const int k = std::min<int>(g.width, (int)g.ready.size());
+            for (int i = 0; i < k; i++) {
+                b.queries.push_back(g.ready.front());
+                g.ready.pop_front();
+            }
+            b.single = (k == 1 && s->single_strategy >= 0);
+            b.launch_ns = s->now();
+            g.busy = true;
+            const int rc = issue(s, b);
+            if (rc) {
+                finish_batch(s, b, rc, s->now());
+                s->cv_done.notify_all();
+                continue;
+            }
+            s->batches++;
+            if (b.single)
+                s->single_queries++;
+            else
+                s->batched_queries += k;
+            s->in_flight.push_back(std::move(b));
+        }
+        // 4. wait
+        bool waiting = false;
+        for (Graph *g : s->graphs)
+            if (g && !g->ready.empty()) waiting = true;
+        if (s->stop && s->in_flight.empty() && s->arrivals.empty() && !waiting) break;
+        if (!s->in_flight.empty()) {
+            lk.unlock();
+            std::this_thread::yield();
+            lk.lock();
+        } else if (!s->arrivals.empty()) {
+            const int64_t dt = s->arrivals.top().arrival_ns - s->now();
+            if (dt > 200000) {
+                s->cv_work.wait_for(lk, std::chrono::nanoseconds(dt - 100000));
+            } else {
+                lk.unlock();
+                std::this_thread::yield();
+                lk.lock();
+            }
+        } else {
+            s->cv_work.wait(lk);
+        }
+    }
+}
+
+int check_query(b40c_server *s, int32_t graph, int32_t source)
+{
+    if (graph < 0 || graph >= (int32_t)s->graphs.size() || !s->graphs[graph] || s->graphs[graph]->removed)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no graph %d in the server", graph);
+    if (source < 0 || source >= s->graphs[graph]->nodes)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "source %d out of range for graph %d", source, graph);
+    return B40C_SUCCESS;
+}
+
+// Queues one checked query (lock held).
+int64_t enqueue(b40c_server *s, int32_t graph, int32_t source, int32_t depth_limit, int32_t *h_labels,
+                int64_t arrival_ns)
+{
+    Query q;
+    q.ticket = (int64_t)s->results.size();
+    q.graph = graph;
+    q.source = source;
+    q.depth_limit = depth_limit < 0 ? -1 : depth_limit;
+    q.h_labels = h_labels;
+    q.arrival_ns = arrival_ns < 0 ? s->now() : arrival_ns;
+    b40c_server_result r{};
+    r.ticket = q.ticket;
+    r.graph = graph;
+    r.source = source;
+    r.depth_limit = q.depth_limit;
+    r.status = B40C_ERROR_NOT_READY;
+    r.arrival_ns = q.arrival_ns;
+    s->results.push_back(r);
+    s->graphs[graph]->pending++;
+    s->submitted++;
+    s->arrivals.push(q);
+    return q.ticket;
+}
+
+}  // namespace
+
+extern "C" {
+
+int b40c_server_plan_bytes(int64_t nodes, int64_t edges, int32_t max_batch, int64_t *device_bytes)
+{
+    b40c::clear_error();
+    if (!device_bytes || nodes < 1 || edges < 0 || max_batch < 1 || max_batch > 64)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    *device_bytes = rt::planned_bytes(nodes, edges, max_batch, kQueueSizing);
+    return B40C_SUCCESS;
+}
+
+int b40c_server_create(int device, const b40c_server_options *options, b40c_server **out)
+{
+    b40c::clear_error();
+    if (!out) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null out");
+    *out = nullptr;
+    b40c_server_options o{};
+    if (options) o = *options;
+    if (o.max_batch < 0 || o.max_batch > 64) return b40c::fail(B40C_ERROR_INVALID_VALUE, "max_batch must be in 0..64");
+    if (o.single_strategy == 0) o.single_strategy = B40C_DIRECTION_OPTIMIZING;
+    if (o.single_strategy != -1 && o.single_strategy != B40C_DIRECTION_OPTIMIZING &&
+        o.single_strategy != B40C_EXPAND_CONTRACT)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "single_strategy must be -1, B40C_EXPAND_CONTRACT or "
+                                                    "B40C_DIRECTION_OPTIMIZING");
+    if (o.max_in_flight < 0 || o.max_in_flight > 16)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "max_in_flight must be in 0..16");
+    if (o.memory_budget_bytes < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "negative memory budget");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count < 1) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no CUDA device");
+    }
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no current CUDA device");
+    }
+    if (device >= count) return b40c::fail(B40C_ERROR_INVALID_VALUE, "device %d out of range", device);
+    rt::DeviceGuard guard(device);
+    auto *s = new b40c_server();
+    s->device = device;
+    s->max_batch = o.max_batch ? o.max_batch : 64;
+    s->single_strategy = o.single_strategy;
+    s->max_in_flight = o.max_in_flight ? o.max_in_flight : 2;
+    s->t0 = std::chrono::steady_clock::now();
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        delete s;
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "cudaMemGetInfo failed");
+    }
+    s->budget = o.memory_budget_bytes ? o.memory_budget_bytes : (int64_t)(0.9 * (double)free_b);
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMallocHost((void **)&s->landing, sizeof(Landing) * s->max_in_flight) != cudaSuccess) {
+        cudaGetLastError();
+        if (s->stream) cudaStreamDestroy(s->stream);
+        delete s;
+        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server stream or landing area allocation failed");
+    }
+    s->done_ev = new cudaEvent_t[s->max_in_flight]();
+    for (int i = 0; i < s->max_in_flight; i++) {
+        if (cudaEventCreateWithFlags(&s->done_ev[i], cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (int j = 0; j < i; j++) cudaEventDestroy(s->done_ev[j]);
+            delete[] s->done_ev;
+            cudaFreeHost(s->landing);
+            cudaStreamDestroy(s->stream);
+            delete s;
+            return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server event creation failed");
+        }
+        s->free_slots.push_back(s->max_in_flight - 1 - i);
+    }
+    s->worker = std::thread(dispatcher, s);
+    *out = s;
+    return B40C_SUCCESS;
+}
+
+int b40c_server_drain(b40c_server *s)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    s->cv_work.notify_all();
+    s->cv_done.wait(lk, [s] { return s->completed == s->submitted; });
+    return B40C_SUCCESS;
+}
+
+int b40c_server_destroy(b40c_server *s)
+{
+    b40c::clear_error();
+    if (!s) return B40C_SUCCESS;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    rt::DeviceGuard guard(s->device);
+    cudaStreamSynchronize(s->stream);
+    for (Graph *g : s->graphs) {
+        if (g && g->p) b40c_bfs_problem_destroy(g->p);
+        delete g;
+    }
+    for (int i = 0; i < s->max_in_flight; i++) cudaEventDestroy(s->done_ev[i]);
+    delete[] s->done_ev;
+    cudaFreeHost(s->landing);
+    cudaStreamDestroy(s->stream);
+    cudaGetLastError();
+    delete s;
+    return B40C_SUCCESS;
+}
+
+int b40c_server_add_graph(b40c_server *s, const int32_t *row_offsets, const int32_t *column_indices, int64_t nodes,
+                          int64_t edges, int32_t *graph_id)
+{
+    b40c::clear_error();
+    if (!s || !row_offsets || (!column_indices && edges > 0) || !graph_id || nodes < 1 || edges < 0)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    std::lock_guard<std::mutex> admin(s->admin);
+    int64_t free_budget;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        free_budget = s->budget - s->used;
+    }
+    int width = s->max_batch;
+    // widest power-of-two batch (at most max_batch) whose buffers fit the budget
+    while (width > 1 && rt::planned_bytes(nodes, edges, width, kQueueSizing) > free_budget) {
+        int w = 1;
+        while (w * 2 < width) w *= 2;
+        width = w;
+    }
+    const int64_t need = rt::planned_bytes(nodes, edges, width, kQueueSizing);
+    if (need > free_budget)
+        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION,
+                          "graph of %lld vertices and %lld edges needs %lld device bytes; %lld of the budget left",
+                          (long long)nodes, (long long)edges, (long long)need, (long long)free_budget);
+    rt::DeviceGuard guard(s->device);
+    b40c_bfs_problem *p = nullptr;
+    int rc = b40c_bfs_problem_create(row_offsets, column_indices, nodes, edges, 0, 0, s->device, &p);
+    if (rc) return rc;
+    auto bail = [&](int code) {
+        b40c_bfs_problem_destroy(p);
+        return code;
+    };
+    p->stream = s->stream;
+    p->queue_sizing = kQueueSizing;
+    // allocate everything a batch of full width and a single search use, now
+    // rather than while serving; the searches also run the symmetry test once
+    std::vector<int32_t> warm(width, 0);
+    if ((rc = b40c_msbfs_enact(p, warm.data(), nullptr, width, 0, nullptr))) return bail(rc);
+    if (s->single_strategy >= 0 &&
+        (rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, 0, -1, 0, nullptr)))
+        return bail(rc);
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+        const cudaError_t e = cudaGetLastError();
+        return bail(b40c::fail((int)e, "graph warm-up failed: %s", cudaGetErrorString(e)));
+    }
+    auto *g = new Graph();
+    g->p = p;
+    g->nodes = nodes;
+    g->edges = edges;
+    g->width = width;
+    g->bytes = rt::device_bytes(p);
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->used += g->bytes;
+    *graph_id = (int32_t)s->graphs.size();
+    s->graphs.push_back(g);
+    return B40C_SUCCESS;
+}
+
+int b40c_server_remove_graph(b40c_server *s, int32_t graph_id)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    std::lock_guard<std::mutex> admin(s->admin);
+    b40c_bfs_problem *p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (graph_id < 0 || graph_id >= (int32_t)s->graphs.size() || !s->graphs[graph_id] ||
+            s->graphs[graph_id]->removed)
+            return b40c::fail(B40C_ERROR_INVALID_VALUE, "no graph %d in the server", graph_id);
+        Graph *g = s->graphs[graph_id];
+        if (g->pending || g->busy) return b40c::fail(B40C_ERROR_NOT_READY, "graph %d has queries pending", graph_id);
+        g->removed = true;
+        s->used -= g->bytes;
+        p = g->p;
+        g->p = nullptr;
+    }
+    rt::DeviceGuard guard(s->device);
+    return b40c_bfs_problem_destroy(p);
+}
+
+int b40c_server_graph_info(b40c_server *s, int32_t graph_id, int64_t *device_bytes, int32_t *max_batch)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (graph_id < 0 || graph_id >= (int32_t)s->graphs.size() || !s->graphs[graph_id] || s->graphs[graph_id]->removed)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no graph %d in the server", graph_id);
+    if (device_bytes) *device_bytes = s->graphs[graph_id]->bytes;
+    if (max_batch) *max_batch = s->graphs[graph_id]->width;
+    return B40C_SUCCESS;
+}
+
+int b40c_server_now_ns(b40c_server *s, int64_t *now_ns)
+{
+    b40c::clear_error();
+    if (!s || !now_ns) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    *now_ns = s->now();
+    return B40C_SUCCESS;
+}
+
+int b40c_server_submit(b40c_server *s, int32_t graph_id, int32_t source, int32_t depth_limit, int32_t *h_labels,
+                       int64_t arrival_ns, int64_t *ticket)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    int64_t t;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        int rc = check_query(s, graph_id, source);
+        if (rc) return rc;
+        t = enqueue(s, graph_id, source, depth_limit, h_labels, arrival_ns);
+    }
+    s->cv_work.notify_all();
+    if (ticket) *ticket = t;
+    return B40C_SUCCESS;
+}
+
+int b40c_server_submit_many(b40c_server *s, int64_t count, const int32_t *graph_ids, const int32_t *sources,
+                            const int32_t *depth_limits, const int64_t *arrival_ns, int64_t *tickets)
+{
+    b40c::clear_error();
+    if (!s || count < 0 || (count > 0 && (!graph_ids || !sources)))
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (int64_t i = 0; i < count; i++) {
+            int rc = check_query(s, graph_ids[i], sources[i]);
+            if (rc) return rc;
+        }
+        for (int64_t i = 0; i < count; i++) {
+            const int64_t t = enqueue(s, graph_ids[i], sources[i], depth_limits ? depth_limits[i] : -1, nullptr,
+                                      arrival_ns ? arrival_ns[i] : -1);
+            if (tickets) tickets[i] = t;
+        }
+    }
+    s->cv_work.notify_all();
+    return B40C_SUCCESS;
+}
+
+int b40c_server_result_get(b40c_server *s, int64_t ticket, b40c_server_result *out)
+{
+    b40c::clear_error();
+    if (!s || !out) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (ticket < 0 || ticket >= (int64_t)s->results.size())
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no ticket %lld", (long long)ticket);
+    *out = s->results[ticket];
+    return B40C_SUCCESS;
+}
+
+int b40c_server_wait(b40c_server *s, int64_t ticket, b40c_server_result *out)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (ticket < 0 || ticket >= (int64_t)s->results.size())
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no ticket %lld", (long long)ticket);
+    s->cv_done.wait(lk, [s, ticket] { return s->results[ticket].status != B40C_ERROR_NOT_READY; });
+    if (out) *out = s->results[ticket];
+    return B40C_SUCCESS;
+}
+
+int b40c_server_results(b40c_server *s, int64_t first, int64_t count, b40c_server_result *out)
+{
+    b40c::clear_error();
+    if (!s || !out || first < 0 || count < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (first + count > (int64_t)s->results.size())
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "tickets past the last submitted");
+    std::copy(s->results.begin() + first, s->results.begin() + first + count, out);
+    return B40C_SUCCESS;
+}
+
+int b40c_server_counters_get(b40c_server *s, b40c_server_counters *out)
+{
+    b40c::clear_error();
+    if (!s || !out) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    b40c_server_counters c{};
+    c.submitted = s->submitted;
+    c.completed = s->completed;
+    c.failed = s->failed;
+    c.batches = s->batches;
+    c.batched_queries = s->batched_queries;
+    c.single_queries = s->single_queries;
+    c.memory_used_bytes = s->used;
+    c.memory_budget_bytes = s->budget;
+    for (Graph *g : s->graphs)
+        if (g && !g->removed) c.graphs++;
+    *out = c;
+    return B40C_SUCCESS;
+}
+
+}  // extern "C"

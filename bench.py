@@ -296,6 +296,81 @@ def batched_extra(steps, warmup):
     return out
 
 
+SERVED_SET = [("rmat16", dict(kind="rmat", scale=16, ef=16)), ("rmat18", dict(kind="rmat", scale=18, ef=16)),
+              ("rmat20", dict(kind="rmat", scale=20, ef=16)), ("rmat22", dict(kind="rmat", scale=22, ef=16)),
+              ("grid2d2048", dict(kind="grid2d", width=2048)), ("grid3d128", dict(kind="grid3d", width=128))]
+SERVED_BUDGET = 6 << 30  # device bytes the server may hold for the six graphs
+
+
+def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=(0.25, 0.5, 0.75, 0.9)):
+    """The query server on the six resident graphs: a seeded request stream
+    (graph uniform over the six, source uniform over 4096 sampled degree > 0
+    vertices of it, depth limit unlimited w.p. 0.8 else uniform in 2..8).
+      * capacity: all requests queued at t = 0, queries/s to the last answer;
+      * one at a time: the same server with batch width 1 (plain
+        direction-optimizing search per query) on the first requests;
+      * latency: Poisson arrivals at fractions of the capacity, p50/p99 of
+        finish - arrival on the server clock."""
+    from back40computing_b200 import CsrGraph, BuildRmatGraph, BuildGrid2dGraph, BuildGrid3dGraph, sample_sources
+    from back40computing_b200.server import BfsServer, latency_summary
+    graphs = []
+    for name, cfg in SERVED_SET:
+        if resident is not None and name == resident[0]:
+            graphs.append(resident[1])
+            continue
+        g = CsrGraph()
+        if cfg["kind"] == "rmat":
+            n = 1 << cfg["scale"]
+            BuildRmatGraph(n, cfg["ef"] * n, g, True, 0.57, 0.19, 0.19, seed=0, permute=True)
+        elif cfg["kind"] == "grid2d":
+            BuildGrid2dGraph(cfg["width"], g)
+        else:
+            BuildGrid3dGraph(cfg["width"], g)
+        graphs.append(g)
+    rng = np.random.default_rng(0)
+    gid = rng.integers(0, len(graphs), n_requests).astype(np.int32)
+    src = np.empty(n_requests, np.int32)
+    for i, g in enumerate(graphs):
+        pool = sample_sources(g, 4096, seed=i)
+        sel = gid == i
+        src[sel] = pool[rng.integers(0, pool.size, int(sel.sum()))]
+    lim = np.where(rng.random(n_requests) < 0.8, -1, rng.integers(2, 9, n_requests)).astype(np.int32)
+
+    def run(server, count, arrivals):
+        t0 = server.now_ns() + 20_000_000
+        tk = server.submit_many(gid[:count], src[:count], lim[:count], t0 + arrivals)
+        server.drain()
+        return server.results(int(tk[0]), count)
+
+    out = {"graphs": [n for n, _ in SERVED_SET], "budget_bytes": SERVED_BUDGET, "requests": n_requests}
+    with BfsServer(memory_budget_bytes=SERVED_BUDGET) as srv:
+        for g in graphs:
+            srv.add_graph(g)
+        out["widths"] = [srv.graph_info(i)[1] for i in range(len(graphs))]
+        out["memory_used_bytes"] = srv.counters()["memory_used_bytes"]
+        run(srv, 500, np.zeros(500, np.int64))  # warm-up
+        cap = latency_summary(run(srv, n_requests, np.zeros(n_requests, np.int64)))
+        out["capacity"] = cap
+        sweep = []
+        for f in rates:
+            rate = f * cap["queries_per_s"]
+            gaps = rng.exponential(1e9 / rate, n_requests)
+            rec = run(srv, n_requests, np.cumsum(gaps).astype(np.int64))
+            sm = latency_summary(rec)
+            sm["offered_qps"] = rate
+            sweep.append(sm)
+        out["latency_sweep"] = sweep
+    with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_batch=1) as one:
+        for g in graphs:
+            one.add_graph(g)
+        run(one, 50, np.zeros(50, np.int64))
+        base = latency_summary(run(one, baseline_requests, np.zeros(baseline_requests, np.int64)))
+        base["sample"] = f"first {baseline_requests} requests of the stream"
+        out["one_at_a_time"] = base
+    out["speedup_queries_per_s"] = cap["queries_per_s"] / base["queries_per_s"]
+    return out
+
+
 def lattice_extra():
     """grid2d-1000 from the corner and grid3d-256 from the centre: the persistent grid,
     the whole-search CUDA graph and per-level launches."""
@@ -428,6 +503,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         extras["batched"] = batched_extra(max(args.steps, 3), args.warmup)
         extras["lattices"] = lattice_extra()
+        extras["served"] = served_extra((args.config, g) if args.config in dict(SERVED_SET) else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

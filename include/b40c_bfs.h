@@ -142,6 +142,11 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *problem);
  * the handle's own stream. */
 int b40c_bfs_set_stream(b40c_bfs_problem *problem, void *cuda_stream);
 
+/* Device bytes the handle holds now (CSR copy, labels, masks, queues, batch
+ * buffers).  No counterpart in the reference (its GraphSlice allocations are
+ * not reported, csr_problem.cuh:96-172). */
+int b40c_bfs_problem_device_bytes(b40c_bfs_problem *problem, int64_t *bytes);
+
 /* CsrProblem::Reset (csr_problem.cuh:547-750): (re)allocates the frontier
  * queues for frontier_type at queue_sizing x n (vertex) or x m (edge)
  * elements, and initialises labels to -1 and the visited mask to 0. */
@@ -216,14 +221,19 @@ int b40c_bfs_device_view_get(b40c_bfs_problem *problem, b40c_bfs_device_view *vi
  * slot s are what a single-source search from sources[s] with
  * depth_limits[s] produces (distances; -1 unreached or beyond the limit).
  * depth_limits may be NULL (unlimited).  Duplicate sources are allowed.  One
- * persistent cooperative grid, asynchronous like b40c_bfs_enact (the call
- * itself waits for the previous batch's uploads); b40c_bfs_stats reports the
- * deepest search as search_depth. */
+ * persistent cooperative grid, asynchronous like b40c_bfs_enact (the
+ * sources travel as kernel arguments, so batches may be queued back to back);
+ * b40c_bfs_stats reports the deepest search as search_depth and
+ * b40c_msbfs_stats each slot's own. */
 int b40c_msbfs_enact(b40c_bfs_problem *problem, const int32_t *sources, const int32_t *depth_limits, int k,
                      int max_grid_size, const b40c_bfs_policy *policy);
 
 /* Copies slot `slot`'s labels of the last batch to the host. */
 int b40c_msbfs_extract(b40c_bfs_problem *problem, int slot, int32_t *h_labels);
+
+/* search_depths[k]: each slot's search depth in the last batch (max label + 1,
+ * the GetStatistics meaning, enactor_contract_expand.cuh:237-250). */
+int b40c_msbfs_stats(b40c_bfs_problem *problem, int32_t *search_depths);
 
 /* Device array int32[k][nodes] of the last batch's labels (valid until the next batch). */
 int b40c_msbfs_device_labels(b40c_bfs_problem *problem, void **d_labels, int32_t *k);

@@ -57,3 +57,25 @@ def test_policy_validation_without_device():
     assert N.lib().b40c_bfs_default_policy(0, ctypes.byref(pol)) == 0
     assert pol.threads == 256 and pol.chunk_edges == 2048
     assert N.lib().b40c_bfs_default_policy(9, ctypes.byref(pol)) == N.ERROR_INVALID_VALUE
+
+
+def test_server_without_device_reports_status():
+    if N.device_count() > 0:
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    assert N.lib().b40c_server_create(0, None, ctypes.byref(h)) == N.ERROR_NO_DEVICE
+    assert not h.value
+
+
+def test_server_plan_bytes_arithmetic():
+    """Admission's byte plan: the CSR, labels, masks, two vertex frontiers
+    (1.3 n each), look-back slots and k label rows of the batch."""
+    from back40computing_b200.server import BfsServer
+    n, m = 1 << 20, 1 << 24
+    b1, b2, b64 = (BfsServer.plan_bytes(n, m, k) for k in (1, 2, 64))
+    assert b2 - b1 == 4 * n and b64 - b1 == 63 * 4 * n
+    csr = 4 * (n + 1) + 4 * m
+    # labels 4n, batch masks 24n + one label row 4n, two frontiers ~31n, slots ~m/256
+    assert csr + 4 * n + 3 * 8 * n < b1 < csr + 72 * n + m // 8
+    with pytest.raises(N.B40cError):
+        BfsServer.plan_bytes(n, m, 65)
