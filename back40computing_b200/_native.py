@@ -182,6 +182,7 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_server_add_graph": (C.c_int, [C.c_void_p, _P_i32, _P_i32, C.c_int64, C.c_int64, _P_i32]),
     "b40c_server_remove_graph": (C.c_int, [C.c_void_p, C.c_int32]),
     "b40c_server_graph_info": (C.c_int, [C.c_void_p, C.c_int32, _P_i64, _P_i32]),
+    "b40c_server_set_graph_policy": (C.c_int, [C.c_void_p, C.c_int32, C.POINTER(Policy), C.POINTER(Policy)]),
     "b40c_server_plan_bytes": (C.c_int, [C.c_int64, C.c_int64, C.c_int32, _P_i64]),
     "b40c_server_now_ns": (C.c_int, [C.c_void_p, _P_i64]),
     "b40c_server_submit": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32, C.c_void_p, C.c_int64, _P_i64]),

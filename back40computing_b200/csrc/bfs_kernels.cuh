@@ -55,6 +55,7 @@ struct ExpandSmem {
     int32_t q, E;
     unsigned long long visited_edges;  // degree sum of the vertices visited up to this pass
     int32_t prev_bu;                   // the previous level ran bottom-up
+    uint32_t *mask;                    // the visited-mask buffer of this pass (mask or mask_alt)
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -119,14 +120,14 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
         go[t] = valid[t];
         if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
         word[t] = 0;
-        if (go[t] && p.precheck) word[t] = ld_mask(p.mask + (v[t] >> 5));
+        if (go[t] && p.precheck) word[t] = ld_mask(s.mask + (v[t] >> 5));
     }
     bool found[U];
 #pragma unroll
     for (int t = 0; t < U; t++) {
         const unsigned bit = 1u << (v[t] & 31);
         found[t] = false;
-        if (go[t] && !(word[t] & bit)) found[t] = !(atomicOr(p.mask + (v[t] >> 5), bit) & bit);
+        if (go[t] && !(word[t] & bit)) found[t] = !(atomicOr(s.mask + (v[t] >> 5), bit) & bit);
     }
     int r0[U], r1[U];
 #pragma unroll
@@ -420,9 +421,11 @@ constexpr int kBottomUpLongList = 256;  // lists longer than this are searched w
 // unvisited vertex with edges looks for a neighbour whose visited bit is set
 // in the snapshot taken at the start of the level; on an undirected graph
 // such a neighbour is exactly one level up, so the vertex is labelled
-// level + 1 (or that neighbour, the first one in CSR order).  Discoveries go
-// to next_mask (merged into the visited mask after the level, keeping the
-// snapshot intact) and, through emit_frontier, into the next vertex frontier.
+// level + 1 (or that neighbour, the first one in CSR order).  The visited set
+// is read from the pass's mask buffer (s.mask, unchanged during the level)
+// and written, old bits | discoveries, to every word of the other buffer,
+// which the next pass reads; discoveries also go, through emit_frontier, into
+// the next vertex frontier.
 // A warp handles blocks of 32 consecutive vertices (one visited-mask word);
 // each thread first issues, for all of its PER vertices at once, the
 // vertices' own visited words, their rows and their first kBottomUpProbe
@@ -438,6 +441,8 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr int PER = kChunkMax / B;
     constexpr int K = kBottomUpProbe;
+    const uint32_t *mask = s.mask;
+    uint32_t *mask_out = (s.mask == p.mask) ? p.mask_alt : p.mask;
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
@@ -447,7 +452,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
 #pragma unroll
         for (int t = 0; t < PER; t++) {
             const int vb = cs + t * B + (tid & ~31);
-            word[t] = vb < re ? ld_cg(p.mask + (vb >> 5)) : 0xffffffffu;
+            word[t] = vb < re ? ld_cg(mask + (vb >> 5)) : 0xffffffffu;
         }
         int r0[PER], r1[PER];
         bool todo[PER];
@@ -475,7 +480,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
 #pragma unroll
             for (int t = 0; t < PER; t++)
 #pragma unroll
-                for (int k = 0; k < K; k++) w[t][k] = nb[t][k] >= 0 ? ld_mask(p.mask + (nb[t][k] >> 5)) : 0u;
+                for (int k = 0; k < K; k++) w[t][k] = nb[t][k] >= 0 ? ld_mask(mask + (nb[t][k] >> 5)) : 0u;
 #pragma unroll
             for (int t = 0; t < PER; t++) {
                 parent[t] = -1;
@@ -499,7 +504,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
 #pragma unroll
                     for (int k = 0; k < 4; k++) nb[k] = (e + k < r1[t]) ? ld_stream(p.column_indices + e + k) : -1;
 #pragma unroll
-                    for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(p.mask + (nb[k] >> 5)) : 0u;
+                    for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
 #pragma unroll
                     for (int k = 0; k < 4; k++)
                         if (parent[t] < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent[t] = nb[k];
@@ -517,7 +522,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                 for (int eb = lr0; eb < lr1; eb += 32) {
                     const int ee = eb + lane;
                     const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
-                    const bool hit = nb >= 0 && ((ld_mask(p.mask + (nb >> 5)) >> (nb & 31)) & 1u);
+                    const bool hit = nb >= 0 && ((ld_mask(mask + (nb >> 5)) >> (nb & 31)) & 1u);
                     const unsigned hb = __ballot_sync(0xffffffffu, hit);
                     if (hb) {
                         found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
@@ -535,8 +540,8 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             const int v = vb + lane;
             const bool found = parent[t] >= 0;
             const unsigned fb = __ballot_sync(0xffffffffu, found);
+            if (lane == 0) mask_out[vb >> 5] = word[t] | fb;  // this warp owns the whole word
             if (fb == 0) continue;
-            if (lane == 0) p.next_mask[vb >> 5] = fb;  // this warp owns the whole word
             if (found) {
                 p.labels[v] = PRED ? parent[t] : level + 1;
                 s.flag = 1;
@@ -555,20 +560,6 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         __syncthreads();
         emit_frontier<B>(p, s, pass, vout, qe_out);
         __syncthreads();
-    }
-}
-
-// Folds the bottom-up discoveries of the last level into the visited mask
-// and clears next_mask (the CTA's share of words).
-__device__ __forceinline__ void merge_next_mask(const BfsParams &p)
-{
-    const int stride = gridDim.x * blockDim.x;
-    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < p.mask_words; w += stride) {
-        const unsigned m = ld_cg(p.next_mask + w);
-        if (m) {
-            p.mask[w] |= m;
-            p.next_mask[w] = 0;
-        }
     }
 }
 
@@ -667,6 +658,7 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
         }
         s.visited_edges = ld_cg64(&p.st->visited_edges[pass % 3]) + (unsigned long long)s.E;
         s.prev_bu = ld_cg(&p.st->dir[pass % 3]);
+        s.mask = ld_cg(&p.st->mask_sel[pass % 3]) ? p.mask_alt : p.mask;
         if (p.levels && blockIdx.x == 0 && pass < kMaxLevelRecords) {
             LevelRecord r;
             r.vertices = s.q;
@@ -680,14 +672,15 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
     __syncthreads();
 }
 
-// Direction bookkeeping of pass `pass` (block 0): the visited-edge total
-// and whether the level ran bottom-up, for the next pass.
+// Direction bookkeeping of pass `pass` (block 0): the visited-edge total,
+// whether the level ran bottom-up and which mask buffer the next pass reads
+// (a bottom-up level writes the other one).
 __device__ __forceinline__ void record_direction(const BfsParams &p, unsigned long long visited_edges, int pass,
-                                                 bool bu)
+                                                 bool bu, const uint32_t *pass_mask)
 {
     p.st->visited_edges[(pass + 1) % 3] = visited_edges;
     p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
-    if (bu) p.st->merge_pending = 1;
+    p.st->mask_sel[(pass + 1) % 3] = (pass_mask == p.mask) == bu ? 1 : 0;
     if (bu && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
 }
 
@@ -726,7 +719,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             // ---- small frontiers: CTA 0 alone, level after level ----------------------
             if (blockIdx.x == 0) {
                 for (int solo = 0;; solo++) {
-                    if (tid == 0) record_direction(p, s.visited_edges, pass, false);
+                    if (tid == 0) record_direction(p, s.visited_edges, pass, false, s.mask);
                     expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
                                                 &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
                     __syncthreads();
@@ -754,19 +747,13 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
-        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu);
+        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu, s.mask);
         if (bu)
             bottom_up_range<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         else
             expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
                                         &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);
         __syncthreads();
-        if (bu && p.persistent) {
-            // fold the level's discoveries into the visited mask before the next level
-            if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
-            merge_next_mask(p);
-            if (tid == 0 && blockIdx.x == 0) p.st->merge_pending = 0;
-        }
         worked = true;
         if (s.flag) max_level_seen = level + 1;
         if (!p.persistent) break;
@@ -872,24 +859,6 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
     }
 }
 
-// Non-persistent launches: folds a bottom-up level's discoveries into the
-// visited mask before the next level's launch.
-template <bool PRED>
-__global__ void merge_kernel(BfsParams p)
-{
-    if (ld_cg(&p.st->merge_pending) == 0) return;
-    merge_next_mask(p);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned t = atomicAdd(&p.st->finished, 1u);
-        if (t == gridDim.x - 1) {
-            p.st->finished = 0;
-            p.st->merge_pending = 0;
-        }
-    }
-}
-
 // Sets up a search: the source's label, visited bit and the level-0
 // frontier, plus the search state.  With FULL it first initialises every
 // label to -1 and the visited mask to 0 (what CsrProblem::Reset does,
@@ -907,7 +876,6 @@ __global__ void init_kernel(BfsParams p)
         for (long long i = t0; i < p.nodes; i += stride) p.labels[i] = (VERTEX_FRONTIER && i == src) ? src_label : -1;
         for (long long w = t0; w < p.mask_words; w += stride) {
             p.mask[w] = (VERTEX_FRONTIER && w == (src >> 5)) ? (1u << (src & 31)) : 0u;
-            if (p.next_mask) p.next_mask[w] = 0u;
         }
     } else if (VERTEX_FRONTIER && t0 == 0) {
         p.labels[src] = src_label;
@@ -928,7 +896,7 @@ __global__ void init_kernel(BfsParams p)
         st->finished = 0;
         st->qe[1] = st->qe[2] = 0;
         st->dir[0] = st->dir[1] = st->dir[2] = 0;
-        st->merge_pending = 0;
+        st->mask_sel[0] = st->mask_sel[1] = st->mask_sel[2] = 0;
         st->visited_edges[0] = st->visited_edges[1] = st->visited_edges[2] = 0;
         if (VERTEX_FRONTIER) {
             const int deg = r1 - r0;

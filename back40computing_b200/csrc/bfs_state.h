@@ -49,10 +49,10 @@ struct alignas(128) SearchState {
     uint32_t finished;         // CTAs that finished the current non-persistent launch
     int32_t src;               // source vertex (read by the init kernel)
     int32_t depth_limit;       // < 0: unlimited
-    int32_t merge_pending;     // a bottom-up level left discoveries in the next-mask
     // direction-optimizing bookkeeping, rotating like qe: pass k reads [k % 3]
     // and block 0 writes [(k + 1) % 3]
     int32_t dir[3];            // 1: the previous level ran bottom-up
+    int32_t mask_sel[3];       // which visited-mask buffer holds the visited set (0: mask, 1: mask_alt)
     unsigned long long visited_edges[3];  // degree sum of the vertices visited before the pass
     // level at which a persistent launch resumes after a small-frontier phase of
     // CTA 0, by phase parity (a slot is rewritten only two phases later, after
@@ -112,7 +112,8 @@ struct BfsParams {
     int32_t bu_alpha;         // switch to bottom-up when frontier edges > unvisited edges / alpha
     int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
     int32_t small_edges;      // persistent launches: frontiers with at most this many edges run on CTA 0 alone
-    uint32_t *next_mask;      // bottom-up discoveries of the current level (merged into mask after it)
+    uint32_t *mask_alt;       // second visited-mask buffer: a bottom-up level reads one buffer and writes
+                              // every word of the other (old bits | its discoveries), then they swap
     LevelRecord *levels;      // per-pass records when instrumented, else null
     unsigned long long *duty; // [0] sum over CTAs of busy ns, [1] sum of lifetime ns (instrumented)
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none

@@ -19,7 +19,6 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     BfsParams k = make_params(p, pol);
     k.direction_opt = direction_opt ? 1 : 0;
     const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
-    const void *merge = (const void *)dev::merge_kernel<PRED>;
     const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
@@ -28,9 +27,9 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     if (mode == B40C_ENACT_GRAPH) {
         if ((rc = mark_search_start(p))) return rc;
         KernelNode init{init_kernel_ptr<PRED>(true, true), dim3(init_grid(p, true)), dim3(kThreads), 0, k};
-        KernelNode body[2] = {{merge, dim3(grid), dim3(kThreads), 0, k}, {kern, dim3(grid), dim3(kThreads), smem, k}};
+        KernelNode body[1] = {{kern, dim3(grid), dim3(kThreads), smem, k}};
         const int slot = direction_opt ? B40C_HYBRID + 1 : B40C_EXPAND_CONTRACT;
-        if ((rc = run_graph(p, slot, init, direction_opt ? body : body + 1, direction_opt ? 2 : 1))) return rc;
+        if ((rc = run_graph(p, slot, init, body, 1))) return rc;
         return finish_timing(p);
     }
     if ((rc = upload_source(p))) return rc;
@@ -50,10 +49,7 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
             const int q = qe_count(p->h_st->qe[level % 3]), E = qe_edges(p->h_st->qe[level % 3]);
             if (q == 0) break;
             int g = std::max(1, std::min(grid, (E + 255) / 256));
-            if (direction_opt) {
-                if ((rc = launch_plain(p, merge, grid, 0, k, "merge launch"))) return rc;
-                g = grid;  // a bottom-up level spans every vertex
-            }
+            if (direction_opt) g = grid;  // a bottom-up level spans every vertex
             if ((rc = launch_plain(p, kern, g, smem, k, "expand-contract level launch"))) return rc;
         }
     } else {

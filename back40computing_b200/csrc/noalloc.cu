@@ -154,7 +154,7 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
     k.bu_alpha = 14;
     k.bu_beta = 24;
     k.small_edges = 1024;
-    k.next_mask = nullptr;
+    k.mask_alt = nullptr;  // never bottom-up
     k.levels = nullptr;
     k.duty = nullptr;
     k.cond_handle = 0;

@@ -123,7 +123,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.direction_opt = 0;
     k.bu_alpha = pol.bottom_up_alpha;
     k.bu_beta = pol.bottom_up_beta;
-    k.next_mask = p->d_next;
+    k.mask_alt = p->d_next;
     k.small_edges = pol.small_frontier_edges;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
@@ -549,12 +549,9 @@ int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t no
     if ((rc = alloc_dev((void **)&p->d_labels, sizeof(int32_t) * nodes, "labels"))) return bail(rc);
     if ((rc = alloc_dev((void **)&p->d_mask, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "visited mask")))
         return bail(rc);
-    if ((rc = alloc_dev((void **)&p->d_next, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "next mask")))
+    // second mask buffer: written whole by a bottom-up level before anything reads it
+    if ((rc = alloc_dev((void **)&p->d_next, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "second mask")))
         return bail(rc);
-    if (cudaMemsetAsync(p->d_next, 0, sizeof(uint32_t) * p->mask_words, p->stream) != cudaSuccess) {
-        cudaGetLastError();
-        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "next mask reset failed"));
-    }
     if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
     if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
         cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {
@@ -656,7 +653,6 @@ int b40c_bfs_problem_reset(b40c_bfs_problem *p, int frontier_type, double queue_
     // labels <- -1, visited mask <- 0 (csr_problem.cuh:723-745)
     CUDA_TRY(cudaMemsetAsync(p->d_labels, 0xff, sizeof(int32_t) * p->nodes, p->stream), "label reset");
     CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, sizeof(uint32_t) * p->mask_words, p->stream), "mask reset");
-    CUDA_TRY(cudaMemsetAsync(p->d_next, 0, sizeof(uint32_t) * p->mask_words, p->stream), "next mask reset");
     CUDA_TRY(cudaStreamSynchronize(p->stream), "reset synchronize");
     p->needs_init = false;
     return B40C_SUCCESS;

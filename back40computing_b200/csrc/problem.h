@@ -40,7 +40,7 @@ struct b40c_bfs_problem {
     // search arrays
     int32_t *d_labels = nullptr;
     uint32_t *d_mask = nullptr;
-    uint32_t *d_next = nullptr;  // bottom-up discoveries of a level (direction-optimizing), kept zero between levels
+    uint32_t *d_next = nullptr;  // second visited-mask buffer (bottom-up levels write it whole)
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
     // batched multi-source searches (allocated on first use)

@@ -63,6 +63,8 @@ struct Graph {
     bool removed = false;
     int64_t pending = 0;      // queries submitted and not yet finished
     std::deque<Query> ready;  // arrived, waiting for a batch
+    bool has_single = false, has_batch = false;
+    b40c_bfs_policy single{}, batch{};  // tuned policies (else the library defaults)
 };
 
 // Page-locked landing area of one in-flight batch.
@@ -146,7 +148,8 @@ int issue(b40c_server *s, Batch &b)
     int rc;
     if (b.single) {
         const Query &q = b.queries[0];
-        rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, q.source, q.depth_limit, 0, nullptr);
+        rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, q.source, q.depth_limit, 0,
+                                    g.has_single ? &g.single : nullptr);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(&l->max_level, &p->st->max_level, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream),
                  "depth copy");
@@ -160,7 +163,7 @@ int issue(b40c_server *s, Batch &b)
             src[i] = b.queries[i].source;
             lim[i] = b.queries[i].depth_limit;
         }
-        rc = b40c_msbfs_enact(p, src, lim, k, 0, nullptr);
+        rc = b40c_msbfs_enact(p, src, lim, k, 0, g.has_batch ? &g.batch : nullptr);
         if (rc) return rc;
         CUDA_TRY(cudaMemcpyAsync(l->depth, p->d_ms_depth, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s->stream),
                  "depth copy");
@@ -527,6 +530,28 @@ int b40c_server_remove_graph(b40c_server *s, int32_t graph_id)
     }
     rt::DeviceGuard guard(s->device);
     return b40c_bfs_problem_destroy(p);
+}
+
+int b40c_server_set_graph_policy(b40c_server *s, int32_t graph_id, const b40c_bfs_policy *single,
+                                  const b40c_bfs_policy *batch)
+{
+    b40c::clear_error();
+    if (!s) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null server");
+    b40c_bfs_policy a{}, b{};
+    int rc;
+    if (single && (rc = rt::resolve_policy(s->single_strategy < 0 ? B40C_EXPAND_CONTRACT : s->single_strategy, single,
+                                           &a)))
+        return rc;
+    if (batch && (rc = rt::resolve_policy(B40C_EXPAND_CONTRACT, batch, &b))) return rc;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (graph_id < 0 || graph_id >= (int32_t)s->graphs.size() || !s->graphs[graph_id] || s->graphs[graph_id]->removed)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no graph %d in the server", graph_id);
+    Graph *g = s->graphs[graph_id];
+    g->has_single = single != nullptr;
+    g->has_batch = batch != nullptr;
+    if (single) g->single = *single;
+    if (batch) g->batch = *batch;
+    return B40C_SUCCESS;
 }
 
 int b40c_server_graph_info(b40c_server *s, int32_t graph_id, int64_t *device_bytes, int32_t *max_batch)

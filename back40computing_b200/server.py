@@ -48,6 +48,20 @@ class BfsServer:
                 "b40c_server_add_graph")
         return gid.value
 
+    def set_graph_policy(self, graph_id: int, single: N.Policy | None = None, batch: N.Policy | None = None) -> None:
+        N.check(N.lib().b40c_server_set_graph_policy(self.handle, int(graph_id),
+                                                     C.byref(single) if single is not None else None,
+                                                     C.byref(batch) if batch is not None else None),
+                "b40c_server_set_graph_policy")
+
+    def add_tuned_graph(self, graph: CsrGraph) -> int:
+        """add_graph plus the autotuner's policies for the graph's class."""
+        from . import autotune
+        gid = self.add_graph(graph)
+        cls = autotune.classify(graph)
+        self.set_graph_policy(gid, autotune.policy_for(cls, "direction-optimizing"), autotune.policy_for(cls, "batched"))
+        return gid
+
     def remove_graph(self, graph_id: int) -> None:
         N.check(N.lib().b40c_server_remove_graph(self.handle, int(graph_id)), "b40c_server_remove_graph")
 

@@ -21,6 +21,8 @@
 
 #include <stdint.h>
 
+#include "b40c_bfs.h"
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -80,6 +82,12 @@ int b40c_server_add_graph(b40c_server *server, const int32_t *row_offsets, const
 /* Frees a graph's memory; B40C_ERROR_NOT_READY (600) while it has queries
  * pending or in flight. */
 int b40c_server_remove_graph(b40c_server *server, int32_t graph_id);
+
+/* Kernel policies for a graph's lone-query searches and its batches (either
+ * may be NULL: the library defaults); e.g. the autotuner's choice for the
+ * graph's class.  Validated like b40c_bfs_enact's policy argument. */
+int b40c_server_set_graph_policy(b40c_server *server, int32_t graph_id, const b40c_bfs_policy *single,
+                                 const b40c_bfs_policy *batch);
 
 /* Device bytes a graph holds and its batch width. */
 int b40c_server_graph_info(b40c_server *server, int32_t graph_id, int64_t *device_bytes, int32_t *max_batch);
