@@ -622,10 +622,13 @@ struct DutyClock {
     }
 };
 
-// Epilogue of a non-persistent launch that completed a level: the last CTA
-// to finish advances the level and decides whether the search continues
-// (and, inside a captured graph, sets the WHILE node's condition).
-__device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int next_pass, bool limit_hit)
+// Epilogue of every non-persistent launch: the last CTA to finish advances
+// the level (unless `stop`: the launch found nothing to do -- an empty
+// frontier or an error -- or overflowed) and decides whether the search
+// continues; inside a captured graph it sets the WHILE node's condition, so
+// a launch must never end without coming here or the loop would not stop.
+__device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int next_pass, bool limit_hit,
+                                              bool stop = false)
 {
     if (threadIdx.x != 0) return;
     __threadfence();
@@ -633,9 +636,15 @@ __device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int
     if (t == gridDim.x - 1) {
         __threadfence();
         p.st->finished = 0;
-        p.st->cur_level = level + 1;
-        const int qn = qe_count(ld_cg64(&p.st->qe[next_pass % 3]));
-        const bool done = (qn == 0) || limit_hit || (ld_cg(&p.st->error) != 0);
+        if (!stop) p.st->cur_level = level + 1;
+        // a breadth-first search has at most one level per vertex: past that a
+        // replayed loop is stopped whatever the counters say
+        if (level + 1 > p.nodes) {
+            atomicOr(&p.st->error, kErrLevels);
+            stop = true;
+        }
+        const int qn = stop ? 0 : qe_count(ld_cg64(&p.st->qe[next_pass % 3]));
+        const bool done = stop || (qn == 0) || limit_hit || (ld_cg(&p.st->error) != 0);
         if (done) p.st->done = 1;
         if (p.cond_handle) cudaGraphSetConditional((cudaGraphConditionalHandle)p.cond_handle, done ? 0u : 1u);
     }
@@ -771,8 +780,9 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             p.st->cur_level = level;
             p.st->done = 1;
         }
-    } else if (worked || limit_hit) {
-        finish_launch(p, level, level + 1, limit_hit);
+    } else {
+        // a launch that broke out before its level (empty frontier, error) stops the search
+        finish_launch(p, level, level + 1, limit_hit, !(worked || limit_hit));
     }
 }
 
@@ -856,6 +866,10 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
         }
     } else if (completed_level || limit_hit) {
         finish_launch(p, level, 2 * (level + 1), limit_hit);
+    } else if (p.phase_mask & 2) {
+        // an expand launch that broke out (overflow, error) stops the search; a
+        // contract-only launch leaves the level's epilogue to its expand launch
+        finish_launch(p, level, 2 * (level + 1), false, true);
     }
 }
 

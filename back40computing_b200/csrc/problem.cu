@@ -244,6 +244,8 @@ int check_state_errors(b40c_bfs_problem *p)
     if (e & dev::kErrOverflow)
         return b40c::fail(B40C_ERROR_INVALID_CONFIGURATION,
                           "Frontier queue overflow.  Please increase queue-sizing factor.");
+    if (e & dev::kErrLevels)
+        return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a replayed search ran more levels than the graph has vertices");
     if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk | dev::kErrInjected))
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a bounded device-side wait expired (error bits 0x%x)", e);
     return B40C_SUCCESS;

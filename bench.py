@@ -196,17 +196,21 @@ def cpu_search_fn():
 
 def cpu_baseline(g, srcs, deg, budget_s):
     """Serial CPU BFS on a bounded sample of the sources (one core)."""
+    import resource
     run, kind = cpu_search_fn()
-    edges, t, used = 0, 0.0, 0
+    edges, t, used, user = 0, 0.0, 0, 0.0
     for s in srcs:
+        u0 = resource.getrusage(resource.RUSAGE_THREAD).ru_utime
         t0 = time.perf_counter()
         labels = run(g.row_offsets, g.column_indices, s)
         t += time.perf_counter() - t0
+        user += resource.getrusage(resource.RUSAGE_THREAD).ru_utime - u0
         edges += visited(deg, labels)[1]
         used += 1
         if t >= budget_s:
             break
     return {"value": edges / t / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
+            "host_cores": os.cpu_count(), "wall_s": t, "user_cpu_s": user,
             "sample": f"{used} of {len(srcs)} sources, serial SimpleReferenceBfs, wall clock ({t:.1f} s)"}
 
 
@@ -257,7 +261,9 @@ def run_reference(args, rank):
 def batched_extra(steps, warmup):
     """64-source batched search on the random 2^21 x 16 symmetrised graph against 64
     one-at-a-time plain searches (direction-optimizing and expand-contract) on the
-    same GPU; labels of two slots are checked against the oracle."""
+    same GPU; labels and search depths of two slots are checked against the oracle.
+    Algorithmic bytes of a batch: 4 * sum_v deg(v) * L_v + 4 * sum_s V_c(s), L_v =
+    the number of distinct levels at which v is in some source's frontier."""
     import oracle
     from back40computing_b200 import CsrProblem, sample_sources
     from back40computing_b200 import _native as N
@@ -267,14 +273,22 @@ def batched_extra(steps, warmup):
     srcs = sample_sources(g, 64, seed=0)
     p = CsrProblem.from_graph(g)
     p.msbfs(srcs)
-    ec = []
+    depths = p.msbfs_depths()
+    ec, vc = [], []
+    levels = np.zeros(g.nodes, np.uint64)
     for slot in range(64):
         lab = p.labels_of(slot)
-        ec.append(visited(deg, lab)[1])
+        v, e = visited(deg, lab)
+        ec.append(e)
+        vc.append(v)
+        m = lab >= 0
+        levels[m] |= np.left_shift(np.uint64(1), lab[m].astype(np.uint64))
         if slot in (0, 37):
-            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
-            if oracle.compare_labels(lab, want) != -1:
+            want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
+            if oracle.compare_labels(lab, want) != -1 or depths[slot] != depth:
                 raise SystemExit("batched parity failure against the oracle")
+    lv = np.bitwise_count(levels).astype(np.int64)
+    balg = 4.0 * float((deg * lv).sum()) + 4.0 * float(sum(vc))
     for _ in range(warmup):
         p.msbfs(srcs)
     for _ in range(steps):
@@ -289,9 +303,13 @@ def batched_extra(steps, warmup):
         seq[STRATEGY_NAMES[st]] = float(p.recent_search_ms(64).sum())
     total = float(sum(ec))
     best_seq = min(seq.values())
+    peak, _ = measured_peak()
+    achieved = balg / (batch_ms * 1e-3) / 1e9
     out = {"workload": CONFIGS["random21"]["workload"], "batch_ms": batch_ms,
            "gteps": total / (batch_ms * 1e-3) / 1e9, "queries_per_s": 64 / (batch_ms * 1e-3),
-           "sequential_ms": seq, "speedup_vs_best_sequential": best_seq / batch_ms}
+           "sequential_ms": seq, "speedup_vs_best_sequential": best_seq / batch_ms,
+           "roofline": {"bytes_per_batch_alg": balg, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak}}
     p.Destroy()
     return out
 

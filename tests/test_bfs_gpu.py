@@ -336,3 +336,21 @@ def test_many_queued_enacts_wrap_the_source_ring():
         N.check(e._enact(p, int(srcs[i % 7]), N.ENACT_FUSED, 0))
     want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[299 % 7]))
     assert oracle.compare_labels(p.labels(), want) == -1
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+@pytest.mark.parametrize("mode", MODES)
+def test_source_without_edges(strategy, mode):
+    """A source with no edges: an empty first frontier must end the search in
+    every mode (in a captured graph the loop condition is set to stop)."""
+    g = _graph("rmat", 1 << 12, 1 << 15)
+    deg = np.diff(g.row_offsets)
+    iso = int(np.flatnonzero(deg == 0)[0])
+    p = CsrProblem.from_graph(g)
+    for s in (iso, int(sample_sources(g, 1, seed=4)[0]), iso):
+        got = search(p, s, strategy=strategy, mode=mode)
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, s)
+        assert oracle.compare_labels(got, want) == -1
+        e = ENACTORS[strategy]()
+        e._problem = p
+        assert e.GetStatistics()[1] == depth
