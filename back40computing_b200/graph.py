@@ -7,6 +7,8 @@ the library's native multi-threaded builders through the C ABI.
 from __future__ import annotations
 
 import ctypes as C
+import os
+import sys
 
 import numpy as np
 
@@ -133,6 +135,34 @@ def BuildRandomRegularishGraph(nodes: int, degree: int, graph: CsrGraph, seed: i
                                symmetrize: bool = False) -> int:
     """rr.cuh:53-91 with a seeded generator; optionally symmetrised."""
     return _build("b40c_build_rr", graph, int(nodes), int(degree), int(bool(symmetrize)), int(seed))
+
+
+def _read(fn_name: str, graph: CsrGraph, path, *args) -> int:
+    """Runs a reader; returns 0, or -1 with the parse error printed (the
+    reference builders' convention)."""
+    csr = N.Csr()
+    p = None if path is None else os.fsencode(path)
+    rc = getattr(N.lib(), fn_name)(p, *args, int(graph.pinned), C.byref(csr))
+    if rc != N.SUCCESS:
+        print(f"{fn_name}: {N.lib().b40c_last_error_string().decode(errors='replace')}", file=sys.stderr)
+        return -1
+    graph._adopt(csr)
+    return 0
+
+
+def BuildMarketGraph(path, graph: CsrGraph, undirected: bool) -> int:
+    """market.cuh:180-208 (ReadMarketStream :49-160).  path None = stdin."""
+    return _read("b40c_read_market", graph, path, int(bool(undirected)))
+
+
+def BuildDimacsGraph(path, graph: CsrGraph, undirected: bool, splice: int = 0) -> int:
+    """dimacs.cuh:235-283 (ReadDimacsStream :52-228); splice > 0 reads path.0, path.1, ..."""
+    return _read("b40c_read_dimacs", graph, path, int(bool(undirected)), int(splice))
+
+
+def BuildMetisGraph(path, graph: CsrGraph) -> int:
+    """metis.cuh:193-230 (ReadMetisStream :51-187).  path None = stdin."""
+    return _read("b40c_read_metis", graph, path)
 
 
 def sample_sources(graph: CsrGraph, count: int, seed: int = 0) -> np.ndarray:

@@ -285,6 +285,23 @@ int b40c_build_grid2d(int32_t width, int pinned, b40c_csr *out);
  * -x,+x,-y,+y,-z,+z, then a self-loop. */
 int b40c_build_grid3d(int32_t width, int pinned, b40c_csr *out);
 
+/* Graph files (path NULL = standard input).  Return 0, or
+ * B40C_ERROR_INVALID_VALUE with the parse error in b40c_last_error_string().
+ * Vertex ids in the files are 1-based; rows keep file order (FromCoo's
+ * stable by-row sort, csr_graph.cuh:109-152).
+ *   b40c_read_market  -- ReadMarketStream (market.cuh:49-160): "rows cols nnz",
+ *                        then "col row [value]" lines; `undirected` adds each
+ *                        entry's reverse edge right after it.
+ *   b40c_read_dimacs  -- ReadDimacsStream (dimacs.cuh:52-228): "p <type> n m",
+ *                        "a u v [w]" arcs; `splice` > 0 merges <path>.0,
+ *                        <path>.1, ... by smallest row; `undirected` adds each
+ *                        arc's reverse edge ahead of it.
+ *   b40c_read_metis   -- ReadMetisStream (metis.cuh:51-187): "n m", then one
+ *                        adjacency line per vertex; 2m (or m) ids expected. */
+int b40c_read_market(const char *path, int undirected, int pinned, b40c_csr *out);
+int b40c_read_dimacs(const char *path, int undirected, int splice, int pinned, b40c_csr *out);
+int b40c_read_metis(const char *path, int pinned, b40c_csr *out);
+
 /* BuildRmatGraph (rmat.cuh:128-206): `edges` R-MAT draws over `nodes` (a power
  * of two) with per-level +-5% parameter noise (VaryParams, rmat.cuh:83-116),
  * walk starting at u = v = 1 (rmat.cuh:167-169; the id `nodes` wraps to 0),

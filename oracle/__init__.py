@@ -80,6 +80,12 @@ def rlib():
         L.ref_build_rr.argtypes = [C.c_int32, C.c_int32, C.c_uint, PP, PP, _P64, _P64]
         L.ref_random_node.restype = C.c_int32
         L.ref_random_node.argtypes = [C.c_int32, C.c_uint, C.c_int]
+        L.ref_read_market.restype = C.c_int
+        L.ref_read_market.argtypes = [C.c_char_p, C.c_int, PP, PP, _P64, _P64]
+        L.ref_read_dimacs.restype = C.c_int
+        L.ref_read_dimacs.argtypes = [C.c_char_p, C.c_int, C.c_int, PP, PP, _P64, _P64]
+        L.ref_read_metis.restype = C.c_int
+        L.ref_read_metis.argtypes = [C.c_char_p, PP, PP, _P64, _P64]
         L.ref_free.restype = None
         L.ref_free.argtypes = [C.c_void_p]
         _r = L
@@ -144,6 +150,19 @@ def ref_build(kind, *args):
     rc = getattr(L, "ref_build_" + kind)(*args, C.byref(ro_p), C.byref(ci_p), C.byref(n), C.byref(m))
     if rc != 0:
         raise RuntimeError(f"reference builder {kind} failed")
+    return _take(L, ro_p, ci_p, n, m)
+
+
+def ref_read(kind, path, *args):
+    """Runs a reference graph reader (market / dimacs / metis) on a file;
+    returns (row_offsets, column_indices), or None when it reports an error."""
+    L = rlib()
+    ro_p, ci_p = _P32(), _P32()
+    n, m = C.c_int64(0), C.c_int64(0)
+    rc = getattr(L, "ref_read_" + kind)(os.fsencode(path), *args, C.byref(ro_p), C.byref(ci_p), C.byref(n),
+                                        C.byref(m))
+    if rc != 0:
+        return None
     return _take(L, ro_p, ci_p, n, m)
 
 

@@ -24,6 +24,11 @@
 #include <b40c/graph/builder/rmat.cuh>
 #include <b40c/graph/builder/random.cuh>
 #include <b40c/graph/builder/rr.cuh>
+#include <sstream>
+#include <vector>
+#include <b40c/graph/builder/market.cuh>
+#include <b40c/graph/builder/dimacs.cuh>
+#include <b40c/graph/builder/metis.cuh>
 
 using namespace b40c;
 using namespace b40c::graph;
@@ -135,6 +140,30 @@ extern "C" int32_t ref_random_node(int32_t nodes, unsigned seed, int reseed)
 {
     if (reseed) srand(seed);
     return builder::RandomNode(nodes);
+}
+
+// The reference's graph file readers (market.cuh, dimacs.cuh, metis.cuh).
+extern "C" int ref_read_market(const char *path, int undirected, int32_t **ro, int32_t **ci, int64_t *n,
+                               int64_t *m)
+{
+    Graph g;
+    if (builder::BuildMarketGraph<false>((char *)path, g, undirected != 0) != 0) return -1;
+    return take(g, ro, ci, n, m);
+}
+
+extern "C" int ref_read_dimacs(const char *path, int undirected, int splice, int32_t **ro, int32_t **ci,
+                               int64_t *n, int64_t *m)
+{
+    Graph g;
+    if (builder::BuildDimacsGraph<false>((char *)path, g, undirected != 0, splice) != 0) return -1;
+    return take(g, ro, ci, n, m);
+}
+
+extern "C" int ref_read_metis(const char *path, int32_t **ro, int32_t **ci, int64_t *n, int64_t *m)
+{
+    Graph g;
+    if (builder::BuildMetisGraph<false>((char *)path, g) != 0) return -1;
+    return take(g, ro, ci, n, m);
 }
 
 extern "C" void ref_free(void *p) { free(p); }

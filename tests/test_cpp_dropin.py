@@ -78,3 +78,30 @@ def test_dropin_driver_validates_on_gpu(exes, args):
     r = subprocess.run([exes["test_bfs_dropin"], *args], capture_output=True, text=True, timeout=300)
     assert r.returncode == 0, r.stdout[-2000:] + r.stderr[-2000:]
     assert r.stdout.count("CORRECT") >= 6 and "INCORRECT" not in r.stdout
+
+
+def test_file_readers_through_cpp_headers(exes, tmp_path):
+    """BuildMarketGraph / BuildDimacsGraph / BuildMetisGraph from the C++
+    headers give the graphs the Python readers give."""
+    from back40computing_b200 import CsrGraph, BuildMarketGraph, BuildDimacsGraph, BuildMetisGraph
+    rng = np.random.default_rng(5)
+    n, m = 120, 700
+    a, b = rng.integers(1, n + 1, m), rng.integers(1, n + 1, m)
+    mtx = tmp_path / "g.mtx"
+    mtx.write_text(f"%%MatrixMarket matrix coordinate pattern general\n{n} {n} {m}\n" +
+                   "".join(f"{x} {y}\n" for x, y in zip(a, b)))
+    gr = tmp_path / "g.gr"
+    gr.write_text(f"p sp {n} {m}\n" + "".join(f"a {x} {y} 1\n" for x, y in zip(a, b)))
+    met = tmp_path / "g.graph"
+    adj = [[] for _ in range(n)]
+    for x, y in zip(a, b):
+        adj[x - 1].append(y)
+    met.write_text(f"{n} {m}\n" + "".join(" ".join(map(str, row)) + "\n" for row in adj))
+    cases = [(("market", mtx, 1), lambda g: BuildMarketGraph(str(mtx), g, True)),
+             (("dimacs", gr, 0, 0), lambda g: BuildDimacsGraph(str(gr), g, False)),
+             (("metis", met), lambda g: BuildMetisGraph(str(met), g))]
+    for args, fn in cases:
+        ro, ci = _dump(exes["builder_dump"], str(tmp_path), 0, *args)
+        g = CsrGraph()
+        assert fn(g) == 0
+        assert np.array_equal(ro, g.row_offsets) and np.array_equal(ci, g.column_indices), args[0]
