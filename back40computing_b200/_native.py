@@ -173,6 +173,10 @@ SIGNATURES: dict[str, tuple] = {
                                   C.c_uint64, C.c_int, C.c_int, C.POINTER(Csr)]),
     "b40c_build_random": (C.c_int, [C.c_int64, C.c_int64, C.c_int, C.c_uint64, C.c_int, C.POINTER(Csr)]),
     "b40c_build_rr": (C.c_int, [C.c_int64, C.c_int32, C.c_int, C.c_uint64, C.c_int, C.POINTER(Csr)]),
+    "b40c_coo_to_csr_device": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64, C.c_int64, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]),
+    "b40c_bfs_problem_create_coo": (C.c_int, [_P_i32, _P_i32, C.c_int64, C.c_int64, C.c_int, C.c_int,
+                                              C.POINTER(C.c_void_p)]),
     "b40c_read_market": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.POINTER(Csr)]),
     "b40c_read_dimacs": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.POINTER(Csr)]),
     "b40c_read_metis": (C.c_int, [C.c_char_p, C.c_int, C.POINTER(Csr)]),

@@ -79,6 +79,21 @@ class CsrProblem:
                                   graph.row_offsets, 1), "FromHostProblem")
         return p
 
+    @classmethod
+    def from_coo(cls, rows, cols, nodes: int, mark_predecessors: bool = False, device: int = 0) -> "CsrProblem":
+        """A problem from a host COO edge list, converted to CSR on the GPU
+        (rows keep their input order, as CsrGraph::FromCoo)."""
+        r = np.ascontiguousarray(rows, dtype=np.int32)
+        c = np.ascontiguousarray(cols, dtype=np.int32)
+        p = cls(mark_predecessors, device)
+        h = C.c_void_p()
+        N.check(N.lib().b40c_bfs_problem_create_coo(N.i32p(r), N.i32p(c), int(nodes), int(r.size),
+                                                    int(bool(mark_predecessors)), int(device), C.byref(h)),
+                "b40c_bfs_problem_create_coo")
+        p._h = h
+        p.nodes, p.edges, p.num_gpus = int(nodes), int(r.size), 1
+        return p
+
     @property
     def handle(self) -> C.c_void_p:
         if not self._h:

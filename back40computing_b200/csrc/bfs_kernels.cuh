@@ -637,9 +637,10 @@ __device__ __forceinline__ void finish_launch(const BfsParams &p, int level, int
         __threadfence();
         p.st->finished = 0;
         if (!stop) p.st->cur_level = level + 1;
-        // a breadth-first search has at most one level per vertex: past that a
-        // replayed loop is stopped whatever the counters say
-        if (level + 1 > p.nodes) {
+        // a search has at most one level per vertex, plus the final empty
+        // contraction of the edge strategies: past that a replayed loop is
+        // stopped whatever the counters say
+        if (level > p.nodes) {
             atomicOr(&p.st->error, kErrLevels);
             stop = true;
         }

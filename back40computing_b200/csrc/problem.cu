@@ -1,4 +1,5 @@
 // Problem allocation, policies and the C ABI of the BFS library.
+#include <functional>
 #include <vector>
 
 #include "bfs_kernels.cuh"
@@ -417,6 +418,87 @@ int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode 
 }  // namespace rt
 }  // namespace b40c
 
+namespace b40c {
+namespace rt {
+
+int create_problem(int64_t nodes, int64_t edges, int mark_pred, int stream_from_host, int device,
+                   const std::function<int(b40c_bfs_problem *)> &load, b40c_bfs_problem **out)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) {
+        cudaGetLastError();
+        return b40c::fail(B40C_ERROR_NO_DEVICE, "no current CUDA device");
+    }
+    if (device >= ndev) return b40c::fail(B40C_ERROR_INVALID_VALUE, "invalid device %d", device);
+    DeviceGuard guard(device);
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (prop.major != 10)
+        return b40c::fail(B40C_ERROR_INVALID_DEVICE_FUNCTION, "kernels are built for sm_100a; device is sm_%d%d",
+                          prop.major, prop.minor);
+    auto *p = new b40c_bfs_problem();
+    p->device = device;
+    p->nodes = nodes;
+    p->edges = edges;
+    p->mark_pred = mark_pred ? 1 : 0;
+    p->stream_from_host = stream_from_host ? 1 : 0;
+    p->sms = prop.multiProcessorCount;
+    int rc = B40C_SUCCESS;
+    auto bail = [&](int code) {
+        b40c_bfs_problem_destroy(p);
+        return code;
+    };
+    if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "stream creation failed"));
+    }
+    p->stream = p->own_stream;
+    if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
+    }
+    for (int i = 0; i < b40c_bfs_problem::kRing; i++)
+        if (cudaEventCreate(&p->ring_a[i]) != cudaSuccess || cudaEventCreate(&p->ring_b[i]) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
+        }
+    if ((rc = load(p))) return bail(rc);
+    p->mask_words = (int32_t)((nodes + 31) / 32);
+    if ((rc = alloc_dev((void **)&p->d_labels, sizeof(int32_t) * nodes, "labels"))) return bail(rc);
+    if ((rc = alloc_dev((void **)&p->d_mask, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "visited mask")))
+        return bail(rc);
+    // second mask buffer: written whole by a bottom-up level before anything reads it
+    if ((rc = alloc_dev((void **)&p->d_next, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "second mask")))
+        return bail(rc);
+    if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
+    if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
+        cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "state allocation failed"));
+    }
+    memset(p->h_st, 0, sizeof(SearchState));
+    if (cudaMallocHost((void **)&p->h_src_ring, 2 * sizeof(int32_t) * b40c_bfs_problem::kRing) != cudaSuccess) {
+        cudaGetLastError();
+        p->h_src_ring = nullptr;
+        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "pinned source ring allocation failed"));
+    }
+    if ((rc = ensure_slots(p))) return bail(rc);
+    if (cudaStreamSynchronize(p->stream) != cudaSuccess) {
+        cudaError_t e = cudaGetLastError();
+        return bail(b40c::fail((int)e, "problem setup failed: %s", cudaGetErrorString(e)));
+    }
+    *out = p;
+    return B40C_SUCCESS;
+}
+
+}  // namespace rt
+}  // namespace b40c
+
+
 // ---- C ABI -----------------------------------------------------------------------------
 
 extern "C" {
@@ -470,109 +552,50 @@ int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t no
         if ((uint32_t)h_ci[e] >= (uint32_t)nodes)
             return b40c::fail(B40C_ERROR_INVALID_VALUE, "column index %d at edge %lld out of range", h_ci[e],
                               (long long)e);
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        return b40c::fail(B40C_ERROR_NO_DEVICE, "no CUDA device available");
-    }
-    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) {
-        cudaGetLastError();
-        return b40c::fail(B40C_ERROR_NO_DEVICE, "no current CUDA device");
-    }
-    if (device >= ndev) return b40c::fail(B40C_ERROR_INVALID_VALUE, "invalid device %d", device);
-    DeviceGuard guard(device);
-    cudaDeviceProp prop;
-    CUDA_TRY(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
-    if (prop.major != 10)
-        return b40c::fail(B40C_ERROR_INVALID_DEVICE_FUNCTION, "kernels are built for sm_100a; device is sm_%d%d",
-                          prop.major, prop.minor);
-    auto *p = new b40c_bfs_problem();
-    p->device = device;
-    p->nodes = nodes;
-    p->edges = edges;
-    p->mark_pred = mark_pred ? 1 : 0;
-    p->stream_from_host = stream_from_host ? 1 : 0;
-    p->sms = prop.multiProcessorCount;
-    int rc = B40C_SUCCESS;
-    auto bail = [&](int code) {
-        b40c_bfs_problem_destroy(p);
-        return code;
-    };
-    if (cudaStreamCreateWithFlags(&p->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
-        cudaGetLastError();
-        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "stream creation failed"));
-    }
-    p->stream = p->own_stream;
-    if (cudaEventCreate(&p->ev0) != cudaSuccess || cudaEventCreate(&p->ev1) != cudaSuccess) {
-        cudaGetLastError();
-        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
-    }
-    for (int i = 0; i < b40c_bfs_problem::kRing; i++)
-        if (cudaEventCreate(&p->ring_a[i]) != cudaSuccess || cudaEventCreate(&p->ring_b[i]) != cudaSuccess) {
-            cudaGetLastError();
-            return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "event creation failed"));
-        }
-    if (p->stream_from_host) {
-        // zero-copy: the kernels read the caller's host arrays over the bus
-        // (csr_problem.cuh:351-363); pin them in place when they are not pinned yet
-        const void *arrs[2] = {h_ro, h_ci};
-        const size_t bytes[2] = {sizeof(int32_t) * (size_t)(nodes + 1), sizeof(int32_t) * (size_t)std::max<int64_t>(edges, 1)};
-        int32_t **dst[2] = {&p->d_ro, &p->d_ci};
-        for (int i = 0; i < 2; i++) {
-            cudaPointerAttributes attr;
-            cudaError_t e = cudaPointerGetAttributes(&attr, arrs[i]);
-            if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
-                cudaGetLastError();
-                e = cudaHostRegister((void *)arrs[i], bytes[i], cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+    auto load = [&](b40c_bfs_problem *p) -> int {
+        if (p->stream_from_host) {
+            // zero-copy: the kernels read the caller's host arrays over the bus
+            // (csr_problem.cuh:351-363); pin them in place when they are not pinned yet
+            const void *arrs[2] = {h_ro, h_ci};
+            const size_t bytes[2] = {sizeof(int32_t) * (size_t)(nodes + 1),
+                                     sizeof(int32_t) * (size_t)std::max<int64_t>(edges, 1)};
+            int32_t **dst[2] = {&p->d_ro, &p->d_ci};
+            for (int i = 0; i < 2; i++) {
+                cudaPointerAttributes attr;
+                cudaError_t e = cudaPointerGetAttributes(&attr, arrs[i]);
+                if (e != cudaSuccess || attr.type != cudaMemoryTypeHost) {
+                    cudaGetLastError();
+                    e = cudaHostRegister((void *)arrs[i], bytes[i], cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+                    if (e != cudaSuccess) {
+                        cudaGetLastError();
+                        return b40c::fail((int)e, "cudaHostRegister for stream-from-host failed: %s",
+                                          cudaGetErrorString(e));
+                    }
+                    (i == 0 ? p->reg_ro : p->reg_ci) = arrs[i];
+                }
+                e = cudaHostGetDevicePointer((void **)dst[i], (void *)arrs[i], 0);
                 if (e != cudaSuccess) {
                     cudaGetLastError();
-                    return bail(b40c::fail((int)e, "cudaHostRegister for stream-from-host failed: %s", cudaGetErrorString(e)));
+                    return b40c::fail((int)e, "cudaHostGetDevicePointer failed: %s", cudaGetErrorString(e));
                 }
-                (i == 0 ? p->reg_ro : p->reg_ci) = arrs[i];
             }
-            e = cudaHostGetDevicePointer((void **)dst[i], (void *)arrs[i], 0);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                return bail(b40c::fail((int)e, "cudaHostGetDevicePointer failed: %s", cudaGetErrorString(e)));
-            }
+            p->own_csr = false;
+            return B40C_SUCCESS;
         }
-        p->own_csr = false;
-    } else {
-        if ((rc = alloc_dev((void **)&p->d_ro, sizeof(int32_t) * (nodes + 1), "row offsets"))) return bail(rc);
+        int rc;
+        if ((rc = alloc_dev((void **)&p->d_ro, sizeof(int32_t) * (nodes + 1), "row offsets"))) return rc;
         if ((rc = alloc_dev((void **)&p->d_ci, sizeof(int32_t) * std::max<int64_t>(edges, 1), "column indices")))
-            return bail(rc);
-        if (cudaMemcpyAsync(p->d_ro, h_ro, sizeof(int32_t) * (nodes + 1), cudaMemcpyHostToDevice, p->stream) != cudaSuccess ||
-            (edges > 0 && cudaMemcpyAsync(p->d_ci, h_ci, sizeof(int32_t) * edges, cudaMemcpyHostToDevice, p->stream) != cudaSuccess)) {
+            return rc;
+        if (cudaMemcpyAsync(p->d_ro, h_ro, sizeof(int32_t) * (nodes + 1), cudaMemcpyHostToDevice, p->stream) !=
+                cudaSuccess ||
+            (edges > 0 &&
+             cudaMemcpyAsync(p->d_ci, h_ci, sizeof(int32_t) * edges, cudaMemcpyHostToDevice, p->stream) != cudaSuccess)) {
             cudaGetLastError();
-            return bail(b40c::fail(B40C_ERROR_INVALID_VALUE, "CSR upload failed"));
+            return b40c::fail(B40C_ERROR_INVALID_VALUE, "CSR upload failed");
         }
-    }
-    p->mask_words = (int32_t)((nodes + 31) / 32);
-    if ((rc = alloc_dev((void **)&p->d_labels, sizeof(int32_t) * nodes, "labels"))) return bail(rc);
-    if ((rc = alloc_dev((void **)&p->d_mask, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "visited mask")))
-        return bail(rc);
-    // second mask buffer: written whole by a bottom-up level before anything reads it
-    if ((rc = alloc_dev((void **)&p->d_next, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "second mask")))
-        return bail(rc);
-    if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
-    if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
-        cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {
-        cudaGetLastError();
-        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "state allocation failed"));
-    }
-    memset(p->h_st, 0, sizeof(SearchState));
-    if (cudaMallocHost((void **)&p->h_src_ring, 2 * sizeof(int32_t) * b40c_bfs_problem::kRing) != cudaSuccess) {
-        cudaGetLastError();
-        p->h_src_ring = nullptr;
-        return bail(b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "pinned source ring allocation failed"));
-    }
-    if ((rc = ensure_slots(p))) return bail(rc);
-    if (cudaStreamSynchronize(p->stream) != cudaSuccess) {
-        cudaError_t e = cudaGetLastError();
-        return bail(b40c::fail((int)e, "problem setup failed: %s", cudaGetErrorString(e)));
-    }
-    *out = p;
-    return B40C_SUCCESS;
+        return B40C_SUCCESS;
+    };
+    return rt::create_problem(nodes, edges, mark_pred, stream_from_host, device, load, out);
 }
 
 int b40c_bfs_problem_destroy(b40c_bfs_problem *p)

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 
 #include "b40c_bfs.h"
 #include "bfs_state.h"
@@ -117,6 +118,10 @@ int ensure_vf(b40c_bfs_problem *p, int i, int64_t cap);
 int ensure_ef(b40c_bfs_problem *p, int i, int64_t cap);
 int64_t cap_of(double qs, int64_t base);
 int64_t device_bytes(const b40c_bfs_problem *p);
+// A problem handle whose CSR arrays `load` fills (upload, zero-copy mapping or
+// a device-side build); everything else is allocated here.
+int create_problem(int64_t nodes, int64_t edges, int mark_pred, int stream_from_host, int device,
+                   const std::function<int(b40c_bfs_problem *)> &load, b40c_bfs_problem **out);
 int64_t planned_bytes(int64_t n, int64_t m, int k, double qs);
 int ensure_slots(b40c_bfs_problem *p);
 BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol);

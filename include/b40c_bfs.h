@@ -285,6 +285,20 @@ int b40c_build_grid2d(int32_t width, int pinned, b40c_csr *out);
  * -x,+x,-y,+y,-z,+z, then a self-loop. */
 int b40c_build_grid3d(int32_t width, int pinned, b40c_csr *out);
 
+/* COO -> CSR on the GPU (CsrGraph::FromCoo, csr_graph.cuh:109-152, done on
+ * the device): d_rows/d_cols[edges] device arrays of 0-based ids are turned
+ * into d_row_offsets[nodes + 1] and d_column_indices[edges] with rows in
+ * input order (a stable radix sort by row).  Ids outside [0, nodes) return
+ * B40C_ERROR_INVALID_VALUE.  Synchronous on cuda_stream; temporary device
+ * memory of about 16 bytes per edge is allocated and freed inside. */
+int b40c_coo_to_csr_device(const int32_t *d_rows, const int32_t *d_cols, int64_t nodes, int64_t edges,
+                           int32_t *d_row_offsets, int32_t *d_column_indices, void *cuda_stream);
+
+/* A problem handle built from a host COO edge list (FromCoo + FromHostProblem
+ * in one step): the list is uploaded and converted on the GPU. */
+int b40c_bfs_problem_create_coo(const int32_t *h_rows, const int32_t *h_cols, int64_t nodes, int64_t edges,
+                                int mark_predecessors, int device, b40c_bfs_problem **out);
+
 /* Graph files (path NULL = standard input).  Return 0, or
  * B40C_ERROR_INVALID_VALUE with the parse error in b40c_last_error_string().
  * Vertex ids in the files are 1-based; rows keep file order (FromCoo's
