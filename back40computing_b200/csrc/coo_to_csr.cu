@@ -281,7 +281,7 @@ int b40c_coo_to_csr_device(const int32_t *d_rows, const int32_t *d_cols, int64_t
                            int32_t *d_row_offsets, int32_t *d_column_indices, void *cuda_stream)
 {
     b40c::clear_error();
-    if (!d_rows || !d_cols || !d_row_offsets || (!d_column_indices && edges > 0) || nodes <= 0 || edges < 0 ||
+    if (((!d_rows || !d_cols || !d_column_indices) && edges > 0) || !d_row_offsets || nodes <= 0 || edges < 0 ||
         nodes >= INT32_MAX || edges >= INT32_MAX)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "b40c_coo_to_csr_device: bad arguments");
     int device = 0, sms = 0;
