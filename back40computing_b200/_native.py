@@ -43,6 +43,7 @@ class Policy(C.Structure):
         ("bottom_up_alpha", C.c_int32),
         ("bottom_up_beta", C.c_int32),
         ("small_frontier_edges", C.c_int32),
+        ("bottom_up_scan", C.c_int32),
     ]
 
 

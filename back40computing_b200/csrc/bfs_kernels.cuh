@@ -56,6 +56,7 @@ struct ExpandSmem {
     unsigned long long visited_edges;  // degree sum of the vertices visited up to this pass
     int32_t prev_bu;                   // the previous level ran bottom-up
     uint32_t *mask;                    // the visited-mask buffer of this pass (mask or mask_alt)
+    int32_t wl_count;                  // bottom-up worklist entries of the current chunk
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -434,6 +435,170 @@ constexpr int kBottomUpLongList = 256;  // lists longer than this are searched w
 // whole warp, 32 neighbours at a time).
 constexpr int kBottomUpProbe = 2;
 
+// Bottom-up continuation, one lane per vertex: each lane scans its own list
+// on, four neighbours at a time; lists longer than kBottomUpLongList are
+// searched by the whole warp, 32 neighbours at a time.
+template <int PER, int K>
+__device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, const bool (&todo)[PER],
+                                                const int (&r0)[PER], const int (&r1)[PER], int (&parent)[PER])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
+        if (!__any_sync(0xffffffffu, more)) continue;
+        const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
+        bool scan = more && !longlist;
+        int e = r0[t] + K;
+        while (__any_sync(0xffffffffu, scan)) {
+            if (scan) {
+                int nb[4];
+                unsigned w[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) nb[k] = (e + k < r1[t]) ? ld_stream(p.column_indices + e + k) : -1;
+#pragma unroll
+                for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (parent[t] < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent[t] = nb[k];
+                e += 4;
+                if (parent[t] >= 0 || e >= r1[t]) scan = false;
+            }
+        }
+        unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+        while (lmask) {
+            const int owner = __ffs(lmask) - 1;
+            lmask &= lmask - 1;
+            const int lr0 = __shfl_sync(0xffffffffu, r0[t], owner) + K;
+            const int lr1 = __shfl_sync(0xffffffffu, r1[t], owner);
+            int found_u = -1;
+            for (int eb = lr0; eb < lr1; eb += 32) {
+                const int ee = eb + lane;
+                const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
+                const bool hit = nb >= 0 && ((ld_mask(mask + (nb >> 5)) >> (nb & 31)) & 1u);
+                const unsigned hb = __ballot_sync(0xffffffffu, hit);
+                if (hb) {
+                    found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
+                    break;
+                }
+            }
+            if (lane == owner) parent[t] = found_u;
+        }
+    }
+}
+
+// Bottom-up continuation, the CTA together: the unresolved vertices of the
+// chunk (no parent among their first K neighbours, more neighbours left) form
+// a shared worklist (colstart = next edge, rel = remaining edges, then their
+// exclusive scan; out = parent found); its edges are then scanned
+// edge-parallel in rounds of kChunkMax positions, each thread issuing PER
+// independent neighbour loads and mask probes per round, skipping vertices
+// resolved in earlier rounds.  Any visited neighbour is a valid parent (all
+// are one level up); several hits for one vertex simply overwrite each other.
+template <int B, bool PRED, int PER, int K>
+__device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSmem<B, PRED> &s, const uint32_t *mask,
+                                                   const bool (&todo)[PER], const int (&r0)[PER],
+                                                   const int (&r1)[PER], int (&parent)[PER])
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) s.wl_count = 0;
+    __syncthreads();
+    // a candidate's worklist slot is kept in stage[t * B + tid] (free during
+    // bottom-up levels), not in registers
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
+        const unsigned bal = __ballot_sync(0xffffffffu, more);
+        if (bal == 0) continue;
+        const int leader = __ffs(bal) - 1;
+        int base = 0;
+        if (lane == leader) base = atomicAdd(&s.wl_count, __popc(bal));
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (more) {
+            const int sl = base + __popc(bal & lanemask_lt());
+            s.stage[t * B + tid] = sl;
+            s.colstart[sl] = r0[t] + K;
+            s.rel[sl] = r1[t] - r0[t] - K;
+            s.out[sl] = -1;
+        }
+    }
+    __syncthreads();
+    const int W = s.wl_count;
+    if (W == 0) return;  // CTA-uniform
+    // exclusive scan of the remaining lengths, in place, with the total at rel[W]
+    {
+        int loc[PER];
+        unsigned long long sum = 0;
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int i = tid * PER + k;
+            loc[k] = i < W ? s.rel[i] : 0;
+            sum += (unsigned long long)loc[k];
+        }
+        unsigned long long total;
+        unsigned long long run = cta_exclusive_scan<B>(sum, s.scan_warp, &total);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < PER; k++) {
+            const int i = tid * PER + k;
+            if (i < W) s.rel[i] = (int)run;
+            run += (unsigned long long)loc[k];
+        }
+        if (tid == 0) s.rel[W] = (int)total;
+    }
+    __syncthreads();
+    const int D = s.rel[W];
+    for (int base = 0; base < D; base += kChunkMax) {
+        const int len = min(kChunkMax, D - base);
+        // owner map of this round's positions (entries have nonzero lengths)
+        {
+            const int x0 = tid * PER;
+            if (x0 < len) {
+                int lo = 0, hi = W - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi + 1) >> 1;
+                    if (s.rel[mid] <= base + x0) lo = mid; else hi = mid - 1;
+                }
+                int j = lo;
+                int next = s.rel[j + 1];
+#pragma unroll
+                for (int k = 0; k < PER; k++) {
+                    const int x = x0 + k;
+                    if (x < len) {
+                        while (base + x >= next) {
+                            j++;
+                            next = s.rel[j + 1];
+                        }
+                        s.own[x] = (uint16_t)j;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        int nb[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) {
+            const int x = u * B + tid;
+            nb[u] = -1;
+            if (x < len) {
+                const int j = s.own[x];
+                if (s.out[j] < 0) nb[u] = ld_stream(p.column_indices + s.colstart[j] + (base + x - s.rel[j]));
+            }
+        }
+        unsigned w[PER];
+#pragma unroll
+        for (int u = 0; u < PER; u++) w[u] = nb[u] >= 0 ? ld_mask(mask + (nb[u] >> 5)) : 0u;
+#pragma unroll
+        for (int u = 0; u < PER; u++)
+            if (nb[u] >= 0 && ((w[u] >> (nb[u] & 31)) & 1u)) s.out[s.own[u * B + tid]] = nb[u];
+        __syncthreads();
+    }
+#pragma unroll
+    for (int t = 0; t < PER; t++)
+        if (todo[t] && parent[t] < 0 && r1[t] - r0[t] > K) parent[t] = s.out[s.stage[t * B + tid]];
+    __syncthreads();  // the output phase reuses colstart / rel / out
+}
+
 template <int B, bool PRED>
 __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
                                                 const VertexFrontier &vout, unsigned long long *qe_out)
@@ -490,48 +655,10 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             }
         }
         // ---- continue the scan for candidates still without a parent ---------------
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
-            if (!__any_sync(0xffffffffu, more)) continue;
-            const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
-            bool scan = more && !longlist;
-            int e = r0[t] + K;
-            while (__any_sync(0xffffffffu, scan)) {
-                if (scan) {
-                    int nb[4];
-                    unsigned w[4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) nb[k] = (e + k < r1[t]) ? ld_stream(p.column_indices + e + k) : -1;
-#pragma unroll
-                    for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
-#pragma unroll
-                    for (int k = 0; k < 4; k++)
-                        if (parent[t] < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent[t] = nb[k];
-                    e += 4;
-                    if (parent[t] >= 0 || e >= r1[t]) scan = false;
-                }
-            }
-            unsigned lmask = __ballot_sync(0xffffffffu, longlist);
-            while (lmask) {
-                const int owner = __ffs(lmask) - 1;
-                lmask &= lmask - 1;
-                const int lr0 = __shfl_sync(0xffffffffu, r0[t], owner) + K;
-                const int lr1 = __shfl_sync(0xffffffffu, r1[t], owner);
-                int found_u = -1;
-                for (int eb = lr0; eb < lr1; eb += 32) {
-                    const int ee = eb + lane;
-                    const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
-                    const bool hit = nb >= 0 && ((ld_mask(mask + (nb >> 5)) >> (nb & 31)) & 1u);
-                    const unsigned hb = __ballot_sync(0xffffffffu, hit);
-                    if (hb) {
-                        found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
-                        break;
-                    }
-                }
-                if (lane == owner) parent[t] = found_u;
-            }
-        }
+        if (p.bu_scan == 2)
+            bottom_up_worklist<B, PRED, PER, K>(p, s, mask, todo, r0, r1, parent);
+        else
+            bottom_up_lanes<PER, K>(p, mask, todo, r0, r1, parent);
         // ---- label, mark and append the discoveries --------------------------------
 #pragma unroll
         for (int t = 0; t < PER; t++) {

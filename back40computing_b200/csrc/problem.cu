@@ -126,6 +126,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.bu_beta = pol.bottom_up_beta;
     k.mask_alt = p->d_next;
     k.small_edges = pol.small_frontier_edges;
+    k.bu_scan = pol.bottom_up_scan;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
     k.cond_handle = 0;
@@ -146,6 +147,7 @@ b40c_bfs_policy default_policy(int strategy)
     pol.bottom_up_alpha = 14;  // Beamer et al.'s defaults
     pol.bottom_up_beta = 24;
     pol.small_frontier_edges = 1024;
+    pol.bottom_up_scan = 2;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     (void)strategy;
     return pol;
@@ -167,6 +169,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->bottom_up_alpha) d.bottom_up_alpha = in->bottom_up_alpha;
         if (in->bottom_up_beta) d.bottom_up_beta = in->bottom_up_beta;
         if (in->small_frontier_edges) d.small_frontier_edges = in->small_frontier_edges;
+        if (in->bottom_up_scan) d.bottom_up_scan = in->bottom_up_scan;
     }
     if (d.threads != kThreads)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: %d)", d.threads, kThreads);
@@ -182,6 +185,8 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     if (d.bottom_up_alpha < 1 || d.bottom_up_beta < 1)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_alpha and bottom_up_beta must be >= 1");
     if (d.saturation_quit < 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.saturation_quit must be >= 1");
+    if (d.bottom_up_scan != 1 && d.bottom_up_scan != 2)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_scan must be 1 (per lane) or 2 (per CTA)");
     if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
     *out = d;
     return B40C_SUCCESS;

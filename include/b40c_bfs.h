@@ -74,7 +74,7 @@ enum {
  * template parameters, e.g. enactor_contract_expand.cuh:339-373).  A zero
  * field means "use the tuned default". */
 typedef struct b40c_bfs_policy {
-    int32_t threads;               /* CTA size: 128, 256 or 512 */
+    int32_t threads;               /* CTA size (256: the size the kernels are built for) */
     int32_t ctas_per_sm;           /* resident CTAs per SM for persistent grids (0 = occupancy limit) */
     int32_t chunk_edges;           /* edges per CTA work chunk in the edge-balanced expansion (<= 4096) */
     int32_t warp_gather_threshold; /* run length at or above which a warp gathers cooperatively (>= 32) */
@@ -93,6 +93,10 @@ typedef struct b40c_bfs_policy {
     int32_t small_frontier_edges;  /* fused searches: runs of levels whose frontier has at most this many
                                       edges are processed by one CTA alone (CTA-level barriers only);
                                       -1 disables */
+    int32_t bottom_up_scan;        /* bottom-up levels, vertices whose first neighbours are not yet
+                                      visited: 1 = each lane scans its own list on (lists longer than 256
+                                      by the whole warp), 2 = the CTA scans all such lists together,
+                                      edge-parallel; 0 = default */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

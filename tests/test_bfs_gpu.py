@@ -354,3 +354,24 @@ def test_source_without_edges(strategy, mode):
         e = ENACTORS[strategy]()
         e._problem = p
         assert e.GetStatistics()[1] == depth
+
+
+@pytest.mark.parametrize("scan", [1, 2])
+@pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 15, 12)), ("grid3d", (24,))])
+@pytest.mark.parametrize("preds", [False, True])
+def test_bottom_up_scan_variants(scan, kind, args, preds):
+    """Both bottom-up continuations (per lane, CTA worklist) give the oracle's
+    distances and valid predecessors; alpha 2 forces many bottom-up levels."""
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g, mark_predecessors=preds)
+    pol = N.Policy()
+    pol.bottom_up_scan = scan
+    pol.bottom_up_alpha = 2
+    for s in sample_sources(g, 3, seed=9):
+        got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, policy=pol)
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        if preds:
+            assert got[s] == -2
+            assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+        else:
+            assert oracle.compare_labels(got, want) == -1
