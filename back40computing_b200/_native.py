@@ -156,6 +156,7 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_bfs_problem_is_symmetric": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_set_instrument": (C.c_int, [C.c_void_p, C.c_int]),
     "b40c_bfs_level_records": (C.c_int, [C.c_void_p, C.POINTER(LevelRecord), C.c_int, _P_i32]),
+    "b40c_bfs_cta_arrivals": (C.c_int, [C.c_void_p, C.POINTER(C.c_uint64), C.c_int, _P_i32]),
     "b40c_bfs_last_elapsed_ms": (C.c_int, [C.c_void_p, C.POINTER(C.c_float)]),
     "b40c_bfs_recent_search_ms": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_float)]),
     "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),

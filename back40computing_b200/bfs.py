@@ -141,6 +141,15 @@ class CsrProblem:
             a["ns"] = b["t_ns"] - a["t_ns"]
         return [r for r in recs if r["pass_"] >= 0]
 
+    def cta_arrivals(self, max_passes: int = 64) -> np.ndarray:
+        """[pass, cta] end-of-level barrier arrival times (ns) of the last
+        instrumented persistent search; 0 where a CTA did not arrive."""
+        buf = np.zeros(max_passes * 2048, dtype=np.uint64)
+        g = C.c_int32(0)
+        N.check(N.lib().b40c_bfs_cta_arrivals(self.handle, buf.ctypes.data_as(C.POINTER(C.c_uint64)),
+                                              int(max_passes), C.byref(g)), "cta_arrivals")
+        return buf[:max_passes * g.value].reshape(max_passes, g.value)
+
     # ---- batched multi-source searches ------------------------------------------------
     def msbfs(self, sources, depth_limits=None, policy: N.Policy | None = None, max_grid_size: int = 0) -> None:
         """Searches up to 64 sources together (asynchronous); see labels_of()."""

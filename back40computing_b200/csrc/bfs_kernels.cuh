@@ -220,7 +220,13 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
             vout.v[g] = s.out[j];
             vout.col[g] = s.colstart[j];
             vout.P[g] = (int)d;
-            for (unsigned c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) vout.cf[c] = (int)g;
+            for (unsigned c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) {
+                if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never written past the end
+                    atomicOr(&p.st->error, kErrOverflow);
+                    break;
+                }
+                vout.cf[c] = (int)g;
+            }
         } else {
             atomicOr(&p.st->error, kErrOverflow);
         }
@@ -788,6 +794,11 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
         s.q = qe_count(x);
         s.E = qe_edges(x);
         s.flag = 0;
+        if ((unsigned)s.E > (unsigned)p.edges || (unsigned)s.q > (unsigned)max(p.vcap, p.ecap)) {
+            // counters past the graph's size: stop before any frontier read
+            atomicOr(&p.st->error, kErrOverflow);
+            s.q = 0;
+        }
         if (blockIdx.x == 0) {
             p.st->qe[(pass + 2) % 3] = 0;
             p.st->tile_ctr[(pass + 1) % 3] = 0;
@@ -894,6 +905,8 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         worked = true;
         if (s.flag) max_level_seen = level + 1;
         if (!p.persistent) break;
+        if (p.arrive && tid == 0 && pass < kMaxArrivePasses && blockIdx.x < kMaxArriveCtas)
+            p.arrive[pass * kMaxArriveCtas + blockIdx.x] = globaltimer_ns();
         if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
         if ((int)blockIdx.x == p.skip_arrival_cta) {
             if (tid == 0) atomicOr(&p.st->error, kErrInjected);
@@ -1046,7 +1059,7 @@ __global__ void init_kernel(BfsParams p)
             p.vf[0].v[0] = src;
             p.vf[0].col[0] = r0;
             p.vf[0].P[0] = 0;
-            for (int c = 0; c * kChunkGrain < deg; c++) p.vf[0].cf[c] = 0;
+            for (int c = 0; c * kChunkGrain < deg && c < p.cf_cap; c++) p.vf[0].cf[c] = 0;
         } else {
             // edge frontier: the source is the only item; its predecessor is -2
             st->qe[0] = pack(1u, 0u);

@@ -78,6 +78,10 @@ struct LevelRecord {
     unsigned long long t_ns;   // %globaltimer when block 0 started the pass
 };
 constexpr int kMaxLevelRecords = 1 << 16;
+// Per-CTA arrival times at the end-of-level grid barrier, for the first
+// kMaxArrivePasses passes of an instrumented persistent search.
+constexpr int kMaxArrivePasses = 64;
+constexpr int kMaxArriveCtas = 2048;
 
 // Kernel parameter block.
 struct BfsParams {
@@ -91,6 +95,7 @@ struct BfsParams {
     int32_t vcap;  // vertex frontier capacity (entries)
     int32_t ecap;  // edge frontier capacity (entries)
     int32_t max_chunks;
+    int32_t cf_cap;  // entries of each vertex frontier's cf array (a level's edge total / kChunkGrain + 2)
     VertexFrontier vf[2];
     EdgeFrontier ef[2];
     dev::LookbackSlot *slots;
@@ -117,6 +122,7 @@ struct BfsParams {
                               // every word of the other (old bits | its discoveries), then they swap
     LevelRecord *levels;      // per-pass records when instrumented, else null
     unsigned long long *duty; // [0] sum over CTAs of busy ns, [1] sum of lifetime ns (instrumented)
+    unsigned long long *arrive;  // [pass][cta] %globaltimer at the end-of-level barrier (instrumented)
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
 };
 

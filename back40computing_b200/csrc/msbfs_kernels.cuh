@@ -311,6 +311,10 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             s.q = qe_count(x);
             s.E = qe_edges(x);
             s.flag = 0;
+            if ((unsigned)s.E > (unsigned)p.edges || (unsigned)s.q > (unsigned)p.vcap) {
+                atomicOr(&p.st->error, kErrOverflow);  // never read a frontier past its arrays
+                s.q = 0;
+            }
             s.found = 0;
             unsigned long long act = 0;
             for (int src = 0; src < m.k; src++)
@@ -432,7 +436,8 @@ __global__ void msbfs_seed_kernel(BfsParams p, MsParams m, int32_t *limits_out, 
                 p.vf[0].v[g] = v;
                 p.vf[0].col[g] = r0;
                 p.vf[0].P[g] = d;
-                for (int c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) p.vf[0].cf[c] = g;
+                for (int c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg && c < p.cf_cap; c++)
+                    p.vf[0].cf[c] = g;
                 g++;
                 d += deg;
             }

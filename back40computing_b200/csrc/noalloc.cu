@@ -138,6 +138,7 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
     k.vcap = (int32_t)kMaxNodes;
     k.ecap = 0;
     k.max_chunks = 0;
+    k.cf_cap = (int32_t)(kMaxEdges / dev::kChunkGrain + 2);
     k.slots = nullptr;
     k.st = st;
     k.max_levels = INT32_MAX;

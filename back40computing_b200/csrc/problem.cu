@@ -105,6 +105,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.vcap = (int32_t)std::min(p->vcap[0] ? p->vcap[0] : INT32_MAX, p->vcap[1] ? p->vcap[1] : INT32_MAX);
     k.ecap = (int32_t)std::min(p->ecap[0] ? p->ecap[0] : INT32_MAX, p->ecap[1] ? p->ecap[1] : INT32_MAX);
     k.max_chunks = p->max_slots;
+    k.cf_cap = (int32_t)((std::max<int64_t>(p->edges, 1) + dev::kChunkGrain - 1) / dev::kChunkGrain + 2);
     k.vf[0] = p->vf[0];
     k.vf[1] = p->vf[1];
     k.ef[0] = p->ef[0];
@@ -129,6 +130,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.bu_scan = pol.bottom_up_scan;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
+    k.arrive = p->instrument ? p->d_arrive : nullptr;
     k.cond_handle = 0;
     return k;
 }
@@ -215,6 +217,7 @@ int64_t device_bytes(const b40c_bfs_problem *p)
     if (p->d_ms_labels) t += a(4 * n * (int64_t)p->ms_labels_k);
     if (p->d_levels) t += a((int64_t)sizeof(LevelRecord) * kMaxLevelRecords);
     if (p->d_duty) t += a(4 * sizeof(unsigned long long));
+    if (p->d_arrive) t += a((int64_t)sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas);
     return t;
 }
 
@@ -269,6 +272,7 @@ int persistent_grid(b40c_bfs_problem *p, const void *kernel, const b40c_bfs_poli
     int g = per_sm * p->sms;
     if (max_grid > 0) g = std::min(g, max_grid);
     *grid = std::max(g, 1);
+    p->last_grid = *grid;
     return B40C_SUCCESS;
 }
 
@@ -343,6 +347,8 @@ int begin_instrumented(b40c_bfs_problem *p)
     if (!p->instrument) return B40C_SUCCESS;
     CUDA_TRY(cudaMemsetAsync(p->d_levels, 0, sizeof(LevelRecord) * kMaxLevelRecords, p->stream), "level records reset");
     CUDA_TRY(cudaMemsetAsync(p->d_duty, 0, 4 * sizeof(unsigned long long), p->stream), "duty reset");
+    CUDA_TRY(cudaMemsetAsync(p->d_arrive, 0, sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas, p->stream),
+             "arrival reset");
     return B40C_SUCCESS;
 }
 
@@ -622,6 +628,7 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     free_batch(p);
     if (p->d_levels) cudaFree(p->d_levels);
     if (p->d_duty) cudaFree(p->d_duty);
+    if (p->d_arrive) cudaFree(p->d_arrive);
     for (int i = 0; i < 2; i++) {
         free_vf(p->vf[i]);
         free_ef(p->ef[i]);
@@ -767,8 +774,30 @@ int b40c_bfs_set_instrument(b40c_bfs_problem *p, int on)
         int rc;
         if ((rc = alloc_dev((void **)&p->d_levels, sizeof(LevelRecord) * kMaxLevelRecords, "level records"))) return rc;
         if ((rc = alloc_dev((void **)&p->d_duty, 4 * sizeof(unsigned long long), "duty counters"))) return rc;
+        if ((rc = alloc_dev((void **)&p->d_arrive, sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas,
+                            "arrival times")))
+            return rc;
     }
     p->instrument = on != 0;
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_cta_arrivals(b40c_bfs_problem *p, uint64_t *out, int max_passes, int *ctas)
+{
+    b40c::clear_error();
+    if (!p || !out || !ctas || max_passes < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "bad arguments");
+    if (!p->instrument || !p->d_arrive)
+        return b40c::fail(B40C_ERROR_NOT_READY, "instrumentation is off (b40c_bfs_set_instrument)");
+    DeviceGuard guard(p->device);
+    const int passes = std::min(max_passes, kMaxArrivePasses);
+    const int g = std::min(p->last_grid, kMaxArriveCtas);
+    std::vector<unsigned long long> h((size_t)kMaxArrivePasses * kMaxArriveCtas);
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "stream synchronize");
+    CUDA_TRY(cudaMemcpy(h.data(), p->d_arrive, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost),
+             "arrival read");
+    for (int k = 0; k < passes; k++)
+        for (int c = 0; c < g; c++) out[(size_t)k * g + c] = h[(size_t)k * kMaxArriveCtas + c];
+    *ctas = g;
     return B40C_SUCCESS;
 }
 

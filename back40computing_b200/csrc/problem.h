@@ -55,6 +55,8 @@ struct b40c_bfs_problem {
     bool instrument = false;
     b40c::LevelRecord *d_levels = nullptr;
     unsigned long long *d_duty = nullptr;
+    unsigned long long *d_arrive = nullptr;  // [kMaxArrivePasses][kMaxArriveCtas]
+    int last_grid = 0;                       // CTAs of the last persistent launch
     // frontiers
     b40c::VertexFrontier vf[2] = {};
     int64_t vcap[2] = {0, 0};
