@@ -39,6 +39,16 @@ namespace dev {
 constexpr int kChunkMax = 2048;   // edges (or edge-frontier items) per sub-round
 constexpr int kChunkGrain = 256;  // CTA ranges start at multiples of this; granularity of the cf index
 
+// Output entries of one emit whose degree spans many kChunkGrain chunks: their
+// cf entries are written by the whole CTA instead of one thread.
+constexpr int kCfBigEntries = 32;
+constexpr unsigned kCfSerialChunks = 8;  // entries spanning more chunks than this go to CfBig
+struct CfBig {
+    int32_t count;
+    int32_t g[kCfBigEntries];
+    uint32_t c0[kCfBigEntries], c1[kCfBigEntries];
+};
+
 template <int B, bool PRED>
 struct ExpandSmem {
     // per-sub-round run tables; after the gather they hold the sub-round's
@@ -57,6 +67,7 @@ struct ExpandSmem {
     int32_t prev_bu;                   // the previous level ran bottom-up
     uint32_t *mask;                    // the visited-mask buffer of this pass (mask or mask_alt)
     int32_t wl_count;                  // bottom-up worklist entries of the current chunk
+    CfBig big;                         // emit_frontier: entries whose cf runs the CTA writes together
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -176,6 +187,7 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cnt = s.out_count;
+    if (tid == 0) s.big.count = 0;  // read after the scan's barriers
     constexpr int PER = kChunkMax / B;
     const int per = (cnt + B - 1) / B;
     const int jb = min(tid * per, cnt), je = min(jb + per, cnt);
@@ -220,18 +232,39 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
             vout.v[g] = s.out[j];
             vout.col[g] = s.colstart[j];
             vout.P[g] = (int)d;
-            for (unsigned c = (d + kChunkGrain - 1) / kChunkGrain; c * kChunkGrain < d + deg; c++) {
-                if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never written past the end
-                    atomicOr(&p.st->error, kErrOverflow);
-                    break;
+            // cf[c] = g for the chunks c starting inside [d, d + deg)
+            const unsigned c0 = (d + kChunkGrain - 1) / kChunkGrain, c1 = (d + deg + kChunkGrain - 1) / kChunkGrain;
+            int big = -1;
+            if (c1 - c0 > kCfSerialChunks) {
+                big = atomicAdd(&s.big.count, 1);
+                if (big < kCfBigEntries) {
+                    s.big.g[big] = (int)g;
+                    s.big.c0[big] = c0;
+                    s.big.c1[big] = c1;
                 }
-                vout.cf[c] = (int)g;
+            }
+            if (big < 0 || big >= kCfBigEntries) {
+                for (unsigned c = c0; c < c1; c++) {
+                    if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never past the end
+                        atomicOr(&p.st->error, kErrOverflow);
+                        break;
+                    }
+                    vout.cf[c] = (int)g;
+                }
             }
         } else {
             atomicOr(&p.st->error, kErrOverflow);
         }
         g++;
         d += deg;
+    }
+    __syncthreads();
+    // hub entries: their chunk runs are written by the whole CTA
+    const int nbig = min(s.big.count, kCfBigEntries);
+    for (int b = 0; b < nbig; b++) {
+        const unsigned c1 = min(s.big.c1[b], (unsigned)p.cf_cap);
+        if (tid == 0 && s.big.c1[b] > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);
+        for (unsigned c = s.big.c0[b] + tid; c < c1; c += B) vout.cf[c] = s.big.g[b];
     }
 }
 
@@ -440,11 +473,12 @@ constexpr int kBottomUpLongList = 256;  // lists longer than this are searched w
 // (short lists one lane each, four neighbours at a time; long lists by the
 // whole warp, 32 neighbours at a time).
 constexpr int kBottomUpProbe = 2;
+constexpr int kBottomUpLaneSteps = 4;  // bottom_up_scan 3: lane steps (4 neighbours each) before the worklist
 
 // Bottom-up continuation, one lane per vertex: each lane scans its own list
 // on, four neighbours at a time; lists longer than kBottomUpLongList are
 // searched by the whole warp, 32 neighbours at a time.
-template <int PER, int K>
+template <int PER, int K, int MAX_ITER>
 __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, const bool (&todo)[PER],
                                                 const int (&r0)[PER], const int (&r1)[PER], int (&parent)[PER])
 {
@@ -453,9 +487,11 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
     for (int t = 0; t < PER; t++) {
         const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
         if (!__any_sync(0xffffffffu, more)) continue;
-        const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
+        // capped: no warp-cooperative lists, at most MAX_ITER steps per lane
+        const bool longlist = MAX_ITER == 0 && more && (r1[t] - r0[t]) > kBottomUpLongList;
         bool scan = more && !longlist;
         int e = r0[t] + K;
+        int iter = 0;
         while (__any_sync(0xffffffffu, scan)) {
             if (scan) {
                 int nb[4];
@@ -470,6 +506,7 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
                 e += 4;
                 if (parent[t] >= 0 || e >= r1[t]) scan = false;
             }
+            if (MAX_ITER > 0 && ++iter >= MAX_ITER) break;  // warp-uniform
         }
         unsigned lmask = __ballot_sync(0xffffffffu, longlist);
         while (lmask) {
@@ -501,7 +538,7 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
 // independent neighbour loads and mask probes per round, skipping vertices
 // resolved in earlier rounds.  Any visited neighbour is a valid parent (all
 // are one level up); several hits for one vertex simply overwrite each other.
-template <int B, bool PRED, int PER, int K>
+template <int B, bool PRED, int PER, int KS>
 __device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSmem<B, PRED> &s, const uint32_t *mask,
                                                    const bool (&todo)[PER], const int (&r0)[PER],
                                                    const int (&r1)[PER], int (&parent)[PER])
@@ -513,7 +550,7 @@ __device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSme
     // bottom-up levels), not in registers
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
+        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > KS;
         const unsigned bal = __ballot_sync(0xffffffffu, more);
         if (bal == 0) continue;
         const int leader = __ffs(bal) - 1;
@@ -523,8 +560,8 @@ __device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSme
         if (more) {
             const int sl = base + __popc(bal & lanemask_lt());
             s.stage[t * B + tid] = sl;
-            s.colstart[sl] = r0[t] + K;
-            s.rel[sl] = r1[t] - r0[t] - K;
+            s.colstart[sl] = r0[t] + KS;
+            s.rel[sl] = r1[t] - r0[t] - KS;
             s.out[sl] = -1;
         }
     }
@@ -601,7 +638,7 @@ __device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSme
     }
 #pragma unroll
     for (int t = 0; t < PER; t++)
-        if (todo[t] && parent[t] < 0 && r1[t] - r0[t] > K) parent[t] = s.out[s.stage[t * B + tid]];
+        if (todo[t] && parent[t] < 0 && r1[t] - r0[t] > KS) parent[t] = s.out[s.stage[t * B + tid]];
     __syncthreads();  // the output phase reuses colstart / rel / out
 }
 
@@ -661,10 +698,17 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             }
         }
         // ---- continue the scan for candidates still without a parent ---------------
-        if (p.bu_scan == 2)
+        if (p.bu_scan == 2) {
             bottom_up_worklist<B, PRED, PER, K>(p, s, mask, todo, r0, r1, parent);
-        else
-            bottom_up_lanes<PER, K>(p, mask, todo, r0, r1, parent);
+        } else if (p.bu_scan == 3) {
+            // short scans per lane, then whatever is left edge-parallel: lists the
+            // lanes did not finish are mostly vertices with no parent this level,
+            // whose lists must be read whole anyway
+            bottom_up_lanes<PER, K, kBottomUpLaneSteps>(p, mask, todo, r0, r1, parent);
+            bottom_up_worklist<B, PRED, PER, K + 4 * kBottomUpLaneSteps>(p, s, mask, todo, r0, r1, parent);
+        } else {
+            bottom_up_lanes<PER, K, 0>(p, mask, todo, r0, r1, parent);
+        }
         // ---- label, mark and append the discoveries --------------------------------
 #pragma unroll
         for (int t = 0; t < PER; t++) {
@@ -1059,13 +1103,18 @@ __global__ void init_kernel(BfsParams p)
             p.vf[0].v[0] = src;
             p.vf[0].col[0] = r0;
             p.vf[0].P[0] = 0;
-            for (int c = 0; c * kChunkGrain < deg && c < p.cf_cap; c++) p.vf[0].cf[c] = 0;
         } else {
             // edge frontier: the source is the only item; its predecessor is -2
             st->qe[0] = pack(1u, 0u);
             p.ef[0].v[0] = src;
             if (PRED) p.ef[0].pred[0] = -2;
         }
+    }
+    if (VERTEX_FRONTIER) {
+        // the source owns every chunk of the level-0 frontier (a hub source has many)
+        const int deg = p.row_offsets[src + 1] - p.row_offsets[src];
+        const long long chunks = min((long long)(deg + kChunkGrain - 1) / kChunkGrain, (long long)p.cf_cap);
+        for (long long c = t0; c < chunks; c += stride) p.vf[0].cf[c] = 0;
     }
 }
 

@@ -10,6 +10,8 @@
 namespace b40c {
 namespace rt {
 
+constexpr int kBatchPullAlpha = 6;
+
 void free_batch(b40c_bfs_problem *p)
 {
     if (p->d_ms_visited) cudaFree(p->d_ms_visited);
@@ -128,6 +130,10 @@ int b40c_msbfs_enact(b40c_bfs_problem *p, const int32_t *sources, const int32_t 
     b40c_bfs_policy pol;
     int rc = resolve_policy(B40C_EXPAND_CONTRACT, policy, &pol);
     if (rc) return rc;
+    // batches pull once a level's frontier holds more than 1/6 of the edges
+    // (measured on B200: R-MAT 20 batches 4.46 ms at 1/14, 0.82 ms at 1/6;
+    // lattices and uniform graphs unchanged or slightly faster)
+    if (!policy || policy->bottom_up_alpha == 0) pol.bottom_up_alpha = kBatchPullAlpha;
     DeviceGuard guard(p->device);
     return enact_batch(p, sources, depth_limits, k, max_grid_size, pol);
 }

@@ -149,7 +149,7 @@ b40c_bfs_policy default_policy(int strategy)
     pol.bottom_up_alpha = 14;  // Beamer et al.'s defaults
     pol.bottom_up_beta = 24;
     pol.small_frontier_edges = 1024;
-    pol.bottom_up_scan = 2;
+    pol.bottom_up_scan = 1;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     (void)strategy;
     return pol;
@@ -187,8 +187,9 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     if (d.bottom_up_alpha < 1 || d.bottom_up_beta < 1)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_alpha and bottom_up_beta must be >= 1");
     if (d.saturation_quit < 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.saturation_quit must be >= 1");
-    if (d.bottom_up_scan != 1 && d.bottom_up_scan != 2)
-        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_scan must be 1 (per lane) or 2 (per CTA)");
+    if (d.bottom_up_scan < 1 || d.bottom_up_scan > 3)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE,
+                          "policy.bottom_up_scan must be 1 (per lane), 2 (per CTA) or 3 (lanes, then per CTA)");
     if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
     *out = d;
     return B40C_SUCCESS;

@@ -271,8 +271,10 @@ def batched_extra(steps, warmup):
     g, _ = build_graph("random21")
     deg = np.diff(g.row_offsets).astype(np.int64)
     srcs = sample_sources(g, 64, seed=0)
+    from back40computing_b200 import autotune
+    pol = autotune.policy_for(g, "batched")
     p = CsrProblem.from_graph(g)
-    p.msbfs(srcs)
+    p.msbfs(srcs, policy=pol)
     depths = p.msbfs_depths()
     ec, vc = [], []
     levels = np.zeros(g.nodes, np.uint64)
@@ -290,13 +292,13 @@ def batched_extra(steps, warmup):
     lv = np.bitwise_count(levels).astype(np.int64)
     balg = 4.0 * float((deg * lv).sum()) + 4.0 * float(sum(vc))
     for _ in range(warmup):
-        p.msbfs(srcs)
+        p.msbfs(srcs, policy=pol)
     for _ in range(steps):
-        p.msbfs(srcs)
+        p.msbfs(srcs, policy=pol)
     batch_ms = float(p.recent_search_ms(steps).mean())
     seq = {}
     for st in (4, 0):
-        e = ENACTORS[st]()
+        e = ENACTORS[st](policy=autotune.policy_for(g, STRATEGY_NAMES[st]))
         N.check(p.Reset(e.GetFrontierType(), 1.3))
         for s in srcs:
             N.check(e._enact(p, int(s), 0, 0))
@@ -363,7 +365,7 @@ def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=
     out = {"graphs": [n for n, _ in SERVED_SET], "budget_bytes": SERVED_BUDGET, "requests": n_requests}
     with BfsServer(memory_budget_bytes=SERVED_BUDGET) as srv:
         for g in graphs:
-            srv.add_graph(g)
+            srv.add_tuned_graph(g)
         out["widths"] = [srv.graph_info(i)[1] for i in range(len(graphs))]
         out["memory_used_bytes"] = srv.counters()["memory_used_bytes"]
         run(srv, 500, np.zeros(500, np.int64))  # warm-up
@@ -380,7 +382,7 @@ def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=
         out["latency_sweep"] = sweep
     with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_batch=1) as one:
         for g in graphs:
-            one.add_graph(g)
+            one.add_tuned_graph(g)
         run(one, 50, np.zeros(50, np.int64))
         base = latency_summary(run(one, baseline_requests, np.zeros(baseline_requests, np.int64)))
         base["sample"] = f"first {baseline_requests} requests of the stream"
@@ -439,7 +441,11 @@ def main():
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
     problem.set_stream(stream.cuda_stream)
-    enactor = ENACTORS[args.strategy]()
+    from back40computing_b200 import autotune
+    graph_class = autotune.classify(g)
+    kind = {0: "expand-contract", 4: "direction-optimizing"}.get(args.strategy)
+    policy = autotune.policy_for(graph_class, kind) if kind else None
+    enactor = ENACTORS[args.strategy](policy=policy)
     N.check(problem.Reset(enactor.GetFrontierType(), 1.3), "Reset")
 
     def enact(s):
@@ -535,6 +541,7 @@ def main():
             "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
                        "vertices": g.nodes, "edges": g.edges, "searches_per_step": len(srcs),
                        "strategy": STRATEGY_NAMES[args.strategy],
+                       "policy": f"autotuned for class {graph_class}" if policy is not None else "library defaults",
                        "topdown_expand_contract": topdown,
                        "mode": ["fused persistent", "per-level launches", "cuda graph"][args.mode],
                        "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6),

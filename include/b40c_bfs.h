@@ -95,8 +95,9 @@ typedef struct b40c_bfs_policy {
                                       -1 disables */
     int32_t bottom_up_scan;        /* bottom-up levels, vertices whose first neighbours are not yet
                                       visited: 1 = each lane scans its own list on (lists longer than 256
-                                      by the whole warp), 2 = the CTA scans all such lists together,
-                                      edge-parallel; 0 = default */
+                                      by the whole warp; default), 2 = the CTA scans all such lists
+                                      together, edge-parallel, 3 = lanes for 16 more neighbours, then
+                                      the CTA edge-parallel for what is left; 0 = default */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

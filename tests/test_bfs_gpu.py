@@ -356,7 +356,7 @@ def test_source_without_edges(strategy, mode):
         assert e.GetStatistics()[1] == depth
 
 
-@pytest.mark.parametrize("scan", [1, 2])
+@pytest.mark.parametrize("scan", [1, 2, 3])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 15, 12)), ("grid3d", (24,))])
 @pytest.mark.parametrize("preds", [False, True])
 def test_bottom_up_scan_variants(scan, kind, args, preds):
