@@ -54,10 +54,13 @@ def test_mixed_stream_matches_oracle(single_strategy):
         ids = [srv.add_graph(g) for g in gs]
         assert ids == list(range(len(gs)))
         outs, tickets = [], []
+        # one common arrival time a little ahead, so the queries meet in the
+        # queues and get batched whatever the submission pace
+        when = srv.now_ns() + 200_000_000
         for i in range(gid.size):
             out = np.empty(gs[gid[i]].nodes, np.int32)
             outs.append(out)
-            tickets.append(srv.submit(int(gid[i]), int(src[i]), int(lim[i]), labels=out))
+            tickets.append(srv.submit(int(gid[i]), int(src[i]), int(lim[i]), labels=out, arrival_ns=when))
         srv.drain()
         recs = srv.results(0, gid.size)
         assert (recs["status"] == 0).all()
