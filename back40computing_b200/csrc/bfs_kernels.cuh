@@ -780,11 +780,11 @@ struct DutyClock {
     {
         if (p.duty && threadIdx.x == 0) t0 = globaltimer_ns();
     }
-    __device__ bool barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word, int *s_flag)
+    __device__ bool barrier(SearchState *st, unsigned &generation, int *s_flag)
     {
         unsigned long long a = 0;
         if (p.duty && threadIdx.x == 0) a = globaltimer_ns();
-        const bool ok = grid_barrier(counter, generation, error_word, s_flag);
+        const bool ok = grid_barrier(&st->barrier, &st->release, generation, &st->error, s_flag);
         if (p.duty && threadIdx.x == 0) waited += globaltimer_ns() - a;
         return ok;
     }
@@ -932,7 +932,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                 if (tid == 0) p.st->solo_resume[solo_phase & 1] = level;
             }
             worked = true;
-            if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+            if (!duty.barrier(p.st, generation, &s_ok)) break;
             // not st->cur_level: CTA 0 may already have moved it on by the time a slow CTA reads
             level = ld_cg(&p.st->solo_resume[solo_phase & 1]) - 1;  // the loop increment brings it back
             solo_phase++;
@@ -956,7 +956,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             if (tid == 0) atomicOr(&p.st->error, kErrInjected);
             return;  // never arrives: the others' bounded waits must expire
         }
-        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+        if (!duty.barrier(p.st, generation, &s_ok)) break;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
     duty.finish();
@@ -1010,7 +1010,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
                     if (tid == 0) atomicOr(&p.st->error, kErrInjected);
                     return;
                 }
-                if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+                if (!duty.barrier(p.st, generation, &s_ok)) break;
             }
         }
         const int dl = p.st->depth_limit;
@@ -1034,7 +1034,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
             completed_level = true;
             if (p.persistent) {
                 if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
-                if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+                if (!duty.barrier(p.st, generation, &s_ok)) break;
             }
         }
         if (!p.persistent) break;
@@ -1087,6 +1087,7 @@ __global__ void init_kernel(BfsParams p)
         st->cur_level = 0;
         st->epoch += 1ull << 24;
         st->barrier = 0;
+        st->release = 0;
         st->error = 0;
         st->max_level = 0;
         st->done = 0;

@@ -32,21 +32,26 @@ struct EdgeFrontier {
 // Rotating/ping-pong counters written by the kernels (the role of the
 // reference's CtaWorkProgress, util/cta_work_progress.cuh:69-223).
 struct alignas(128) SearchState {
+    // ---- line 0: frontier counters, updated by every CTA (one atomic per tile)
     // Frontier sizes, rotating over passes (a pass is one level of
     // expand-contract, or one phase of a level of the edge strategies):
     // pass k reads qe[k % 3] and accumulates its output frontier into
     // qe[(k + 1) % 3]; each value packs (count << 32 | edge total).
     unsigned long long qe[3];
     uint32_t tile_ctr[3];      // look-back tile counters, by pass % 3
-    int32_t cur_level;         // next level to process
-    unsigned long long epoch;  // look-back epoch base for this search
-    unsigned long long barrier;  // grid-barrier arrivals of the current persistent launch
+    // ---- line 1: grid-barrier arrivals (atomics only, nobody polls this line)
+    alignas(128) unsigned long long barrier;  // arrivals of the current persistent launch
+    uint32_t finished;         // CTAs that finished the current non-persistent launch
+    // ---- line 2: what waiting CTAs poll (the barrier's release and the error word)
+    alignas(128) unsigned long long release;  // generation of the last completed grid barrier
     uint32_t error;            // dev::kErr* bits
+    // ---- line 3 on: per-search bookkeeping
+    alignas(128) int32_t cur_level;  // next level to process
+    unsigned long long epoch;  // look-back epoch base for this search
     int32_t max_level;         // deepest level at which a vertex was labelled
     int32_t done;              // 1 once the frontier emptied (or the depth limit was hit)
     int32_t saturated;         // 1 when a hybrid fused launch handed off
     unsigned long long total_queued;  // sum of processed frontier lengths
-    uint32_t finished;         // CTAs that finished the current non-persistent launch
     int32_t src;               // source vertex (read by the init kernel)
     int32_t depth_limit;       // < 0: unlimited
     // direction-optimizing bookkeeping, rotating like qe: pass k reads [k % 3]

@@ -363,14 +363,14 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
                 atomicMax(m.depth + src, level + 2);
             }
         }
-        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+        if (!duty.barrier(p.st, generation, &s_ok)) break;
         // clear this level's frontier masks (the queue lists every vertex with edges that has one)
         {
             const VertexFrontier in = p.vf[level & 1];
             unsigned long long *fcur = m.fmask[level & 1];
             for (int i = blockIdx.x * B + tid; i < s.q; i += gridDim.x * B) fcur[ld_cg(in.v + i)] = 0ull;
         }
-        if (!duty.barrier(&p.st->barrier, generation, &p.st->error, &s_ok)) break;
+        if (!duty.barrier(p.st, generation, &s_ok)) break;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
     duty.finish();
@@ -396,6 +396,7 @@ __global__ void msbfs_init_kernel(BfsParams p, MsParams m)
         st->epoch += 1ull << 24;
         st->cur_level = 0;
         st->barrier = 0;
+        st->release = 0;
         st->error = 0;
         st->max_level = 0;
         st->done = 0;
