@@ -1074,11 +1074,20 @@ __global__ void init_kernel(BfsParams p)
     if (FULL) {
         for (long long i = t0; i < p.nodes; i += stride) p.labels[i] = (VERTEX_FRONTIER && i == src) ? src_label : -1;
         for (long long w = t0; w < p.mask_words; w += stride) {
-            p.mask[w] = (VERTEX_FRONTIER && w == (src >> 5)) ? (1u << (src & 31)) : 0u;
+            // edgeless vertices start visited; the source's bit is set for a vertex
+            // frontier and clear for an edge frontier (whose contraction labels it)
+            uint32_t m = p.iso ? p.iso[w] : 0u;
+            if (w == (src >> 5)) m = VERTEX_FRONTIER ? (m | (1u << (src & 31))) : (m & ~(1u << (src & 31)));
+            p.mask[w] = m;
         }
-    } else if (VERTEX_FRONTIER && t0 == 0) {
-        p.labels[src] = src_label;
-        p.mask[src >> 5] = 1u << (src & 31);
+    } else if (t0 == 0) {
+        // after a reset (labels -1, mask = the edgeless bits)
+        if (VERTEX_FRONTIER) {
+            p.labels[src] = src_label;
+            p.mask[src >> 5] |= 1u << (src & 31);
+        } else {
+            p.mask[src >> 5] &= ~(1u << (src & 31));
+        }
     }
     if (t0 == 0) {
         SearchState *st = p.st;

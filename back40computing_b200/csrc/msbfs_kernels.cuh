@@ -386,7 +386,8 @@ __global__ void msbfs_init_kernel(BfsParams p, MsParams m)
     const long long total = (long long)m.k * p.nodes;
     for (long long i = t0; i < total; i += stride) m.labels[i] = -1;
     for (long long v = t0; v < p.nodes; v += stride) {
-        m.visited[v] = 0;
+        // vertices without edges count as visited by every source: pull levels skip them
+        m.visited[v] = (p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u)) ? ~0ull : 0ull;
         m.fmask[0][v] = 0;
         m.fmask[1][v] = 0;
     }

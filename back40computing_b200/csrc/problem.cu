@@ -99,6 +99,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.column_indices = p->d_ci;
     k.labels = p->d_labels;
     k.mask = p->d_mask;
+    k.iso = p->d_iso;
     k.nodes = (int32_t)p->nodes;
     k.edges = (int32_t)p->edges;
     k.mask_words = p->mask_words;
@@ -206,6 +207,7 @@ int64_t device_bytes(const b40c_bfs_problem *p)
     if (p->d_labels) t += a(4 * n);
     const int64_t mask = a(4 * ((int64_t)(p->mask_words + 63) / 64 * 64));
     if (p->d_mask) t += mask;
+    if (p->d_iso) t += mask;
     if (p->d_next) t += mask;
     if (p->st) t += a(sizeof(SearchState));
     if (p->slots) t += a((int64_t)sizeof(dev::LookbackSlot) * p->max_slots);
@@ -234,7 +236,7 @@ int64_t planned_bytes(int64_t n, int64_t m, int k, double qs)
     const int64_t cap = std::max<int64_t>(cap_of(qs, n), 1);
     const int64_t cf_len = (std::max<int64_t>(m, 1) + dev::kChunkGrain - 1) / dev::kChunkGrain + 2;
     int64_t t = a(4 * (n + 1)) + a(4 * std::max<int64_t>(m, 1));
-    t += a(4 * n) + 2 * mask + a(sizeof(SearchState)) + a((int64_t)sizeof(dev::LookbackSlot) * slots);
+    t += a(4 * n) + 3 * mask + a(sizeof(SearchState)) + a((int64_t)sizeof(dev::LookbackSlot) * slots);
     t += 2 * (2 * a(4 * cap) + a(4 * (cap + 1)) + a(4 * cf_len));
     if (k > 0) t += 3 * a(8 * n) + 2 * a(4 * 64) + a(4 * n * (int64_t)k);
     return t;
@@ -287,6 +289,19 @@ int finish_timing(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
+
+// Bit v of word v >> 5: vertex v has no edges.
+__global__ void edgeless_mask_kernel(const int32_t *ro, int32_t nodes, uint32_t *iso, int32_t words)
+{
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        uint32_t bits = 0;
+        for (int b = 0; b < 32; b++) {
+            const int v = w * 32 + b;
+            if (v < nodes && ro[v + 1] == ro[v]) bits |= 1u << b;
+        }
+        iso[w] = bits;
+    }
+}
 
 // Order-independent fingerprints of the edge multiset and of its reversal:
 // sums of a 64-bit mix (splitmix64's finaliser) of (u << 32 | v) and of
@@ -486,6 +501,13 @@ int create_problem(int64_t nodes, int64_t edges, int mark_pred, int stream_from_
     // second mask buffer: written whole by a bottom-up level before anything reads it
     if ((rc = alloc_dev((void **)&p->d_next, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "second mask")))
         return bail(rc);
+    // vertices without edges: never reached, never anyone's neighbour; marking
+    // them visited up front lets bottom-up levels skip them by the word test
+    if ((rc = alloc_dev((void **)&p->d_iso, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "edgeless mask")))
+        return bail(rc);
+    edgeless_mask_kernel<<<std::max(1, std::min<int>(p->sms * 8, (p->mask_words + 255) / 256)), 256, 0, p->stream>>>(
+        p->d_ro, (int32_t)nodes, p->d_iso, p->mask_words);
+    if (cudaGetLastError() != cudaSuccess) return bail(b40c::fail(B40C_ERROR_INVALID_CONFIGURATION, "edgeless mask launch"));
     if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
     if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
         cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {
@@ -625,6 +647,7 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->reg_ci) cudaHostUnregister((void *)p->reg_ci);
     if (p->d_labels) cudaFree(p->d_labels);
     if (p->d_mask) cudaFree(p->d_mask);
+    if (p->d_iso) cudaFree(p->d_iso);
     if (p->d_next) cudaFree(p->d_next);
     free_batch(p);
     if (p->d_levels) cudaFree(p->d_levels);
@@ -690,7 +713,9 @@ int b40c_bfs_problem_reset(b40c_bfs_problem *p, int frontier_type, double queue_
     }
     // labels <- -1, visited mask <- 0 (csr_problem.cuh:723-745)
     CUDA_TRY(cudaMemsetAsync(p->d_labels, 0xff, sizeof(int32_t) * p->nodes, p->stream), "label reset");
-    CUDA_TRY(cudaMemsetAsync(p->d_mask, 0, sizeof(uint32_t) * p->mask_words, p->stream), "mask reset");
+    CUDA_TRY(cudaMemcpyAsync(p->d_mask, p->d_iso, sizeof(uint32_t) * p->mask_words, cudaMemcpyDeviceToDevice,
+                             p->stream),
+             "mask reset");
     CUDA_TRY(cudaStreamSynchronize(p->stream), "reset synchronize");
     p->needs_init = false;
     return B40C_SUCCESS;

@@ -42,6 +42,7 @@ struct b40c_bfs_problem {
     int32_t *d_labels = nullptr;
     uint32_t *d_mask = nullptr;
     uint32_t *d_next = nullptr;  // second visited-mask buffer (bottom-up levels write it whole)
+    uint32_t *d_iso = nullptr;   // bit v: vertex v has no edges (pre-set in the visited mask of every search)
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
     // batched multi-source searches (allocated on first use)

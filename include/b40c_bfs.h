@@ -107,7 +107,8 @@ typedef struct b40c_bfs_device_view {
     void *d_row_offsets;    /* int32[nodes + 1] */
     void *d_column_indices; /* int32[edges] */
     void *d_labels;         /* int32[nodes] */
-    void *d_visited_mask;   /* bit v&7 of byte v>>3 (same layout as the reference's uchar mask) */
+    void *d_visited_mask;   /* bit v&7 of byte v>>3 (same layout as the reference's uchar mask);
+                               vertices without edges also have their bit set */
     int64_t visited_mask_bytes;
     int64_t nodes;
     int64_t edges;
