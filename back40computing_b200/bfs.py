@@ -141,14 +141,16 @@ class CsrProblem:
             a["ns"] = b["t_ns"] - a["t_ns"]
         return [r for r in recs if r["pass_"] >= 0]
 
-    def cta_arrivals(self, max_passes: int = 64) -> np.ndarray:
+    def cta_arrivals(self, max_passes: int = 64, phases: bool = False) -> np.ndarray:
         """[pass, cta] end-of-level barrier arrival times (ns) of the last
-        instrumented persistent search; 0 where a CTA did not arrive."""
-        buf = np.zeros(max_passes * 2048, dtype=np.uint64)
+        instrumented persistent search (0 where a CTA did not arrive); with
+        phases=True [pass, cta, 8] including the in-level phase stamps."""
+        buf = np.zeros(max_passes * 2048 * 8, dtype=np.uint64)
         g = C.c_int32(0)
         N.check(N.lib().b40c_bfs_cta_arrivals(self.handle, buf.ctypes.data_as(C.POINTER(C.c_uint64)),
                                               int(max_passes), C.byref(g)), "cta_arrivals")
-        return buf[:max_passes * g.value].reshape(max_passes, g.value)
+        a = buf[:max_passes * g.value * 8].reshape(max_passes, g.value, 8)
+        return a if phases else a[:, :, 7]
 
     # ---- batched multi-source searches ------------------------------------------------
     def msbfs(self, sources, depth_limits=None, policy: N.Policy | None = None, max_grid_size: int = 0) -> None:

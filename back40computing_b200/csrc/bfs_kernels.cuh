@@ -72,6 +72,21 @@ struct ExpandSmem {
     unsigned long long prefix;
 };
 
+__device__ __forceinline__ unsigned long long globaltimer_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Instrumented searches: thread 0 records when its CTA reached `phase` of pass
+// `pass` (first work chunk of the level only for phases < kPhaseArrive).
+__device__ __forceinline__ void stamp(const BfsParams &p, int pass, int phase)
+{
+    if (p.arrive && threadIdx.x == 0 && pass < kMaxArrivePasses && blockIdx.x < kMaxArriveCtas)
+        p.arrive[((size_t)pass * kMaxArriveCtas + blockIdx.x) * kPhaseStamps + phase] = globaltimer_ns();
+}
+
 // Packed (count, degree) pair: count in the high 32 bits.
 __device__ __forceinline__ unsigned long long pack(unsigned cnt, unsigned deg)
 {
@@ -299,9 +314,11 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
     cta_range(E, part, parts, rs, re);
     if (rs >= re) return;
     int i_cur = ld_cg(in.cf + rs / kChunkGrain);  // entry owning position rs
+    if (FUSED_CULL) stamp(p, pass, 0);
     for (int cs = rs; cs < re; cs += kChunkMax) {
         const int ce = min(cs + kChunkMax, re);
         const int len = ce - cs;
+        const bool first = FUSED_CULL && cs == rs;
         // ---- load the runs of entries i_cur.. that start before ce ----------------
         if (tid == 0) s.out_count = 0;
         int k = 0;
@@ -324,6 +341,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
             if (c < B) break;
         }
         if (tid == 0) s.rel[k] = len;
+        if (first) stamp(p, pass, 1);
         const int j_last = k - 1;  // its run may continue into the next sub-round
 
         // ---- CTA-cooperative gather: a sub-round inside one adjacency list is
@@ -380,6 +398,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         }
         __syncthreads();
 
+        if (first) stamp(p, pass, 2);
         // ---- gather: thread t takes positions t, t + B, ...: a warp reads 32
         // consecutive positions (one coalesced segment of any run >= 32 long) ------
         int v[PER], u[PER];
@@ -411,10 +430,13 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
             continue;
         }
         __syncthreads();  // run tables consumed: they now collect the sub-round's output
+        if (first) stamp(p, pass, 3);
         discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level + 1);
         __syncthreads();
+        if (first) stamp(p, pass, 4);
         emit_frontier<B>(p, s, pass, vout, qe_out);
         __syncthreads();
+        if (first) stamp(p, pass, 5);
     }
 }
 
@@ -757,12 +779,6 @@ __device__ __forceinline__ bool choose_bottom_up(const BfsParams &p, bool was_bo
 // Level drivers
 // ------------------------------------------------------------------------------------
 
-__device__ __forceinline__ unsigned long long globaltimer_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
 
 __device__ __forceinline__ unsigned long long ld_cg64(const unsigned long long *p)
 {
@@ -949,8 +965,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         worked = true;
         if (s.flag) max_level_seen = level + 1;
         if (!p.persistent) break;
-        if (p.arrive && tid == 0 && pass < kMaxArrivePasses && blockIdx.x < kMaxArriveCtas)
-            p.arrive[pass * kMaxArriveCtas + blockIdx.x] = globaltimer_ns();
+        stamp(p, pass, kPhaseArrive);
         if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
         if ((int)blockIdx.x == p.skip_arrival_cta) {
             if (tid == 0) atomicOr(&p.st->error, kErrInjected);

@@ -83,10 +83,14 @@ struct LevelRecord {
     unsigned long long t_ns;   // %globaltimer when block 0 started the pass
 };
 constexpr int kMaxLevelRecords = 1 << 16;
-// Per-CTA arrival times at the end-of-level grid barrier, for the first
-// kMaxArrivePasses passes of an instrumented persistent search.
+// Per-CTA times (%globaltimer ns) for the first kMaxArrivePasses passes of an
+// instrumented persistent search: [pass][cta][kPhaseStamps], phases 0..5
+// mark steps of the CTA's first work chunk of the level (see stamp sites),
+// phase kPhaseArrive its arrival at the end-of-level grid barrier.
 constexpr int kMaxArrivePasses = 64;
 constexpr int kMaxArriveCtas = 2048;
+constexpr int kPhaseStamps = 8;
+constexpr int kPhaseArrive = 7;
 
 // Kernel parameter block.
 struct BfsParams {

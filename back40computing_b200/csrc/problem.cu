@@ -220,7 +220,7 @@ int64_t device_bytes(const b40c_bfs_problem *p)
     if (p->d_ms_labels) t += a(4 * n * (int64_t)p->ms_labels_k);
     if (p->d_levels) t += a((int64_t)sizeof(LevelRecord) * kMaxLevelRecords);
     if (p->d_duty) t += a(4 * sizeof(unsigned long long));
-    if (p->d_arrive) t += a((int64_t)sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas);
+    if (p->d_arrive) t += a((int64_t)sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas * kPhaseStamps);
     return t;
 }
 
@@ -363,7 +363,8 @@ int begin_instrumented(b40c_bfs_problem *p)
     if (!p->instrument) return B40C_SUCCESS;
     CUDA_TRY(cudaMemsetAsync(p->d_levels, 0, sizeof(LevelRecord) * kMaxLevelRecords, p->stream), "level records reset");
     CUDA_TRY(cudaMemsetAsync(p->d_duty, 0, 4 * sizeof(unsigned long long), p->stream), "duty reset");
-    CUDA_TRY(cudaMemsetAsync(p->d_arrive, 0, sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas, p->stream),
+    CUDA_TRY(cudaMemsetAsync(p->d_arrive, 0, sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas * kPhaseStamps,
+                             p->stream),
              "arrival reset");
     return B40C_SUCCESS;
 }
@@ -800,7 +801,8 @@ int b40c_bfs_set_instrument(b40c_bfs_problem *p, int on)
         int rc;
         if ((rc = alloc_dev((void **)&p->d_levels, sizeof(LevelRecord) * kMaxLevelRecords, "level records"))) return rc;
         if ((rc = alloc_dev((void **)&p->d_duty, 4 * sizeof(unsigned long long), "duty counters"))) return rc;
-        if ((rc = alloc_dev((void **)&p->d_arrive, sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas,
+        if ((rc = alloc_dev((void **)&p->d_arrive,
+                            sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas * kPhaseStamps,
                             "arrival times")))
             return rc;
     }
@@ -817,12 +819,14 @@ int b40c_bfs_cta_arrivals(b40c_bfs_problem *p, uint64_t *out, int max_passes, in
     DeviceGuard guard(p->device);
     const int passes = std::min(max_passes, kMaxArrivePasses);
     const int g = std::min(p->last_grid, kMaxArriveCtas);
-    std::vector<unsigned long long> h((size_t)kMaxArrivePasses * kMaxArriveCtas);
+    std::vector<unsigned long long> h((size_t)kMaxArrivePasses * kMaxArriveCtas * kPhaseStamps);
     CUDA_TRY(cudaStreamSynchronize(p->stream), "stream synchronize");
     CUDA_TRY(cudaMemcpy(h.data(), p->d_arrive, sizeof(unsigned long long) * h.size(), cudaMemcpyDeviceToHost),
              "arrival read");
     for (int k = 0; k < passes; k++)
-        for (int c = 0; c < g; c++) out[(size_t)k * g + c] = h[(size_t)k * kMaxArriveCtas + c];
+        for (int c = 0; c < g; c++)
+            for (int f = 0; f < kPhaseStamps; f++)
+                out[((size_t)k * g + c) * kPhaseStamps + f] = h[((size_t)k * kMaxArriveCtas + c) * kPhaseStamps + f];
     *ctas = g;
     return B40C_SUCCESS;
 }

@@ -205,12 +205,14 @@ typedef struct b40c_level_record {
 
 int b40c_bfs_set_instrument(b40c_bfs_problem *problem, int on);
 
-/* Per-CTA end-of-level arrival times (%globaltimer ns) of the last
- * instrumented persistent search: out[pass * ctas + cta] for the first
- * max_passes (<= 64) passes; 0 where a CTA did not arrive (solo phases).
- * The spread between a pass's first and last arrival is its load imbalance
- * (the per-CTA clocks of the reference's KernelRuntimeStats,
- * util/kernel_runtime_stats.cuh:45-126).  out needs max_passes x 2048 entries. */
+/* Per-CTA times (%globaltimer ns) of the last instrumented persistent search,
+ * out[(pass * ctas + cta) * 8 + phase] for the first max_passes (<= 64)
+ * passes; phase 7 is the CTA's arrival at the end-of-level grid barrier,
+ * phases 0-5 steps of its first work chunk of a top-down level (start,
+ * frontier entries loaded, gather set up, gathered, discovered, emitted); 0
+ * where a CTA did not get there.  The spread of a pass's arrivals is its load
+ * imbalance (the per-CTA clocks of the reference's KernelRuntimeStats,
+ * util/kernel_runtime_stats.cuh:45-126).  out needs max_passes x 2048 x 8 entries. */
 int b40c_bfs_cta_arrivals(b40c_bfs_problem *problem, uint64_t *out, int max_passes, int *ctas);
 
 /* Copies the last instrumented search's records (at most max_records) plus a
