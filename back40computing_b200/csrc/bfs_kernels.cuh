@@ -39,16 +39,6 @@ namespace dev {
 constexpr int kChunkMax = 2048;   // edges (or edge-frontier items) per sub-round
 constexpr int kChunkGrain = 256;  // CTA ranges start at multiples of this; granularity of the cf index
 
-// Output entries of one emit whose degree spans many kChunkGrain chunks: their
-// cf entries are written by the whole CTA instead of one thread.
-constexpr int kCfBigEntries = 32;
-constexpr unsigned kCfSerialChunks = 8;  // entries spanning more chunks than this go to CfBig
-struct CfBig {
-    int32_t count;
-    int32_t g[kCfBigEntries];
-    uint32_t c0[kCfBigEntries], c1[kCfBigEntries];
-};
-
 template <int B, bool PRED>
 struct ExpandSmem {
     // per-sub-round run tables; after the gather they hold the sub-round's
@@ -67,7 +57,6 @@ struct ExpandSmem {
     int32_t prev_bu;                   // the previous level ran bottom-up
     uint32_t *mask;                    // the visited-mask buffer of this pass (mask or mask_alt)
     int32_t wl_count;                  // bottom-up worklist entries of the current chunk
-    CfBig big;                         // emit_frontier: entries whose cf runs the CTA writes together
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -202,7 +191,6 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cnt = s.out_count;
-    if (tid == 0) s.big.count = 0;  // read after the scan's barriers
     constexpr int PER = kChunkMax / B;
     const int per = (cnt + B - 1) / B;
     const int jb = min(tid * per, cnt), je = min(jb + per, cnt);
@@ -239,47 +227,38 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
     __syncthreads();
     const unsigned long long prefix = s.prefix;
     if (prefix == ~0ull) return;
-    unsigned g = (unsigned)(prefix >> 32) + (unsigned)(excl >> 32);
-    unsigned d = (unsigned)(prefix & 0xffffffffu) + (unsigned)(excl & 0xffffffffu);
+    const unsigned g0 = (unsigned)(prefix >> 32), d0 = (unsigned)(prefix & 0xffffffffu);
+    unsigned g = g0 + (unsigned)(excl >> 32);
+    unsigned d = d0 + (unsigned)(excl & 0xffffffffu);
     for (int j = jb; j < je; j++) {
         const unsigned deg = (unsigned)s.rel[j];
         if ((int)g < p.vcap) {
             vout.v[g] = s.out[j];
             vout.col[g] = s.colstart[j];
             vout.P[g] = (int)d;
-            // cf[c] = g for the chunks c starting inside [d, d + deg)
-            const unsigned c0 = (d + kChunkGrain - 1) / kChunkGrain, c1 = (d + deg + kChunkGrain - 1) / kChunkGrain;
-            int big = -1;
-            if (c1 - c0 > kCfSerialChunks) {
-                big = atomicAdd(&s.big.count, 1);
-                if (big < kCfBigEntries) {
-                    s.big.g[big] = (int)g;
-                    s.big.c0[big] = c0;
-                    s.big.c1[big] = c1;
-                }
-            }
-            if (big < 0 || big >= kCfBigEntries) {
-                for (unsigned c = c0; c < c1; c++) {
-                    if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never past the end
-                        atomicOr(&p.st->error, kErrOverflow);
-                        break;
-                    }
-                    vout.cf[c] = (int)g;
-                }
-            }
         } else {
             atomicOr(&p.st->error, kErrOverflow);
         }
+        s.colstart[j] = (int)(d - d0);  // tile-relative degree prefix, for the cf pass below
         g++;
         d += deg;
     }
     __syncthreads();
-    // hub entries: their chunk runs are written by the whole CTA
-    const int nbig = min(s.big.count, kCfBigEntries);
-    for (int b = 0; b < nbig; b++) {
-        const unsigned c1 = min(s.big.c1[b], (unsigned)p.cf_cap);
-        if (tid == 0 && s.big.c1[b] > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);
-        for (unsigned c = s.big.c0[b] + tid; c < c1; c += B) vout.cf[c] = s.big.g[b];
+    // cf[c] = the entry owning flattened position c * kChunkGrain, for every
+    // chunk starting inside this tile, written by the whole CTA (a tile's
+    // entries can span thousands of chunks when it holds high-degree vertices)
+    const unsigned tdeg = (unsigned)(tot & 0xffffffffu);
+    const unsigned c0 = (d0 + kChunkGrain - 1) / kChunkGrain, c1 = (d0 + tdeg + kChunkGrain - 1) / kChunkGrain;
+    if (tid == 0 && c1 > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);  // never past the end
+    const unsigned c_end = min(c1, (unsigned)p.cf_cap);
+    for (unsigned c = c0 + tid; c < c_end; c += B) {
+        const int x = (int)(c * kChunkGrain - d0);  // in [0, tdeg)
+        int lo = 0, hi = cnt - 1;                   // last entry whose prefix is <= x
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (s.colstart[mid] <= x) lo = mid; else hi = mid - 1;
+        }
+        if ((int)(g0 + lo) < p.vcap) vout.cf[c] = (int)(g0 + lo);
     }
 }
 

@@ -49,7 +49,6 @@ struct MsSmem {
     int32_t q, E;
     unsigned long long active;
     unsigned long long found;        // sources that reached a vertex this level
-    CfBig big;                       // emit_frontier: hub entries' cf runs
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
