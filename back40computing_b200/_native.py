@@ -44,6 +44,7 @@ class Policy(C.Structure):
         ("bottom_up_beta", C.c_int32),
         ("small_frontier_edges", C.c_int32),
         ("bottom_up_scan", C.c_int32),
+        ("bottom_up_hub_probes", C.c_int32),
     ]
 
 

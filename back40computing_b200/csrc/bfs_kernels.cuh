@@ -479,14 +479,16 @@ constexpr int kBottomUpLaneSteps = 4;  // bottom_up_scan 3: lane steps (4 neighb
 // Bottom-up continuation, one lane per vertex: each lane scans its own list
 // on, four neighbours at a time; lists longer than kBottomUpLongList are
 // searched by the whole warp, 32 neighbours at a time.
-template <int PER, int K, int MAX_ITER>
+template <int PER, int K, int MAX_ITER, int MIN_LEN = K>
 __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, const bool (&todo)[PER],
                                                 const int (&r0)[PER], const int (&r1)[PER], int (&parent)[PER])
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > K;
+        // K neighbours already probed at the list's start; lists of at most
+        // MIN_LEN are finished
+        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > MIN_LEN;
         if (!__any_sync(0xffffffffu, more)) continue;
         // capped: no warp-cooperative lists, at most MAX_ITER steps per lane
         const bool longlist = MAX_ITER == 0 && more && (r1[t] - r0[t]) > kBottomUpLongList;
@@ -679,11 +681,21 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         int parent[PER];
         {
             int nb[PER][K];
+            static_assert(K == 2, "the hub pair supplies two probes");
 #pragma unroll
             for (int t = 0; t < PER; t++) {
                 todo[t] = todo[t] && r1[t] > r0[t];
+                if (p.hub2) {
+                    // the vertex's two highest-degree neighbours (one coalesced 8-byte load)
+                    int2 h = make_int2(-1, -1);
+                    if (todo[t]) h = p.hub2[cs + t * B + tid];
+                    nb[t][0] = h.x;
+                    nb[t][1] = h.y;
+                } else {
 #pragma unroll
-                for (int k = 0; k < K; k++) nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+                    for (int k = 0; k < K; k++)
+                        nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+                }
             }
             unsigned w[PER][K];
 #pragma unroll
@@ -707,6 +719,9 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             // whose lists must be read whole anyway
             bottom_up_lanes<PER, K, kBottomUpLaneSteps>(p, mask, todo, r0, r1, parent);
             bottom_up_worklist<B, PRED, PER, K + 4 * kBottomUpLaneSteps>(p, s, mask, todo, r0, r1, parent);
+        } else if (p.hub2) {
+            // the pair came from anywhere in the list: lists longer than two are scanned from the start
+            bottom_up_lanes<PER, 0, 0, K>(p, mask, todo, r0, r1, parent);
         } else {
             bottom_up_lanes<PER, K, 0>(p, mask, todo, r0, r1, parent);
         }

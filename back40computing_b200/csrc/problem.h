@@ -43,6 +43,7 @@ struct b40c_bfs_problem {
     uint32_t *d_mask = nullptr;
     uint32_t *d_next = nullptr;  // second visited-mask buffer (bottom-up levels write it whole)
     uint32_t *d_iso = nullptr;   // bit v: vertex v has no edges (pre-set in the visited mask of every search)
+    int32_t *d_hub2 = nullptr;   // [2n] per vertex its two highest-degree neighbours (symmetric graphs, lazily)
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
     // batched multi-source searches (allocated on first use)
@@ -154,6 +155,7 @@ int run_graph(b40c_bfs_problem *p, int slot, const KernelNode &init, KernelNode 
 int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                  int32_t depth_limit, bool direction_optimizing);
 int check_symmetric(b40c_bfs_problem *p);
+int ensure_hubs(b40c_bfs_problem *p);
 void free_batch(b40c_bfs_problem *p);
 int ensure_batch(b40c_bfs_problem *p, int k);
 // Queues a batched search of k <= 64 sources on p->stream (asynchronous).

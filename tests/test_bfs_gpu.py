@@ -356,16 +356,18 @@ def test_source_without_edges(strategy, mode):
         assert e.GetStatistics()[1] == depth
 
 
-@pytest.mark.parametrize("scan", [1, 2, 3])
+@pytest.mark.parametrize("scan,hub", [(1, 1), (1, -1), (2, 0), (3, 0)])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 15, 12)), ("grid3d", (24,))])
 @pytest.mark.parametrize("preds", [False, True])
-def test_bottom_up_scan_variants(scan, kind, args, preds):
-    """Both bottom-up continuations (per lane, CTA worklist) give the oracle's
-    distances and valid predecessors; alpha 2 forces many bottom-up levels."""
+def test_bottom_up_scan_variants(scan, hub, kind, args, preds):
+    """Every bottom-up continuation (per lane with or without the hub-pair
+    probes, CTA worklist, hybrid) gives the oracle's distances and valid
+    predecessors; alpha 2 forces many bottom-up levels."""
     g = _graph(kind, *args)
     p = CsrProblem.from_graph(g, mark_predecessors=preds)
     pol = N.Policy()
     pol.bottom_up_scan = scan
+    pol.bottom_up_hub_probes = hub
     pol.bottom_up_alpha = 2
     for s in sample_sources(g, 3, seed=9):
         got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, policy=pol)
