@@ -127,7 +127,7 @@ struct BfsParams {
     int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
     int32_t small_edges;      // persistent launches: frontiers with at most this many edges run on CTA 0 alone
     int32_t bu_scan;          // bottom-up continuation: 1 per lane, 2 per CTA (edge-parallel worklist)
-    const uint32_t *iso;      // bit v: v has no edges; a search starts with these bits visited (null: none)
+    const uint32_t *iso;      // bit v: v has no edges in or out; a search starts with these bits visited (null: none)
     const int2 *hub2;         // per vertex its two highest-degree neighbours, probed first bottom-up (null: off)
     uint32_t *mask_alt;       // second visited-mask buffer: a bottom-up level reads one buffer and writes
                               // every word of the other (old bits | its discoveries), then they swap

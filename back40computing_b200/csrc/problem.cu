@@ -295,16 +295,37 @@ int finish_timing(b40c_bfs_problem *p)
 }
 
 
-// Bit v of word v >> 5: vertex v has no edges.
-__global__ void edgeless_mask_kernel(const int32_t *ro, int32_t nodes, uint32_t *iso, int32_t words)
+// Edgeless vertices (no out-edges and no in-edges, so on a directed graph too
+// nothing can reach them): first each word gets the bits of vertices with
+// out-edges, then every edge sets its head's bit, then the words are inverted.
+__global__ void out_edge_mask_kernel(const int32_t *ro, int32_t nodes, uint32_t *bits, int32_t words)
 {
     for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
-        uint32_t bits = 0;
-        for (int b = 0; b < 32; b++) {
-            const int v = w * 32 + b;
-            if (v < nodes && ro[v + 1] == ro[v]) bits |= 1u << b;
+        uint32_t b = 0;
+        for (int k = 0; k < 32; k++) {
+            const int v = w * 32 + k;
+            if (v < nodes && ro[v + 1] > ro[v]) b |= 1u << k;
         }
-        iso[w] = bits;
+        bits[w] = b;
+    }
+}
+
+__global__ void in_edge_mask_kernel(const int32_t *ci, int64_t edges, uint32_t *bits)
+{
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < edges; e += stride) {
+        const int u = ci[e];
+        const uint32_t bit = 1u << (u & 31);
+        if (!(bits[u >> 5] & bit)) atomicOr(bits + (u >> 5), bit);
+    }
+}
+
+__global__ void invert_mask_kernel(uint32_t *bits, int32_t nodes, int32_t words)
+{
+    for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < words; w += gridDim.x * blockDim.x) {
+        const int left = nodes - w * 32;
+        const uint32_t valid = left >= 32 ? 0xffffffffu : ((1u << left) - 1u);
+        bits[w] = ~bits[w] & valid;
     }
 }
 
@@ -572,9 +593,15 @@ int create_problem(int64_t nodes, int64_t edges, int mark_pred, int stream_from_
     // them visited up front lets bottom-up levels skip them by the word test
     if ((rc = alloc_dev((void **)&p->d_iso, sizeof(uint32_t) * ((p->mask_words + 63) / 64 * 64), "edgeless mask")))
         return bail(rc);
-    edgeless_mask_kernel<<<std::max(1, std::min<int>(p->sms * 8, (p->mask_words + 255) / 256)), 256, 0, p->stream>>>(
-        p->d_ro, (int32_t)nodes, p->d_iso, p->mask_words);
-    if (cudaGetLastError() != cudaSuccess) return bail(b40c::fail(B40C_ERROR_INVALID_CONFIGURATION, "edgeless mask launch"));
+    {
+        const int wb = std::max(1, std::min<int>(p->sms * 8, (p->mask_words + 255) / 256));
+        out_edge_mask_kernel<<<wb, 256, 0, p->stream>>>(p->d_ro, (int32_t)nodes, p->d_iso, p->mask_words);
+        if (edges > 0)
+            in_edge_mask_kernel<<<p->sms * 8, 256, 0, p->stream>>>(p->d_ci, edges, p->d_iso);
+        invert_mask_kernel<<<wb, 256, 0, p->stream>>>(p->d_iso, (int32_t)nodes, p->mask_words);
+        if (cudaGetLastError() != cudaSuccess)
+            return bail(b40c::fail(B40C_ERROR_INVALID_CONFIGURATION, "edgeless mask launch"));
+    }
     if ((rc = alloc_dev((void **)&p->st, sizeof(SearchState), "search state"))) return bail(rc);
     if (cudaMemsetAsync(p->st, 0, sizeof(SearchState), p->stream) != cudaSuccess ||
         cudaMallocHost((void **)&p->h_st, sizeof(SearchState)) != cudaSuccess) {

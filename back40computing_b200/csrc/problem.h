@@ -42,7 +42,7 @@ struct b40c_bfs_problem {
     int32_t *d_labels = nullptr;
     uint32_t *d_mask = nullptr;
     uint32_t *d_next = nullptr;  // second visited-mask buffer (bottom-up levels write it whole)
-    uint32_t *d_iso = nullptr;   // bit v: vertex v has no edges (pre-set in the visited mask of every search)
+    uint32_t *d_iso = nullptr;   // bit v: vertex v has no edges in or out (pre-set in every search's visited mask)
     int32_t *d_hub2 = nullptr;   // [2n] per vertex its two highest-degree neighbours (symmetric graphs, lazily)
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
