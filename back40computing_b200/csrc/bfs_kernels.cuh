@@ -39,6 +39,10 @@ namespace dev {
 constexpr int kChunkMax = 2048;   // edges (or edge-frontier items) per sub-round
 constexpr int kChunkGrain = 256;  // CTA ranges start at multiples of this; granularity of the cf index
 
+// emit_frontier: output entries whose degree spans more chunks than this have
+// their cf runs written by the whole CTA.
+constexpr unsigned kCfSerialChunks = 8;
+
 template <int B, bool PRED>
 struct ExpandSmem {
     // per-sub-round run tables; after the gather they hold the sub-round's
@@ -230,26 +234,40 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
     const unsigned g0 = (unsigned)(prefix >> 32), d0 = (unsigned)(prefix & 0xffffffffu);
     unsigned g = g0 + (unsigned)(excl >> 32);
     unsigned d = d0 + (unsigned)(excl & 0xffffffffu);
+    bool long_run = false;
     for (int j = jb; j < je; j++) {
         const unsigned deg = (unsigned)s.rel[j];
         if ((int)g < p.vcap) {
             vout.v[g] = s.out[j];
             vout.col[g] = s.colstart[j];
             vout.P[g] = (int)d;
+            // cf[c] = g for the chunks c starting inside [d, d + deg); long runs
+            // (high-degree vertices) are left to the whole CTA below
+            const unsigned c0 = (d + kChunkGrain - 1) / kChunkGrain, c1 = (d + deg + kChunkGrain - 1) / kChunkGrain;
+            if (c1 - c0 > kCfSerialChunks) {
+                long_run = true;
+            } else {
+                for (unsigned c = c0; c < c1; c++) {
+                    if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never past the end
+                        atomicOr(&p.st->error, kErrOverflow);
+                        break;
+                    }
+                    vout.cf[c] = (int)g;
+                }
+            }
         } else {
             atomicOr(&p.st->error, kErrOverflow);
         }
-        s.colstart[j] = (int)(d - d0);  // tile-relative degree prefix, for the cf pass below
+        s.colstart[j] = (int)(d - d0);  // tile-relative degree prefix, for the pass below
         g++;
         d += deg;
     }
-    __syncthreads();
-    // cf[c] = the entry owning flattened position c * kChunkGrain, for every
-    // chunk starting inside this tile, written by the whole CTA (a tile's
-    // entries can span thousands of chunks when it holds high-degree vertices)
+    if (!__syncthreads_or(long_run)) return;  // CTA-uniform
+    // the long runs: every chunk of the tile finds its owner entry by binary
+    // search, and the owners spanning more than kCfSerialChunks chunks write
     const unsigned tdeg = (unsigned)(tot & 0xffffffffu);
     const unsigned c0 = (d0 + kChunkGrain - 1) / kChunkGrain, c1 = (d0 + tdeg + kChunkGrain - 1) / kChunkGrain;
-    if (tid == 0 && c1 > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);  // never past the end
+    if (tid == 0 && c1 > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);
     const unsigned c_end = min(c1, (unsigned)p.cf_cap);
     for (unsigned c = c0 + tid; c < c_end; c += B) {
         const int x = (int)(c * kChunkGrain - d0);  // in [0, tdeg)
@@ -258,7 +276,9 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
             const int mid = (lo + hi + 1) >> 1;
             if (s.colstart[mid] <= x) lo = mid; else hi = mid - 1;
         }
-        if ((int)(g0 + lo) < p.vcap) vout.cf[c] = (int)(g0 + lo);
+        const unsigned ed = d0 + (unsigned)s.colstart[lo], edeg = (unsigned)s.rel[lo];
+        const unsigned span = (ed + edeg + kChunkGrain - 1) / kChunkGrain - (ed + kChunkGrain - 1) / kChunkGrain;
+        if (span > kCfSerialChunks && (int)(g0 + lo) < p.vcap) vout.cf[c] = (int)(g0 + lo);
     }
 }
 
@@ -794,7 +814,7 @@ struct DutyClock {
     {
         unsigned long long a = 0;
         if (p.duty && threadIdx.x == 0) a = globaltimer_ns();
-        const bool ok = grid_barrier(&st->barrier, &st->release, generation, &st->error, s_flag);
+        const bool ok = grid_barrier(&st->barrier, generation, &st->error, s_flag);
         if (p.duty && threadIdx.x == 0) waited += globaltimer_ns() - a;
         return ok;
     }
@@ -1105,7 +1125,6 @@ __global__ void init_kernel(BfsParams p)
         st->cur_level = 0;
         st->epoch += 1ull << 24;
         st->barrier = 0;
-        st->release = 0;
         st->error = 0;
         st->max_level = 0;
         st->done = 0;

@@ -39,12 +39,11 @@ struct alignas(128) SearchState {
     // qe[(k + 1) % 3]; each value packs (count << 32 | edge total).
     unsigned long long qe[3];
     uint32_t tile_ctr[3];      // look-back tile counters, by pass % 3
-    // ---- line 1: grid-barrier arrivals (atomics only, nobody polls this line)
+    // ---- line 1: the grid barrier's arrival counter (polled by waiting CTAs)
     alignas(128) unsigned long long barrier;  // arrivals of the current persistent launch
-    uint32_t finished;         // CTAs that finished the current non-persistent launch
-    // ---- line 2: what waiting CTAs poll (the barrier's release and the error word)
-    alignas(128) unsigned long long release;  // generation of the last completed grid barrier
-    uint32_t error;            // dev::kErr* bits
+    // ---- line 2: the error word (polled now and then) and launch epilogue counter
+    alignas(128) uint32_t error;  // dev::kErr* bits
+    uint32_t finished;            // CTAs that finished the current non-persistent launch
     // ---- line 3 on: per-search bookkeeping
     alignas(128) int32_t cur_level;  // next level to process
     unsigned long long epoch;  // look-back epoch base for this search

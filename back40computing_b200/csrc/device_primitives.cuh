@@ -95,39 +95,34 @@ __device__ __forceinline__ unsigned lanemask_lt()
 }
 
 // ---- bounded grid barrier ------------------------------------------------------
-// Arrivals and release live on separate cache lines: every CTA adds one to the
-// monotone arrival counter; the CTA whose arrival completes the g-th barrier
-// (counter reaches g * gridDim.x) publishes g in the release word, which the
-// others poll.  Polls then never queue behind arrivals (or behind the frontier
-// counters' atomics) on one L2 line.  Both words are zeroed before each
+// Monotone arrival counter: the g-th barrier of a launch completes when the
+// counter reaches g * gridDim.x; waiters poll the counter itself (one round
+// trip less than a separate release flag).  The counter sits on its own cache
+// line, away from the frontier counters' atomics.  It is zeroed before each
 // persistent launch.  Requires every CTA to be resident (cooperative launch).
 // Returns false when the wait expired or another CTA reported an error.
-__device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned long long *release,
-                                             unsigned &generation, unsigned *error_word, int *s_flag)
+__device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word,
+                                             int *s_flag)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
         generation++;
         const unsigned long long target = (unsigned long long)generation * gridDim.x;
         __threadfence();
+        atomicAdd(counter, 1ull);
+        unsigned spins = 0;
         int ok = 1;
-        if (atomicAdd(counter, 1ull) + 1 == target) {
-            __threadfence();
-            st_release(release, (unsigned long long)generation);
-        } else {
-            unsigned spins = 0;
-            while (ld_acquire(release) < (unsigned long long)generation) {
-                if (++spins > kSpinLimit) {
-                    atomicOr(error_word, kErrBarrier);
-                    ok = 0;
-                    break;
-                }
-                if ((spins & 7) == 0 && ld_cg(error_word) != 0) {
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(spins < 64 ? 32 : 256);
+        while (ld_acquire(counter) < target) {
+            if (++spins > kSpinLimit) {
+                atomicOr(error_word, kErrBarrier);
+                ok = 0;
+                break;
             }
+            if ((spins & 7) == 0 && ld_cg(error_word) != 0) {
+                ok = 0;
+                break;
+            }
+            __nanosleep(spins < 64 ? 32 : 256);
         }
         __threadfence();
         if (ok && ld_cg(error_word) != 0) ok = 0;

@@ -65,7 +65,6 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         const int threshold = grid * pol.saturation_quit;
         while (true) {
             CUDA_TRY(cudaMemsetAsync(&p->st->barrier, 0, sizeof(unsigned long long), p->stream), "barrier reset");
-            CUDA_TRY(cudaMemsetAsync(&p->st->release, 0, sizeof(unsigned long long), p->stream), "release reset");
             CUDA_TRY(cudaMemsetAsync(&p->st->saturated, 0, sizeof(int32_t), p->stream), "flag reset");
             if ((rc = launch_cooperative(p, kern, grid, smem, kf, "cooperative launch of the contract-expand kernel")))
                 return rc;

@@ -396,7 +396,6 @@ __global__ void msbfs_init_kernel(BfsParams p, MsParams m)
         st->epoch += 1ull << 24;
         st->cur_level = 0;
         st->barrier = 0;
-        st->release = 0;
         st->error = 0;
         st->max_level = 0;
         st->done = 0;
