@@ -59,6 +59,7 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     if ((rc = ensure_slots(p))) return rc;
     if ((rc = ensure_batch(p, k))) return rc;
     if ((rc = check_symmetric(p))) return rc;
+    if (p->symmetric == 1 && pol.bottom_up_hub_probes > 0 && (rc = ensure_hubs(p))) return rc;
     // distinct source vertices with their combined source masks; they travel
     // to the device as kernel arguments, so nothing on the host is reused
     // while an earlier batch is still queued
@@ -81,6 +82,7 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     seed.n_distinct = nd;
 
     BfsParams bp = make_params(p, pol);
+    if (p->symmetric != 1) bp.hub2 = nullptr;  // pull levels (and so the pair) only on symmetric graphs
     dev::MsParams m{};
     m.visited = p->d_ms_visited;
     m.fmask[0] = p->d_ms_fmask[0];

@@ -226,8 +226,15 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
                     r1 = ld_ro(p.row_offsets + v + 1);
                 }
             }
-            const bool longlist = missing && (r1 - r0) > kPullLongList;
             unsigned long long acc = 0;
+            if (missing && p.hub2) {
+                // the vertex's two highest-degree neighbours first (one coalesced load)
+                const int2 h = p.hub2[v];
+                if (h.x >= 0) acc |= ld_cg64(fcur + h.x) & missing;
+                if (h.y >= 0) acc |= ld_cg64(fcur + h.y) & missing;
+                if (acc == missing || r1 - r0 <= 2) missing = 0;  // nothing left to look for
+            }
+            const bool longlist = missing && (r1 - r0) > kPullLongList;
             if (missing && !longlist) {
                 for (int e = r0; e < r1 && acc != missing; e += U) {
                     int nb[U];

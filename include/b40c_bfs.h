@@ -98,9 +98,10 @@ typedef struct b40c_bfs_policy {
                                       by the whole warp; default), 2 = the CTA scans all such lists
                                       together, edge-parallel, 3 = lanes for 16 more neighbours, then
                                       the CTA edge-parallel for what is left; 0 = default */
-    int32_t bottom_up_hub_probes;  /* bottom-up levels (scan 1) first probe each vertex's two
-                                      highest-degree neighbours (a per-vertex pair built once per
-                                      problem, 8 bytes per vertex): 1 = on (default), -1 = off */
+    int32_t bottom_up_hub_probes;  /* bottom-up levels (scan 1) and batched pull levels first probe
+                                      each vertex's two highest-degree neighbours (a per-vertex pair
+                                      built once per symmetric problem, 8 bytes per vertex):
+                                      1 = on (default), -1 = off */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

@@ -377,3 +377,22 @@ def test_bottom_up_scan_variants(scan, hub, kind, args, preds):
             assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
         else:
             assert oracle.compare_labels(got, want) == -1
+
+
+@pytest.mark.parametrize("hub", [1, -1])
+@pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 14, 10))])
+def test_batched_pull_hub_probes(hub, kind, args):
+    """Batched searches with and without the hub-pair probes in pull levels
+    (alpha 2 makes most levels pull) give every slot the oracle's labels."""
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g)
+    srcs = sample_sources(g, 40, seed=12)
+    pol = N.Policy()
+    pol.bottom_up_hub_probes = hub
+    pol.bottom_up_alpha = 2
+    p.msbfs(srcs, policy=pol)
+    depths = p.msbfs_depths()
+    for slot in (0, 7, 39):
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+        assert depths[slot] == depth
