@@ -60,7 +60,10 @@ struct ExpandSmem {
     unsigned long long visited_edges;  // degree sum of the vertices visited up to this pass
     int32_t prev_bu;                   // the previous level ran bottom-up
     uint32_t *mask;                    // the visited-mask buffer of this pass (mask or mask_alt)
-    int32_t wl_count;                  // bottom-up worklist entries of the current chunk
+    int32_t wl_count;                  // bottom-up: still-unvisited vertices of the current chunk (in stage)
+    int32_t ul_in;                     // bottom-up list mode: buffer holding this pass's unvisited list, or -1
+    int32_t ul_n;                      // entries of that list
+    int32_t ul_base;                   // where this chunk's still-unvisited vertices go in the next list
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -140,14 +143,24 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
         go[t] = valid[t];
         if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
         word[t] = 0;
-        if (go[t] && p.precheck) word[t] = ld_mask(s.mask + (v[t] >> 5));
+        if (go[t] && p.precheck && s.ul_in < 0) word[t] = ld_mask(s.mask + (v[t] >> 5));
     }
     bool found[U];
+    if (s.ul_in >= 0) {
+        // after a bottom-up list-mode level the visited mask is not kept: the
+        // labels decide (a distance search's unreached vertices hold -1)
 #pragma unroll
-    for (int t = 0; t < U; t++) {
-        const unsigned bit = 1u << (v[t] & 31);
-        found[t] = false;
-        if (go[t] && !(word[t] & bit)) found[t] = !(atomicOr(s.mask + (v[t] >> 5), bit) & bit);
+        for (int t = 0; t < U; t++) {
+            found[t] = false;
+            if (go[t] && ld_cg(p.labels + v[t]) == -1) found[t] = atomicCAS(p.labels + v[t], -1, label_value) == -1;
+        }
+    } else {
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            const unsigned bit = 1u << (v[t] & 31);
+            found[t] = false;
+            if (go[t] && !(word[t] & bit)) found[t] = !(atomicOr(s.mask + (v[t] >> 5), bit) & bit);
+        }
     }
     int r0[U], r1[U];
 #pragma unroll
@@ -494,27 +507,38 @@ constexpr int kBottomUpLongList = 256;  // lists longer than this are searched w
 // (short lists one lane each, four neighbours at a time; long lists by the
 // whole warp, 32 neighbours at a time).
 constexpr int kBottomUpProbe = 2;
-constexpr int kBottomUpLaneSteps = 4;  // bottom_up_scan 3: lane steps (4 neighbours each) before the worklist
+
+// Visited-before-this-level tests of a batch of neighbours: the level-start
+// mask snapshot (bit test), or in list mode the distance labels (a label in
+// [0, level] was written before this level; this level writes level + 1).
+template <bool LABELS>
+__device__ __forceinline__ unsigned probe_load(const uint32_t *mask, const int32_t *labels, int u)
+{
+    return LABELS ? (unsigned)ld_cg(labels + u) : ld_mask(mask + (u >> 5));
+}
+template <bool LABELS>
+__device__ __forceinline__ bool probe_hit(unsigned x, int u, int level)
+{
+    return LABELS ? ((int)x >= 0 && (int)x <= level) : (((x >> (u & 31)) & 1u) != 0);
+}
 
 // Bottom-up continuation, one lane per vertex: each lane scans its own list
-// on, four neighbours at a time; lists longer than kBottomUpLongList are
-// searched by the whole warp, 32 neighbours at a time.
-template <int PER, int K, int MAX_ITER, int MIN_LEN = K>
-__device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, const bool (&todo)[PER],
-                                                const int (&r0)[PER], const int (&r1)[PER], int (&parent)[PER])
+// on (K neighbours already probed at its start; lists of at most MIN_LEN are
+// finished), four neighbours at a time; lists longer than kBottomUpLongList
+// are searched by the whole warp, 32 neighbours at a time.
+template <int PER, int K, int MIN_LEN, bool LABELS>
+__device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, int level,
+                                                const bool (&todo)[PER], const int (&r0)[PER], const int (&r1)[PER],
+                                                int (&parent)[PER])
 {
     const int lane = threadIdx.x & 31;
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        // K neighbours already probed at the list's start; lists of at most
-        // MIN_LEN are finished
         const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > MIN_LEN;
         if (!__any_sync(0xffffffffu, more)) continue;
-        // capped: no warp-cooperative lists, at most MAX_ITER steps per lane
-        const bool longlist = MAX_ITER == 0 && more && (r1[t] - r0[t]) > kBottomUpLongList;
+        const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
         bool scan = more && !longlist;
         int e = r0[t] + K;
-        int iter = 0;
         while (__any_sync(0xffffffffu, scan)) {
             if (scan) {
                 int nb[4];
@@ -522,14 +546,13 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
 #pragma unroll
                 for (int k = 0; k < 4; k++) nb[k] = (e + k < r1[t]) ? ld_stream(p.column_indices + e + k) : -1;
 #pragma unroll
-                for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
+                for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? probe_load<LABELS>(mask, p.labels, nb[k]) : 0u;
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (parent[t] < 0 && nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) parent[t] = nb[k];
+                    if (parent[t] < 0 && nb[k] >= 0 && probe_hit<LABELS>(w[k], nb[k], level)) parent[t] = nb[k];
                 e += 4;
                 if (parent[t] >= 0 || e >= r1[t]) scan = false;
             }
-            if (MAX_ITER > 0 && ++iter >= MAX_ITER) break;  // warp-uniform
         }
         unsigned lmask = __ballot_sync(0xffffffffu, longlist);
         while (lmask) {
@@ -541,7 +564,7 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
             for (int eb = lr0; eb < lr1; eb += 32) {
                 const int ee = eb + lane;
                 const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
-                const bool hit = nb >= 0 && ((ld_mask(mask + (nb >> 5)) >> (nb & 31)) & 1u);
+                const bool hit = nb >= 0 && probe_hit<LABELS>(probe_load<LABELS>(mask, p.labels, nb), nb, level);
                 const unsigned hb = __ballot_sync(0xffffffffu, hit);
                 if (hb) {
                     found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
@@ -553,116 +576,32 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
     }
 }
 
-// Bottom-up continuation, the CTA together: the unresolved vertices of the
-// chunk (no parent among their first K neighbours, more neighbours left) form
-// a shared worklist (colstart = next edge, rel = remaining edges, then their
-// exclusive scan; out = parent found); its edges are then scanned
-// edge-parallel in rounds of kChunkMax positions, each thread issuing PER
-// independent neighbour loads and mask probes per round, skipping vertices
-// resolved in earlier rounds.  Any visited neighbour is a valid parent (all
-// are one level up); several hits for one vertex simply overwrite each other.
-template <int B, bool PRED, int PER, int KS>
-__device__ __forceinline__ void bottom_up_worklist(const BfsParams &p, ExpandSmem<B, PRED> &s, const uint32_t *mask,
-                                                   const bool (&todo)[PER], const int (&r0)[PER],
-                                                   const int (&r1)[PER], int (&parent)[PER])
+// Still-unvisited vertices of a bottom-up chunk, collected in s.stage (free
+// during bottom-up levels) and then appended to the next unvisited list with
+// one atomic per chunk.  Called by whole warps.
+template <typename Smem>
+__device__ __forceinline__ void append_unvisited(Smem &s, bool keep, int v)
 {
-    const int tid = threadIdx.x, lane = tid & 31;
-    if (tid == 0) s.wl_count = 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, keep);
+    if (bal == 0) return;
+    const int lane = threadIdx.x & 31, leader = __ffs(bal) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(&s.wl_count, __popc(bal));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (keep) s.stage[base + __popc(bal & lanemask_lt())] = v;
+}
+
+template <int B, typename Smem>
+__device__ __forceinline__ void write_unvisited(const BfsParams &p, Smem &s, int32_t *list, unsigned *ctr)
+{
     __syncthreads();
-    // a candidate's worklist slot is kept in stage[t * B + tid] (free during
-    // bottom-up levels), not in registers
-#pragma unroll
-    for (int t = 0; t < PER; t++) {
-        const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > KS;
-        const unsigned bal = __ballot_sync(0xffffffffu, more);
-        if (bal == 0) continue;
-        const int leader = __ffs(bal) - 1;
-        int base = 0;
-        if (lane == leader) base = atomicAdd(&s.wl_count, __popc(bal));
-        base = __shfl_sync(0xffffffffu, base, leader);
-        if (more) {
-            const int sl = base + __popc(bal & lanemask_lt());
-            s.stage[t * B + tid] = sl;
-            s.colstart[sl] = r0[t] + KS;
-            s.rel[sl] = r1[t] - r0[t] - KS;
-            s.out[sl] = -1;
-        }
-    }
+    const int n = s.wl_count;
+    if (n == 0) return;  // CTA-uniform
+    if (threadIdx.x == 0) s.ul_base = (int)atomicAdd(ctr, (unsigned)n);
     __syncthreads();
-    const int W = s.wl_count;
-    if (W == 0) return;  // CTA-uniform
-    // exclusive scan of the remaining lengths, in place, with the total at rel[W]
-    {
-        int loc[PER];
-        unsigned long long sum = 0;
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const int i = tid * PER + k;
-            loc[k] = i < W ? s.rel[i] : 0;
-            sum += (unsigned long long)loc[k];
-        }
-        unsigned long long total;
-        unsigned long long run = cta_exclusive_scan<B>(sum, s.scan_warp, &total);
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < PER; k++) {
-            const int i = tid * PER + k;
-            if (i < W) s.rel[i] = (int)run;
-            run += (unsigned long long)loc[k];
-        }
-        if (tid == 0) s.rel[W] = (int)total;
-    }
-    __syncthreads();
-    const int D = s.rel[W];
-    for (int base = 0; base < D; base += kChunkMax) {
-        const int len = min(kChunkMax, D - base);
-        // owner map of this round's positions (entries have nonzero lengths)
-        {
-            const int x0 = tid * PER;
-            if (x0 < len) {
-                int lo = 0, hi = W - 1;
-                while (lo < hi) {
-                    const int mid = (lo + hi + 1) >> 1;
-                    if (s.rel[mid] <= base + x0) lo = mid; else hi = mid - 1;
-                }
-                int j = lo;
-                int next = s.rel[j + 1];
-#pragma unroll
-                for (int k = 0; k < PER; k++) {
-                    const int x = x0 + k;
-                    if (x < len) {
-                        while (base + x >= next) {
-                            j++;
-                            next = s.rel[j + 1];
-                        }
-                        s.own[x] = (uint16_t)j;
-                    }
-                }
-            }
-        }
-        __syncthreads();
-        int nb[PER];
-#pragma unroll
-        for (int u = 0; u < PER; u++) {
-            const int x = u * B + tid;
-            nb[u] = -1;
-            if (x < len) {
-                const int j = s.own[x];
-                if (s.out[j] < 0) nb[u] = ld_stream(p.column_indices + s.colstart[j] + (base + x - s.rel[j]));
-            }
-        }
-        unsigned w[PER];
-#pragma unroll
-        for (int u = 0; u < PER; u++) w[u] = nb[u] >= 0 ? ld_mask(mask + (nb[u] >> 5)) : 0u;
-#pragma unroll
-        for (int u = 0; u < PER; u++)
-            if (nb[u] >= 0 && ((w[u] >> (nb[u] & 31)) & 1u)) s.out[s.own[u * B + tid]] = nb[u];
-        __syncthreads();
-    }
-#pragma unroll
-    for (int t = 0; t < PER; t++)
-        if (todo[t] && parent[t] < 0 && r1[t] - r0[t] > KS) parent[t] = s.out[s.stage[t * B + tid]];
-    __syncthreads();  // the output phase reuses colstart / rel / out
+    const int base = s.ul_base;
+    for (int j = threadIdx.x; j < n; j += B)
+        if (base + j < p.nodes) list[base + j] = s.stage[j];
 }
 
 template <int B, bool PRED>
@@ -677,7 +616,11 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
-        if (tid == 0) s.out_count = 0;
+        if (tid == 0) {
+            s.out_count = 0;
+            s.wl_count = 0;
+        }
+        __syncthreads();  // the counters are reset before any warp appends
         // ---- own visited words (the snapshot is read coherently: ld.cg) ----------
         unsigned word[PER];
 #pragma unroll
@@ -731,20 +674,10 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             }
         }
         // ---- continue the scan for candidates still without a parent ---------------
-        if (p.bu_scan == 2) {
-            bottom_up_worklist<B, PRED, PER, K>(p, s, mask, todo, r0, r1, parent);
-        } else if (p.bu_scan == 3) {
-            // short scans per lane, then whatever is left edge-parallel: lists the
-            // lanes did not finish are mostly vertices with no parent this level,
-            // whose lists must be read whole anyway
-            bottom_up_lanes<PER, K, kBottomUpLaneSteps>(p, mask, todo, r0, r1, parent);
-            bottom_up_worklist<B, PRED, PER, K + 4 * kBottomUpLaneSteps>(p, s, mask, todo, r0, r1, parent);
-        } else if (p.hub2) {
-            // the pair came from anywhere in the list: lists longer than two are scanned from the start
-            bottom_up_lanes<PER, 0, 0, K>(p, mask, todo, r0, r1, parent);
-        } else {
-            bottom_up_lanes<PER, K, 0>(p, mask, todo, r0, r1, parent);
-        }
+        if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
+            bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
+        else
+            bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
         // ---- label, mark and append the discoveries --------------------------------
 #pragma unroll
         for (int t = 0; t < PER; t++) {
@@ -754,6 +687,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             const bool found = parent[t] >= 0;
             const unsigned fb = __ballot_sync(0xffffffffu, found);
             if (lane == 0) mask_out[vb >> 5] = word[t] | fb;  // this warp owns the whole word
+            if (p.ul[0]) append_unvisited(s, todo[t] && !found, v);
             if (fb == 0) continue;
             if (found) {
                 p.labels[v] = PRED ? parent[t] : level + 1;
@@ -772,6 +706,113 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         }
         __syncthreads();
         emit_frontier<B>(p, s, pass, vout, qe_out);
+        if (p.ul[0]) write_unvisited<B>(p, s, p.ul[0], &p.st->ul_count[(pass + 1) % 3]);
+        __syncthreads();
+    }
+}
+
+// Bottom-up list mode (distance searches, a bottom-up level right after the
+// first one, or later): instead of every vertex id, the CTA's share of the
+// list of vertices still unvisited after the last bottom-up level (entries
+// found meanwhile by top-down levels are skipped by their label).  A
+// neighbour counts as visited when its distance label was written before this
+// level (in [0, level]; this level writes level + 1), so the visited mask is
+// neither read nor written: after the first list-mode level it is given up for
+// the rest of the search (top-down levels then claim vertices on the labels).
+// The vertices still without a parent form the next list.
+template <int B, bool PRED>
+__device__ __forceinline__ void bottom_up_list(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
+                                               const VertexFrontier &vout, unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr int PER = kChunkMax / B;
+    constexpr int K = kBottomUpProbe;
+    const int32_t *in = p.ul[s.ul_in];
+    int32_t *outl = p.ul[s.ul_in ^ 1];
+    unsigned *ctr = &p.st->ul_count[(pass + 1) % 3];
+    int rs, re;
+    cta_range(s.ul_n, blockIdx.x, gridDim.x, rs, re);
+    for (int cs = rs; cs < re; cs += kChunkMax) {
+        if (tid == 0) {
+            s.out_count = 0;
+            s.wl_count = 0;
+        }
+        __syncthreads();
+        int v[PER], r0[PER], r1[PER];
+        bool todo[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int i = cs + t * B + tid;
+            v[t] = i < re ? ld_cg(in + i) : -1;
+        }
+#pragma unroll
+        for (int t = 0; t < PER; t++) todo[t] = v[t] >= 0 && ld_cg(p.labels + v[t]) == -1;
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            r0[t] = r1[t] = 0;
+            if (todo[t]) {
+                r0[t] = ld_ro(p.row_offsets + v[t]);
+                r1[t] = ld_ro(p.row_offsets + v[t] + 1);
+            }
+        }
+        int parent[PER];
+        {
+            int nb[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                if (p.hub2) {
+                    int2 h = make_int2(-1, -1);
+                    if (todo[t]) h = p.hub2[v[t]];
+                    nb[t][0] = h.x;
+                    nb[t][1] = h.y;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+                }
+            }
+            unsigned w[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++)
+#pragma unroll
+                for (int k = 0; k < K; k++) w[t][k] = nb[t][k] >= 0 ? probe_load<true>(nullptr, p.labels, nb[t][k]) : 0u;
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                parent[t] = -1;
+#pragma unroll
+                for (int k = K - 1; k >= 0; k--)
+                    if (nb[t][k] >= 0 && probe_hit<true>(w[t][k], nb[t][k], level)) parent[t] = nb[t][k];
+            }
+        }
+        if (p.hub2)
+            bottom_up_lanes<PER, 0, K, true>(p, nullptr, level, todo, r0, r1, parent);
+        else
+            bottom_up_lanes<PER, K, K, true>(p, nullptr, level, todo, r0, r1, parent);
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            if (t * B >= re - cs) continue;  // CTA-uniform
+            const bool found = parent[t] >= 0;
+            append_unvisited(s, todo[t] && !found, v[t]);
+            const unsigned fb = __ballot_sync(0xffffffffu, found);
+            if (fb == 0) continue;
+            if (found) {
+                p.labels[v[t]] = level + 1;
+                s.flag = 1;
+            }
+            const int leader = __ffs(fb) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&s.out_count, __popc(fb));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (found) {
+                const int slot = base + __popc(fb & lanemask_lt());
+                s.out[slot] = v[t];
+                s.colstart[slot] = r0[t];
+                s.rel[slot] = r1[t] - r0[t];
+            }
+        }
+        __syncthreads();
+        emit_frontier<B>(p, s, pass, vout, qe_out);
+        write_unvisited<B>(p, s, outl, ctr);
         __syncthreads();
     }
 }
@@ -881,6 +922,17 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
         s.visited_edges = ld_cg64(&p.st->visited_edges[pass % 3]) + (unsigned long long)s.E;
         s.prev_bu = ld_cg(&p.st->dir[pass % 3]);
         s.mask = ld_cg(&p.st->mask_sel[pass % 3]) ? p.mask_alt : p.mask;
+        s.ul_in = -1;
+        s.ul_n = 0;
+        if (p.ul[0]) {
+            s.ul_in = ld_cg(&p.st->ul_sel[pass % 3]);
+            s.ul_n = (int)ld_cg(&p.st->ul_count[pass % 3]);
+            if (s.ul_n > p.nodes || s.ul_in > 1) {  // never read past a list
+                atomicOr(&p.st->error, kErrOverflow);
+                s.q = 0;
+            }
+            if (blockIdx.x == 0) p.st->ul_count[(pass + 2) % 3] = 0;
+        }
         if (p.levels && blockIdx.x == 0 && pass < kMaxLevelRecords) {
             LevelRecord r;
             r.vertices = s.q;
@@ -898,11 +950,17 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
 // whether the level ran bottom-up and which mask buffer the next pass reads
 // (a bottom-up level writes the other one).
 __device__ __forceinline__ void record_direction(const BfsParams &p, unsigned long long visited_edges, int pass,
-                                                 bool bu, const uint32_t *pass_mask)
+                                                 bool bu, const uint32_t *pass_mask, int ul_in, int ul_n)
 {
     p.st->visited_edges[(pass + 1) % 3] = visited_edges;
     p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
     p.st->mask_sel[(pass + 1) % 3] = (pass_mask == p.mask) == bu ? 1 : 0;
+    if (p.ul[0]) {
+        // a bottom-up level writes the next list (range mode into buffer 0,
+        // list mode into the other buffer); a top-down level carries it on
+        p.st->ul_sel[(pass + 1) % 3] = bu ? (ul_in < 0 ? 0 : ul_in ^ 1) : ul_in;
+        if (!bu) p.st->ul_count[(pass + 1) % 3] = (uint32_t)ul_n;
+    }
     if (bu && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
 }
 
@@ -941,7 +999,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             // ---- small frontiers: CTA 0 alone, level after level ----------------------
             if (blockIdx.x == 0) {
                 for (int solo = 0;; solo++) {
-                    if (tid == 0) record_direction(p, s.visited_edges, pass, false, s.mask);
+                    if (tid == 0) record_direction(p, s.visited_edges, pass, false, s.mask, s.ul_in, s.ul_n);
                     expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
                                                 &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
                     __syncthreads();
@@ -969,8 +1027,10 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
-        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu, s.mask);
-        if (bu)
+        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n);
+        if (bu && s.ul_in >= 0)
+            bottom_up_list<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        else if (bu)
             bottom_up_range<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         else
             expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
@@ -1134,6 +1194,8 @@ __global__ void init_kernel(BfsParams p)
         st->qe[1] = st->qe[2] = 0;
         st->dir[0] = st->dir[1] = st->dir[2] = 0;
         st->mask_sel[0] = st->mask_sel[1] = st->mask_sel[2] = 0;
+        st->ul_sel[0] = st->ul_sel[1] = st->ul_sel[2] = -1;
+        st->ul_count[0] = st->ul_count[1] = st->ul_count[2] = 0;
         st->visited_edges[0] = st->visited_edges[1] = st->visited_edges[2] = 0;
         if (VERTEX_FRONTIER) {
             const int deg = r1 - r0;

@@ -39,6 +39,11 @@ struct alignas(128) SearchState {
     // qe[(k + 1) % 3]; each value packs (count << 32 | edge total).
     unsigned long long qe[3];
     uint32_t tile_ctr[3];      // look-back tile counters, by pass % 3
+    // bottom-up list mode (direction-optimizing distance searches): the list of
+    // still-unvisited vertices a pass reads, by pass % 3 like qe: buffer index
+    // (-1: none yet) and entries
+    int32_t ul_sel[3];
+    uint32_t ul_count[3];
     // ---- line 1: the grid barrier's arrival counter (polled by waiting CTAs)
     alignas(128) unsigned long long barrier;  // arrivals of the current persistent launch
     // ---- line 2: the error word (polled now and then) and launch epilogue counter
@@ -128,6 +133,7 @@ struct BfsParams {
     int32_t bu_scan;          // bottom-up continuation: 1 per lane, 2 per CTA (edge-parallel worklist)
     const uint32_t *iso;      // bit v: v has no edges in or out; a search starts with these bits visited (null: none)
     const int2 *hub2;         // per vertex its two highest-degree neighbours, probed first bottom-up (null: off)
+    int32_t *ul[2];           // unvisited-vertex lists of bottom-up list mode (null: off; distance mode only)
     uint32_t *mask_alt;       // second visited-mask buffer: a bottom-up level reads one buffer and writes
                               // every word of the other (old bits | its discoveries), then they swap
     LevelRecord *levels;      // per-pass records when instrumented, else null

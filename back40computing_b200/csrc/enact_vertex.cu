@@ -17,9 +17,15 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
     if ((rc = ensure_slots(p))) return rc;
     if (direction_opt && pol.bottom_up_hub_probes > 0 && (rc = ensure_hubs(p))) return rc;
+    if (direction_opt && !PRED && (rc = ensure_unvisited_lists(p))) return rc;
     BfsParams k = make_params(p, pol);
     k.direction_opt = direction_opt ? 1 : 0;
-    if (!direction_opt || pol.bottom_up_scan != 1) k.hub2 = nullptr;
+    if (!direction_opt) k.hub2 = nullptr;
+    if (direction_opt && !PRED) {
+        // distance searches: bottom-up levels after the first one scan the unvisited list
+        k.ul[0] = p->d_ul[0];
+        k.ul[1] = p->d_ul[1];
+    }
     const void *kern = (const void *)dev::ec_kernel<kThreads, PRED>;
     const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
     int grid = 0;

@@ -191,9 +191,8 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     if (d.bottom_up_alpha < 1 || d.bottom_up_beta < 1)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_alpha and bottom_up_beta must be >= 1");
     if (d.saturation_quit < 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.saturation_quit must be >= 1");
-    if (d.bottom_up_scan < 1 || d.bottom_up_scan > 3)
-        return b40c::fail(B40C_ERROR_INVALID_VALUE,
-                          "policy.bottom_up_scan must be 1 (per lane), 2 (per CTA) or 3 (lanes, then per CTA)");
+    if (d.bottom_up_scan != 1)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_scan must be 1 (per-lane list scans)");
     if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
     *out = d;
     return B40C_SUCCESS;
@@ -212,6 +211,8 @@ int64_t device_bytes(const b40c_bfs_problem *p)
     if (p->d_mask) t += mask;
     if (p->d_iso) t += mask;
     if (p->d_hub2) t += a(8 * n);
+    for (int i = 0; i < 2; i++)
+        if (p->d_ul[i]) t += a(4 * n);
     if (p->d_next) t += mask;
     if (p->st) t += a(sizeof(SearchState));
     if (p->slots) t += a((int64_t)sizeof(dev::LookbackSlot) * p->max_slots);
@@ -242,7 +243,8 @@ int64_t planned_bytes(int64_t n, int64_t m, int k, double qs)
     int64_t t = a(4 * (n + 1)) + a(4 * std::max<int64_t>(m, 1));
     t += a(4 * n) + 3 * mask + a(sizeof(SearchState)) + a((int64_t)sizeof(dev::LookbackSlot) * slots);
     t += 2 * (2 * a(4 * cap) + a(4 * (cap + 1)) + a(4 * cf_len));
-    t += a(8 * n);  // hub pairs (built by the server for every graph)
+    t += a(8 * n);      // hub pairs (built by the server for every graph)
+    t += 2 * a(4 * n);  // unvisited lists (direction-optimizing distance searches)
     if (k > 0) t += 3 * a(8 * n) + 2 * a(4 * 64) + a(4 * n * (int64_t)k);
     return t;
 }
@@ -441,6 +443,17 @@ int ensure_hubs(b40c_bfs_problem *p)
     const int blocks = std::max(1, std::min<int>(p->sms * 16, (int)((p->nodes * 32 + 255) / 256)));
     hub_pair_kernel<<<blocks, 256, 0, p->stream>>>(p->d_ro, p->d_ci, (int32_t)p->nodes, (int2 *)p->d_hub2);
     CUDA_TRY(cudaGetLastError(), "hub pair launch");
+    return B40C_SUCCESS;
+}
+
+// The two unvisited-vertex lists of bottom-up list mode (4 bytes per vertex each).
+int ensure_unvisited_lists(b40c_bfs_problem *p)
+{
+    for (int i = 0; i < 2; i++)
+        if (!p->d_ul[i]) {
+            int rc = alloc_dev((void **)&p->d_ul[i], sizeof(int32_t) * (size_t)p->nodes, "unvisited list");
+            if (rc) return rc;
+        }
     return B40C_SUCCESS;
 }
 
@@ -743,6 +756,8 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->d_mask) cudaFree(p->d_mask);
     if (p->d_iso) cudaFree(p->d_iso);
     if (p->d_hub2) cudaFree(p->d_hub2);
+    for (int i = 0; i < 2; i++)
+        if (p->d_ul[i]) cudaFree(p->d_ul[i]);
     if (p->d_next) cudaFree(p->d_next);
     free_batch(p);
     if (p->d_levels) cudaFree(p->d_levels);

@@ -44,6 +44,7 @@ struct b40c_bfs_problem {
     uint32_t *d_next = nullptr;  // second visited-mask buffer (bottom-up levels write it whole)
     uint32_t *d_iso = nullptr;   // bit v: vertex v has no edges in or out (pre-set in every search's visited mask)
     int32_t *d_hub2 = nullptr;   // [2n] per vertex its two highest-degree neighbours (symmetric graphs, lazily)
+    int32_t *d_ul[2] = {nullptr, nullptr};  // [n] each: bottom-up unvisited lists (distance searches, lazily)
     int32_t mask_words = 0;
     int symmetric = -1;          // -1 unknown, else the cached result of the device symmetry test
     // batched multi-source searches (allocated on first use)
@@ -156,6 +157,7 @@ int enact_vertex(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const
                  int32_t depth_limit, bool direction_optimizing);
 int check_symmetric(b40c_bfs_problem *p);
 int ensure_hubs(b40c_bfs_problem *p);
+int ensure_unvisited_lists(b40c_bfs_problem *p);
 void free_batch(b40c_bfs_problem *p);
 int ensure_batch(b40c_bfs_problem *p, int k);
 // Queues a batched search of k <= 64 sources on p->stream (asynchronous).

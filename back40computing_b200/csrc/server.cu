@@ -493,7 +493,8 @@ int b40c_server_add_graph(b40c_server *s, const int32_t *row_offsets, const int3
     if (s->single_strategy >= 0 &&
         (rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, 0, -1, 0, nullptr)))
         return bail(rc);
-    if ((rc = rt::ensure_hubs(p))) return bail(rc);  // charged by the plan whether or not searches use them
+    // charged by the plan whether or not searches use them
+    if ((rc = rt::ensure_hubs(p)) || (rc = rt::ensure_unvisited_lists(p))) return bail(rc);
     if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();
         return bail(b40c::fail((int)e, "graph warm-up failed: %s", cudaGetErrorString(e)));

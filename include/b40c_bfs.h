@@ -93,12 +93,11 @@ typedef struct b40c_bfs_policy {
     int32_t small_frontier_edges;  /* fused searches: runs of levels whose frontier has at most this many
                                       edges are processed by one CTA alone (CTA-level barriers only);
                                       -1 disables */
-    int32_t bottom_up_scan;        /* bottom-up levels, vertices whose first neighbours are not yet
-                                      visited: 1 = each lane scans its own list on (lists longer than 256
-                                      by the whole warp; default), 2 = the CTA scans all such lists
-                                      together, edge-parallel, 3 = lanes for 16 more neighbours, then
-                                      the CTA edge-parallel for what is left; 0 = default */
-    int32_t bottom_up_hub_probes;  /* bottom-up levels (scan 1) and batched pull levels first probe
+    int32_t bottom_up_scan;        /* bottom-up levels, vertices whose first probes found no parent:
+                                      1 = each lane scans its own list on (lists longer than 256 by the
+                                      whole warp); the only variant built (CTA-wide edge-parallel scans
+                                      measured slower); 0 = default */
+    int32_t bottom_up_hub_probes;  /* bottom-up levels and batched pull levels first probe
                                       each vertex's two highest-degree neighbours (a per-vertex pair
                                       built once per symmetric problem, 8 bytes per vertex):
                                       1 = on (default), -1 = off */

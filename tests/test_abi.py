@@ -75,7 +75,8 @@ def test_server_plan_bytes_arithmetic():
     b1, b2, b64 = (BfsServer.plan_bytes(n, m, k) for k in (1, 2, 64))
     assert b2 - b1 == 4 * n and b64 - b1 == 63 * 4 * n
     csr = 4 * (n + 1) + 4 * m
-    # labels 4n, batch masks 24n + one label row 4n, two frontiers ~31n, hub pairs 8n, slots ~m/256
-    assert csr + 4 * n + 3 * 8 * n < b1 < csr + 80 * n + m // 8
+    # labels 4n, batch masks 24n + one label row 4n, two frontiers ~31n, hub pairs 8n,
+    # unvisited lists 8n, slots ~m/256
+    assert csr + 4 * n + 3 * 8 * n < b1 < csr + 88 * n + m // 8
     with pytest.raises(N.B40cError):
         BfsServer.plan_bytes(n, m, 65)

@@ -356,13 +356,12 @@ def test_source_without_edges(strategy, mode):
         assert e.GetStatistics()[1] == depth
 
 
-@pytest.mark.parametrize("scan,hub", [(1, 1), (1, -1), (2, 0), (3, 0)])
+@pytest.mark.parametrize("scan,hub", [(1, 1), (1, -1)])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 15, 12)), ("grid3d", (24,))])
 @pytest.mark.parametrize("preds", [False, True])
 def test_bottom_up_scan_variants(scan, hub, kind, args, preds):
-    """Every bottom-up continuation (per lane with or without the hub-pair
-    probes, CTA worklist, hybrid) gives the oracle's distances and valid
-    predecessors; alpha 2 forces many bottom-up levels."""
+    """Bottom-up levels with and without the hub-pair probes give the oracle's
+    distances and valid predecessors; alpha 2 forces many bottom-up levels."""
     g = _graph(kind, *args)
     p = CsrProblem.from_graph(g, mark_predecessors=preds)
     pol = N.Policy()
@@ -396,3 +395,24 @@ def test_batched_pull_hub_probes(hub, kind, args):
         want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
         assert oracle.compare_labels(p.labels_of(slot), want) == -1
         assert depths[slot] == depth
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("alpha,beta", [(2, 1), (2, 24), (2, 1000), (1, 2)])
+@pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 14, 10)), ("grid3d", (20,))])
+def test_bottom_up_list_mode_and_alternation(mode, alpha, beta, kind, args):
+    """Direction switches in every pattern (bottom-up runs, bottom-up -> top-down
+    -> bottom-up with the unvisited list carried over and top-down levels
+    claiming on the labels) give the oracle's distances in every launch mode."""
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g)
+    pol = N.Policy()
+    pol.bottom_up_alpha = alpha
+    pol.bottom_up_beta = beta
+    for s in sample_sources(g, 3, seed=21):
+        got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, mode=mode, policy=pol)
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        assert oracle.compare_labels(got, want) == -1
+        e = ENACTORS[DIRECTION_OPTIMIZING]()
+        e._problem = p
+        assert e.GetStatistics()[1] == depth
