@@ -45,6 +45,7 @@ class Policy(C.Structure):
         ("small_frontier_edges", C.c_int32),
         ("bottom_up_scan", C.c_int32),
         ("bottom_up_hub_probes", C.c_int32),
+        ("bottom_up_list", C.c_int32),
     ]
 
 

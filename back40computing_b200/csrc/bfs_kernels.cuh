@@ -276,22 +276,40 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
         d += deg;
     }
     if (!__syncthreads_or(long_run)) return;  // CTA-uniform
-    // the long runs: every chunk of the tile finds its owner entry by binary
-    // search, and the owners spanning more than kCfSerialChunks chunks write
+    // the long runs: each thread takes a contiguous stretch of the tile's
+    // chunks, finds the owner of its first chunk by binary search and walks on;
+    // owners spanning more than kCfSerialChunks chunks are written here
     const unsigned tdeg = (unsigned)(tot & 0xffffffffu);
     const unsigned c0 = (d0 + kChunkGrain - 1) / kChunkGrain, c1 = (d0 + tdeg + kChunkGrain - 1) / kChunkGrain;
     if (tid == 0 && c1 > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);
     const unsigned c_end = min(c1, (unsigned)p.cf_cap);
-    for (unsigned c = c0 + tid; c < c_end; c += B) {
-        const int x = (int)(c * kChunkGrain - d0);  // in [0, tdeg)
-        int lo = 0, hi = cnt - 1;                   // last entry whose prefix is <= x
+    const unsigned stretch = (c_end > c0 ? c_end - c0 : 0u) / B + 1;
+    const unsigned cb = c0 + tid * stretch, ce = min(cb + stretch, c_end);
+    if (cb < ce) {
+        const int x0 = (int)(cb * kChunkGrain - d0);  // in [0, tdeg)
+        int lo = 0, hi = cnt - 1;                     // last entry whose prefix is <= x0
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (s.colstart[mid] <= x) lo = mid; else hi = mid - 1;
+            if (s.colstart[mid] <= x0) lo = mid; else hi = mid - 1;
         }
-        const unsigned ed = d0 + (unsigned)s.colstart[lo], edeg = (unsigned)s.rel[lo];
-        const unsigned span = (ed + edeg + kChunkGrain - 1) / kChunkGrain - (ed + kChunkGrain - 1) / kChunkGrain;
-        if (span > kCfSerialChunks && (int)(g0 + lo) < p.vcap) vout.cf[c] = (int)(g0 + lo);
+        int j = lo;
+        int next = j + 1 < cnt ? s.colstart[j + 1] : INT_MAX;
+        bool long_j = false;
+        int j_known = -1;
+        for (unsigned c = cb; c < ce; c++) {
+            const int x = (int)(c * kChunkGrain - d0);
+            while (x >= next) {
+                j++;
+                next = j + 1 < cnt ? s.colstart[j + 1] : INT_MAX;
+            }
+            if (j != j_known) {
+                const unsigned ed = d0 + (unsigned)s.colstart[j], edeg = (unsigned)s.rel[j];
+                long_j = (ed + edeg + kChunkGrain - 1) / kChunkGrain - (ed + kChunkGrain - 1) / kChunkGrain >
+                         kCfSerialChunks;
+                j_known = j;
+            }
+            if (long_j && (int)(g0 + j) < p.vcap) vout.cf[c] = (int)(g0 + j);
+        }
     }
 }
 

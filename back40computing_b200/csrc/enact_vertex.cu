@@ -17,11 +17,12 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     if ((rc = ensure_vf(p, 1, cap_of(p->queue_sizing, p->nodes)))) return rc;
     if ((rc = ensure_slots(p))) return rc;
     if (direction_opt && pol.bottom_up_hub_probes > 0 && (rc = ensure_hubs(p))) return rc;
-    if (direction_opt && !PRED && (rc = ensure_unvisited_lists(p))) return rc;
+    const bool lists = direction_opt && !PRED && pol.bottom_up_list > 0;
+    if (lists && (rc = ensure_unvisited_lists(p))) return rc;
     BfsParams k = make_params(p, pol);
     k.direction_opt = direction_opt ? 1 : 0;
     if (!direction_opt) k.hub2 = nullptr;
-    if (direction_opt && !PRED) {
+    if (lists) {
         // distance searches: bottom-up levels after the first one scan the unvisited list
         k.ul[0] = p->d_ul[0];
         k.ul[1] = p->d_ul[1];

@@ -101,6 +101,9 @@ typedef struct b40c_bfs_policy {
                                       each vertex's two highest-degree neighbours (a per-vertex pair
                                       built once per symmetric problem, 8 bytes per vertex):
                                       1 = on (default), -1 = off */
+    int32_t bottom_up_list;        /* distance searches: the first bottom-up level lists the vertices it
+                                      left unvisited and later bottom-up levels scan only that list
+                                      (testing neighbours on the labels): 1 = on, -1 = off (default) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

@@ -397,10 +397,11 @@ def test_batched_pull_hub_probes(hub, kind, args):
         assert depths[slot] == depth
 
 
+@pytest.mark.parametrize("lists", [1, -1])
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("alpha,beta", [(2, 1), (2, 24), (2, 1000), (1, 2)])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 14, 10)), ("grid3d", (20,))])
-def test_bottom_up_list_mode_and_alternation(mode, alpha, beta, kind, args):
+def test_bottom_up_list_mode_and_alternation(lists, mode, alpha, beta, kind, args):
     """Direction switches in every pattern (bottom-up runs, bottom-up -> top-down
     -> bottom-up with the unvisited list carried over and top-down levels
     claiming on the labels) give the oracle's distances in every launch mode."""
@@ -409,6 +410,7 @@ def test_bottom_up_list_mode_and_alternation(mode, alpha, beta, kind, args):
     pol = N.Policy()
     pol.bottom_up_alpha = alpha
     pol.bottom_up_beta = beta
+    pol.bottom_up_list = lists
     for s in sample_sources(g, 3, seed=21):
         got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, mode=mode, policy=pol)
         want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
