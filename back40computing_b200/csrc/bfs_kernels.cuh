@@ -83,6 +83,16 @@ __device__ __forceinline__ void stamp(const BfsParams &p, int pass, int phase)
         p.arrive[((size_t)pass * kMaxArriveCtas + blockIdx.x) * kPhaseStamps + phase] = globaltimer_ns();
 }
 
+// The same after a CTA barrier (so the stamp marks the slowest warp), only in
+// instrumented searches; `when` and p.arrive are CTA-uniform.
+__device__ __forceinline__ void stamp_synced(const BfsParams &p, int pass, int phase, bool when)
+{
+    if (when && p.arrive) {
+        __syncthreads();
+        stamp(p, pass, phase);
+    }
+}
+
 // Packed (count, degree) pair: count in the high 32 bits.
 __device__ __forceinline__ unsigned long long pack(unsigned cnt, unsigned deg)
 {
@@ -634,11 +644,13 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
+        const bool first = cs == rs;
         if (tid == 0) {
             s.out_count = 0;
             s.wl_count = 0;
         }
         __syncthreads();  // the counters are reset before any warp appends
+        if (first) stamp(p, pass, 0);
         // ---- own visited words (the snapshot is read coherently: ld.cg) ----------
         unsigned word[PER];
 #pragma unroll
@@ -658,6 +670,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                 r1[t] = ld_ro(p.row_offsets + v + 1);
             }
         }
+        stamp_synced(p, pass, 1, first);
         // ---- first K neighbours of every candidate -----------------------------------
         int parent[PER];
         {
@@ -691,11 +704,13 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                     if (nb[t][k] >= 0 && ((w[t][k] >> (nb[t][k] & 31)) & 1u)) parent[t] = nb[t][k];
             }
         }
+        stamp_synced(p, pass, 2, first);
         // ---- continue the scan for candidates still without a parent ---------------
         if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
             bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
         else
             bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
+        stamp_synced(p, pass, 3, first);
         // ---- label, mark and append the discoveries --------------------------------
 #pragma unroll
         for (int t = 0; t < PER; t++) {
@@ -723,9 +738,11 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             }
         }
         __syncthreads();
+        if (first) stamp(p, pass, 4);
         emit_frontier<B>(p, s, pass, vout, qe_out);
         if (p.ul[0]) write_unvisited<B>(p, s, p.ul[0], &p.st->ul_count[(pass + 1) % 3]);
         __syncthreads();
+        if (first) stamp(p, pass, 5);
     }
 }
 
