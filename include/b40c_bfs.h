@@ -83,7 +83,7 @@ typedef struct b40c_bfs_policy {
     int32_t warp_cull;             /* 1: drop duplicate neighbours within a warp before the bitmask test,
                                       -1: do not (default) */
     int32_t bitmask_precheck;      /* 1: read the visited word before the atomic test-and-set (default),
-                                      -1: go straight to the atomic */
+                                      -1: go straight to the atomic (default of direction-optimizing) */
     int32_t queue_allocation;      /* frontier-slot allocation per tile of output: 1 = decoupled look-back
                                       over tile ids, 2 = one packed 64-bit atomicAdd; 0 = default */
     int32_t bottom_up_alpha;       /* direction-optimizing: go bottom-up when frontier edges exceed
@@ -103,7 +103,8 @@ typedef struct b40c_bfs_policy {
                                       1 = on (default), -1 = off */
     int32_t bottom_up_list;        /* distance searches: the first bottom-up level lists the vertices it
                                       left unvisited and later bottom-up levels scan only that list
-                                      (testing neighbours on the labels): 1 = on, -1 = off (default) */
+                                      (testing neighbours on the labels): 1 = on (default of
+                                      direction-optimizing), -1 = off */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
