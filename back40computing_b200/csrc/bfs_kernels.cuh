@@ -141,7 +141,7 @@ __device__ __forceinline__ bool warp_cull(bool valid, int v)
 // output (s.out = vertex, s.colstart = row start, s.rel = degree; the run
 // tables are consumed by then).  All threads of the CTA call it with
 // CTA-uniform `active`.
-template <int B, bool PRED, int U>
+template <int B, bool PRED, int U, bool LISTS = false>
 __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B, PRED> &s, const int (&v)[U],
                                                const int (&u)[U], const bool (&valid)[U], const bool (&active)[U],
                                                int label_value)
@@ -153,10 +153,10 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
         go[t] = valid[t];
         if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
         word[t] = 0;
-        if (go[t] && p.precheck && s.ul_in < 0) word[t] = ld_mask(s.mask + (v[t] >> 5));
+        if (go[t] && p.precheck && !(LISTS && s.ul_in >= 0)) word[t] = ld_mask(s.mask + (v[t] >> 5));
     }
     bool found[U];
-    if (s.ul_in >= 0) {
+    if (LISTS && s.ul_in >= 0) {
         // after a bottom-up list-mode level the visited mask is not kept: the
         // labels decide (a distance search's unreached vertices hold -1)
 #pragma unroll
@@ -341,7 +341,7 @@ __device__ __forceinline__ void cta_range(int n, int part, int parts, int &rs, i
 //   FUSED_CULL = false : two-phase expand: neighbours are written to the edge
 //                        frontier at their flattened edge position.
 // ------------------------------------------------------------------------------------
-template <int B, bool PRED, bool FUSED_CULL>
+template <int B, bool PRED, bool FUSED_CULL, bool LISTS = false>
 __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
                                              int level, int pass, const VertexFrontier &vout,
                                              const EdgeFrontier &eout, unsigned long long *qe_out,
@@ -471,7 +471,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         }
         __syncthreads();  // run tables consumed: they now collect the sub-round's output
         if (first) stamp(p, pass, 3);
-        discover_batch<B, PRED, PER>(p, s, v, u, valid, active, level + 1);
+        discover_batch<B, PRED, PER, LISTS>(p, s, v, u, valid, active, level + 1);
         __syncthreads();
         if (first) stamp(p, pass, 4);
         emit_frontier<B>(p, s, pass, vout, qe_out);
@@ -632,7 +632,7 @@ __device__ __forceinline__ void write_unvisited(const BfsParams &p, Smem &s, int
         if (base + j < p.nodes) list[base + j] = s.stage[j];
 }
 
-template <int B, bool PRED>
+template <int B, bool PRED, bool LISTS>
 __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
                                                 const VertexFrontier &vout, unsigned long long *qe_out)
 {
@@ -720,7 +720,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             const bool found = parent[t] >= 0;
             const unsigned fb = __ballot_sync(0xffffffffu, found);
             if (lane == 0) mask_out[vb >> 5] = word[t] | fb;  // this warp owns the whole word
-            if (p.ul[0]) append_unvisited(s, todo[t] && !found, v);
+            if (LISTS && p.ul[0]) append_unvisited(s, todo[t] && !found, v);
             if (fb == 0) continue;
             if (found) {
                 p.labels[v] = PRED ? parent[t] : level + 1;
@@ -740,7 +740,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         __syncthreads();
         if (first) stamp(p, pass, 4);
         emit_frontier<B>(p, s, pass, vout, qe_out);
-        if (p.ul[0]) write_unvisited<B>(p, s, p.ul[0], &p.st->ul_count[(pass + 1) % 3]);
+        if (LISTS && p.ul[0]) write_unvisited<B>(p, s, p.ul[0], &p.st->ul_count[(pass + 1) % 3]);
         __syncthreads();
         if (first) stamp(p, pass, 5);
     }
@@ -1006,7 +1006,7 @@ constexpr int kSoloLevelCap = 4096;  // small levels CTA 0 runs alone before the
 // persistent launch, a run of levels whose frontiers have at most
 // p.small_edges edges is processed by CTA 0 alone, separated by CTA-level
 // barriers only, while the other CTAs wait at the grid barrier.
-template <int B, bool PRED>
+template <int B, bool PRED, bool LISTS>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1035,8 +1035,8 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             if (blockIdx.x == 0) {
                 for (int solo = 0;; solo++) {
                     if (tid == 0) record_direction(p, s.visited_edges, pass, false, s.mask, s.ul_in, s.ul_n);
-                    expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
-                                                &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
+                    expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1],
+                                                       p.ef[0], &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
                     __syncthreads();
                     if (s.flag) max_level_seen = level + 1;
                     level++;
@@ -1063,13 +1063,13 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
         if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n);
-        if (bu && s.ul_in >= 0)
+        if (LISTS && bu && s.ul_in >= 0)
             bottom_up_list<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         else if (bu)
-            bottom_up_range<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+            bottom_up_range<B, PRED, LISTS>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         else
-            expand_range<B, PRED, true>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
-                                        &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);
+            expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
+                                               &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);
         __syncthreads();
         worked = true;
         if (s.flag) max_level_seen = level + 1;

@@ -67,7 +67,7 @@ static int set_up(int device, DeviceSetup **out)
             cudaGetLastError();
             return b40c::fail((int)e, "cudaGetSymbolAddress of the search scratch failed: %s", cudaGetErrorString(e));
         }
-        const void *kern = (const void *)dev::ec_kernel<kThreads, false>;
+        const void *kern = (const void *)dev::ec_kernel<kThreads, false, false>;
         const size_t smem = sizeof(dev::ExpandSmem<kThreads, false>);
         e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         int per_sm = 0, sms = 0;
@@ -170,7 +170,7 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
     }
     if (e == cudaSuccess) {
         void *args[] = {&k};
-        e = cudaLaunchCooperativeKernel((const void *)dev::ec_kernel<kThreads, false>, dim3(d->grid), dim3(kThreads),
+        e = cudaLaunchCooperativeKernel((const void *)dev::ec_kernel<kThreads, false, false>, dim3(d->grid), dim3(kThreads),
                                         args, sizeof(dev::ExpandSmem<kThreads, false>), stream);
     }
     // wait for the search and read its error word into a local variable

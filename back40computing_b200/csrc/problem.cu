@@ -156,10 +156,12 @@ b40c_bfs_policy default_policy(int strategy)
     pol.bottom_up_list = -1;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     if (strategy == B40C_DIRECTION_OPTIMIZING) {
-        // measured on B200 over 16 sources: R-MAT 22 249 -> 236 us with the
-        // unvisited list, random 2^21 204 -> 200 us; without the visited-word
-        // pre-check a further few percent on both
-        pol.bottom_up_list = 1;
+        // measured on B200 over 16 sources: the kernel variant carrying the
+        // unvisited lists is slower overall (R-MAT 22 241 vs 222 us, random
+        // 2^21 203 vs 172 us: its first bottom-up level loses more than the
+        // later ones gain), so lists stay off; the visited-word pre-check
+        // makes no difference here
+        pol.bottom_up_list = -1;
         pol.bitmask_precheck = -1;
     }
     return pol;

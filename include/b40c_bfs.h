@@ -103,8 +103,9 @@ typedef struct b40c_bfs_policy {
                                       1 = on (default), -1 = off */
     int32_t bottom_up_list;        /* distance searches: the first bottom-up level lists the vertices it
                                       left unvisited and later bottom-up levels scan only that list
-                                      (testing neighbours on the labels): 1 = on (default of
-                                      direction-optimizing), -1 = off */
+                                      (testing neighbours on the labels; a kernel variant of its own):
+                                      1 = on, -1 = off (default: measured slower overall on R-MAT and
+                                      uniform graphs) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
