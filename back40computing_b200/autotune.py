@@ -36,7 +36,7 @@ SEARCH_SPACE = {
     "chunk_edges": [512, 1024, 2048],
     "warp_gather_threshold": [32, 64, 128],
     "cta_gather_threshold": [256, 512, 1024],
-    "small_frontier_edges": [256, 1024, 4096, 16384],
+    "small_frontier_edges": [256, 1024, 2048, 4096, 16384],
     "bottom_up_alpha": [6, 14, 24, 48],
     "bottom_up_beta": [12, 24, 48],
     "bitmask_precheck": [1, -1],

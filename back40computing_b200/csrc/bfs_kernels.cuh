@@ -64,6 +64,7 @@ struct ExpandSmem {
     int32_t ul_in;                     // bottom-up list mode: buffer holding this pass's unvisited list, or -1
     int32_t ul_n;                      // entries of that list
     int32_t ul_base;                   // where this chunk's still-unvisited vertices go in the next list
+    int32_t solo_stop;                 // the solo phase writes its frontier out (CTA-uniform decision)
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -144,16 +145,17 @@ __device__ __forceinline__ bool warp_cull(bool valid, int v)
 template <int B, bool PRED, int U, bool LISTS = false>
 __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B, PRED> &s, const int (&v)[U],
                                                const int (&u)[U], const bool (&valid)[U], const bool (&active)[U],
-                                               int label_value)
+                                               int label_value, bool precheck = true)
 {
     bool go[U];
     unsigned word[U];
+    precheck = precheck && p.precheck && !(LISTS && s.ul_in >= 0);
 #pragma unroll
     for (int t = 0; t < U; t++) {
         go[t] = valid[t];
         if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
         word[t] = 0;
-        if (go[t] && p.precheck && !(LISTS && s.ul_in >= 0)) word[t] = ld_mask(s.mask + (v[t] >> 5));
+        if (go[t] && precheck) word[t] = ld_mask(s.mask + (v[t] >> 5));
     }
     bool found[U];
     if (LISTS && s.ul_in >= 0) {
@@ -345,7 +347,7 @@ template <int B, bool PRED, bool FUSED_CULL, bool LISTS = false>
 __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
                                              int level, int pass, const VertexFrontier &vout,
                                              const EdgeFrontier &eout, unsigned long long *qe_out,
-                                             unsigned &bar_phase, int part, int parts)
+                                             unsigned &bar_phase, int part, int parts, bool defer_emit = false)
 {
     const int tid = threadIdx.x;
     const int q = s.q, E = s.E;
@@ -474,10 +476,68 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         discover_batch<B, PRED, PER, LISTS>(p, s, v, u, valid, active, level + 1);
         __syncthreads();
         if (first) stamp(p, pass, 4);
+        if (defer_emit) return;  // single sub-round (the caller checked): the output stays in s.out / colstart / rel
         emit_frontier<B>(p, s, pass, vout, qe_out);
         __syncthreads();
         if (first) stamp(p, pass, 5);
     }
+}
+
+// Solo levels (CTA 0 alone, one sub-round each) can pass their frontier from
+// one level to the next in shared memory.  A level's discoveries sit in
+// s.out / colstart / rel (n entries: vertex, row start, degree); the next
+// level turns them in place into its run tables (rel = degree prefix with
+// rel[n] = E, colstart = row start, vert = vertex) and runs from there, with
+// no frontier, counter or chunk-index traffic.  solo_level_smem runs such a
+// level: owner map, gather, discovery (atomic test-and-set without the
+// visited-word pre-check), output back in s.out / colstart / rel.
+template <int B, bool PRED, bool LISTS>
+__device__ __forceinline__ void solo_level_smem(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int n, int E)
+{
+    const int tid = threadIdx.x;
+    constexpr int PER = kChunkMax / B;
+    {
+        const int x0 = tid * PER;
+        if (x0 < E) {
+            int lo = 0, hi = n - 1;  // last j with rel[j] <= x0
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s.rel[mid] <= x0) lo = mid; else hi = mid - 1;
+            }
+            int j = lo;
+            int next = s.rel[j + 1];
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                const int x = x0 + t;
+                if (x < E) {
+                    while (x >= next) {
+                        j++;
+                        next = s.rel[j + 1];
+                    }
+                    s.own[x] = (uint16_t)j;
+                }
+            }
+        }
+    }
+    __syncthreads();
+    int v[PER], u[PER];
+    bool valid[PER], active[PER];
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const int x = t * B + tid;
+        active[t] = t * B < E;
+        valid[t] = x < E;
+        v[t] = -1;
+        u[t] = -1;
+        if (valid[t]) {
+            const int j = s.own[x];
+            v[t] = ld_stream(p.column_indices + s.colstart[j] + (x - s.rel[j]));
+            if (PRED) u[t] = s.vert[j];
+        }
+    }
+    __syncthreads();  // run tables consumed: they now collect the level's output
+    discover_batch<B, PRED, PER, LISTS>(p, s, v, u, valid, active, level + 1, false);
+    __syncthreads();
 }
 
 // Contraction of the CTA's range of an edge frontier (q items), in sub-rounds
@@ -1005,7 +1065,8 @@ constexpr int kSoloLevelCap = 4096;  // small levels CTA 0 runs alone before the
 // direction_opt, levels with a large frontier run bottom-up.  In a
 // persistent launch, a run of levels whose frontiers have at most
 // p.small_edges edges is processed by CTA 0 alone, separated by CTA-level
-// barriers only, while the other CTAs wait at the grid barrier.
+// barriers only, while the other CTAs wait at the grid barrier; while those
+// levels fit one sub-round their frontier stays in shared memory.
 template <int B, bool PRED, bool LISTS>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
@@ -1033,14 +1094,83 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         if (p.persistent && s.E <= p.small_edges) {
             // ---- small frontiers: CTA 0 alone, level after level ----------------------
             if (blockIdx.x == 0) {
+                int smem_n = -1;  // >= 0: this level's frontier is the run tables in shared memory (entries)
                 for (int solo = 0;; solo++) {
                     if (tid == 0) record_direction(p, s.visited_edges, pass, false, s.mask, s.ul_in, s.ul_n);
-                    expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1],
-                                                       p.ef[0], &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1);
+                    const bool one_round = s.E > 0 && s.E <= kChunkMax;  // CTA-uniform
+                    if (smem_n >= 0)
+                        solo_level_smem<B, PRED, LISTS>(p, s, level, smem_n, s.E);
+                    else
+                        expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass,
+                                                           p.vf[(level + 1) & 1], p.ef[0],
+                                                           &p.st->qe[(pass + 1) % 3], bar_phase, 0, 1, one_round);
                     __syncthreads();
                     if (s.flag) max_level_seen = level + 1;
                     level++;
                     pass = level;
+                    if (one_round) {
+                        // the discoveries are still in s.out / colstart / rel: stay in
+                        // shared memory while the next level is one sub-round too
+                        constexpr int PER = kChunkMax / B;
+                        const int n = s.out_count;
+                        int deg[PER];
+                        unsigned long long sum = 0;
+#pragma unroll
+                        for (int k = 0; k < PER; k++) {
+                            const int j = tid * PER + k;
+                            deg[k] = j < n ? s.rel[j] : 0;
+                            sum += (unsigned long long)deg[k];
+                        }
+                        unsigned long long En;
+                        unsigned long long run = cta_exclusive_scan<B>(sum, s.scan_warp, &En);
+                        // (a frontier larger than the queue goes out too, so the overflow is reported)
+                        if (tid == 0)
+                            s.solo_stop = n == 0 || n > p.vcap ||
+                                          En > (unsigned long long)min(p.small_edges, kChunkMax) ||
+                                          (dl >= 0 && level >= dl) || solo + 1 >= kSoloLevelCap ||
+                                          ld_cg(&p.st->error) != 0;
+                        __syncthreads();
+                        if (!s.solo_stop) {
+#pragma unroll
+                            for (int k = 0; k < PER; k++) {
+                                const int j = tid * PER + k;
+                                if (j < n) {
+                                    s.rel[j] = (int)run;
+                                    if (PRED) s.vert[j] = s.out[j];
+                                }
+                                run += (unsigned long long)deg[k];
+                            }
+                            if (tid == 0) {
+                                // begin_pass without the frontier counters
+                                s.rel[n] = (int)En;
+                                s.q = n;
+                                s.E = (int)En;
+                                s.flag = 0;
+                                s.out_count = 0;
+                                s.visited_edges += En;
+                                p.st->qe[(pass + 2) % 3] = 0;
+                                p.st->tile_ctr[(pass + 1) % 3] = 0;
+                                atomicAdd(&p.st->total_queued, (unsigned long long)n);
+                                if (p.ul[0]) p.st->ul_count[(pass + 2) % 3] = 0;
+                                if (p.levels && pass < kMaxLevelRecords) {
+                                    LevelRecord r;
+                                    r.vertices = n;
+                                    r.edges = (int)En;
+                                    r.bottom_up = 0;
+                                    r.pass = pass;
+                                    r.t_ns = globaltimer_ns();
+                                    p.levels[pass] = r;
+                                }
+                            }
+                            smem_n = n;
+                            __syncthreads();
+                            continue;
+                        }
+                        // leaving shared memory: the discoveries become the frontier of `pass`
+                        emit_frontier<B>(p, s, pass - 1, p.vf[level & 1], &p.st->qe[pass % 3]);
+                        __syncthreads();
+                        smem_n = -1;
+                    }
                     if (tid == 0) {
                         const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
                         s.q = qe_count(x);
