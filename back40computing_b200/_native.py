@@ -46,6 +46,7 @@ class Policy(C.Structure):
         ("bottom_up_scan", C.c_int32),
         ("bottom_up_hub_probes", C.c_int32),
         ("bottom_up_list", C.c_int32),
+        ("bottom_up_defer_frontier", C.c_int32),
     ]
 
 

@@ -8,7 +8,10 @@ search on the target GPU, cached per graph class in ``tuned_policies.json``
 next to this file and looked up at run time by :func:`policy_for`.
 
 Graph classes (from the degree distribution, :func:`classify`):
-  * ``lattice``    -- bounded degree, high diameter (grid2d / grid3d);
+  * ``lattice-narrow`` -- bounded degree, high diameter, levels of at most a few
+    thousand vertices (grid2d, small grid3d): most levels fit one CTA;
+  * ``lattice-wide``   -- bounded degree, levels of tens of thousands of vertices
+    and more (large grid3d): every level wants the whole grid;
   * ``power-law``  -- heavy-tailed degrees (R-MAT);
   * ``uniform``    -- concentrated degrees, low diameter (random / regular-ish).
 
@@ -27,7 +30,10 @@ import numpy as np
 from . import _native as N
 
 CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned_policies.json")
-CLASSES = ("lattice", "power-law", "uniform")
+CLASSES = ("lattice-narrow", "lattice-wide", "power-law", "uniform")
+# a lattice whose estimated level width (vertices^((d-1)/d), d from the mean
+# degree) is at most this is narrow
+NARROW_WIDTH = 4096
 KINDS = ("direction-optimizing", "expand-contract", "batched")
 
 # knob -> values tried (0 = the library default)
@@ -62,7 +68,11 @@ def classify(graph) -> str:
     cv = float(nz.std() / mean)
     mx = int(nz.max())
     if mx <= 8 and cv < 0.35:
-        return "lattice"
+        # a d-dimensional mesh has about 2d edges per vertex (plus a self-loop
+        # in the reference builders) and levels of about n^((d-1)/d) vertices
+        dim = max(1, int(mean / 2 + 0.25))
+        width = float(nz.size) ** ((dim - 1) / dim)
+        return "lattice-narrow" if width <= NARROW_WIDTH else "lattice-wide"
     if cv > 1.0 or mx > 32 * mean:
         return "power-law"
     return "uniform"
@@ -97,10 +107,13 @@ def _representatives(quick: bool):
     from .graph import CsrGraph, BuildGrid2dGraph, BuildGrid3dGraph, BuildRmatGraph, BuildRandomRegularishGraph
     reps = {}
     g = CsrGraph()
-    BuildGrid3dGraph(64 if quick else 128, g)
+    BuildGrid2dGraph(256 if quick else 1000, g)
     g2 = CsrGraph()
-    BuildGrid2dGraph(256 if quick else 512, g2)
-    reps["lattice"] = [("grid3d", g), ("grid2d", g2)]
+    BuildGrid3dGraph(32 if quick else 64, g2)
+    reps["lattice-narrow"] = [("grid2d", g), ("grid3d-narrow", g2)]
+    g = CsrGraph()
+    BuildGrid3dGraph(100 if quick else 200, g)
+    reps["lattice-wide"] = [("grid3d", g)]
     g = CsrGraph()
     s = 16 if quick else 20
     BuildRmatGraph(1 << s, 16 << s, g, True, 0.57, 0.19, 0.19, seed=1, permute=True)

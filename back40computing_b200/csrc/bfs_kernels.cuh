@@ -65,6 +65,7 @@ struct ExpandSmem {
     int32_t ul_n;                      // entries of that list
     int32_t ul_base;                   // where this chunk's still-unvisited vertices go in the next list
     int32_t solo_stop;                 // the solo phase writes its frontier out (CTA-uniform decision)
+    uint32_t win_word[B];              // bottom-up windows: the window's visited words, discoveries OR'ed in
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
 };
@@ -211,12 +212,13 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
 // offset inside the tile; the tile's base comes from a decoupled look-back
 // over tile ids (taken once the tile's aggregate is known, so no tile ever
 // waits for another tile's gather) or, with alloc_lookback = 0, from one
-// packed 64-bit atomicAdd on the pass's output counter.  Each entry gets its
-// slot, its degree prefix P and its kChunkGrain boundaries in vout.cf.  The
-// pass total accumulates in *qe_out.  All threads must call it.
+// packed 64-bit atomicAdd on the pass's output counter (always with
+// lookback = false).  Each entry gets its slot, its degree prefix P and its
+// kChunkGrain boundaries in vout.cf.  The pass total accumulates in *qe_out.
+// All threads must call it.
 template <int B, typename Smem>
 __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int pass, const VertexFrontier &vout,
-                                              unsigned long long *qe_out)
+                                              unsigned long long *qe_out, bool lookback = true)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cnt = s.out_count;
@@ -232,7 +234,7 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
     if (tot == 0) return;  // CTA-uniform: nothing to allocate
     if (warp == 0) {
         unsigned long long prefix = 0;
-        if (!p.alloc_lookback) {
+        if (!p.alloc_lookback || !lookback) {
             if (lane == 0) prefix = atomicAdd(qe_out, tot);
         } else {
             const unsigned long long epoch = p.st->epoch + (unsigned long long)pass;
@@ -692,9 +694,14 @@ __device__ __forceinline__ void write_unvisited(const BfsParams &p, Smem &s, int
         if (base + j < p.nodes) list[base + j] = s.stage[j];
 }
 
+//
+// With `defer` (CTA-uniform) the discoveries are only counted: each thread
+// sums (1 << 32 | degree) over its discoveries and the CTA adds its total to
+// *qe_out once; materialize_frontier builds the vertex frontier from the two
+// mask buffers if a top-down level follows.
 template <int B, bool PRED, bool LISTS>
 __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
-                                                const VertexFrontier &vout, unsigned long long *qe_out)
+                                                const VertexFrontier &vout, unsigned long long *qe_out, bool defer)
 {
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr int PER = kChunkMax / B;
@@ -703,6 +710,7 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     uint32_t *mask_out = (s.mask == p.mask) ? p.mask_alt : p.mask;
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
+    unsigned long long found_acc = 0;  // defer: this thread's (count << 32 | degree) of discoveries
     for (int cs = rs; cs < re; cs += kChunkMax) {
         const bool first = cs == rs;
         if (tid == 0) {
@@ -786,6 +794,10 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                 p.labels[v] = PRED ? parent[t] : level + 1;
                 s.flag = 1;
             }
+            if (defer) {
+                if (found) found_acc += pack(1u, (unsigned)(r1[t] - r0[t]));
+                continue;
+            }
             const int leader = __ffs(fb) - 1;
             int base = 0;
             if (lane == leader) base = atomicAdd(&s.out_count, __popc(fb));
@@ -797,12 +809,230 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
                 s.rel[slot] = r1[t] - r0[t];
             }
         }
+        if (defer) {
+            if (first) stamp(p, pass, 4);
+            continue;
+        }
         __syncthreads();
         if (first) stamp(p, pass, 4);
         emit_frontier<B>(p, s, pass, vout, qe_out);
         if (LISTS && p.ul[0]) write_unvisited<B>(p, s, p.ul[0], &p.st->ul_count[(pass + 1) % 3]);
         __syncthreads();
         if (first) stamp(p, pass, 5);
+    }
+    if (defer) {
+        unsigned long long tot;
+        cta_exclusive_scan<B>(found_acc, s.scan_warp, &tot);
+        if (tid == 0 && tot != 0) atomicAdd(qe_out, tot);
+    }
+}
+
+// Writes the vertex ids of the set bits of `bits` (the word of vertices
+// v0..v0+31) whose positions, counted from `pos` in bit order, fall in
+// [lo, lo + n), to list[position - lo].
+__device__ __forceinline__ void scatter_bits(unsigned bits, int v0, int pos, int lo, int n, int32_t *list)
+{
+    const int c = __popc(bits);
+    int k = min(c, max(0, lo - pos));
+    const int k1 = min(c, lo + n - pos);
+    if (k >= k1) return;
+    for (int i = 0; i < k; i++) bits &= bits - 1;
+    for (; k < k1; k++) {
+        list[pos + k - lo] = v0 + __ffs(bits) - 1;
+        bits &= bits - 1;
+    }
+}
+
+// Level `level` bottom-up over the CTA's range of vertex ids, in windows of
+// 32 * B ids (one visited word per thread).  The window's unvisited vertices
+// (clear bits of the level-start snapshot) are numbered by a CTA scan and
+// handled in batches of up to kChunkMax from a shared-memory list, so only
+// unvisited vertices take lanes and a mostly visited window costs one batch.
+// A batch: rows and hub pairs (independent loads, issued together), the
+// pair's probes, the per-lane (per-warp for long lists) scan of the rest,
+// then labels; a discovery sets its bit in the window's shared copy of the
+// words (s.win_word), written whole to the other mask buffer when the window
+// ends.  With `defer` (CTA-uniform) discoveries are only counted (one packed
+// atomic per CTA; materialize_frontier builds the frontier when a top-down
+// level follows), else each batch's discoveries are emitted.
+template <int B, bool PRED>
+__device__ __forceinline__ void bottom_up_windows(const BfsParams &p, ExpandSmem<B, PRED> &s, int level, int pass,
+                                                  const VertexFrontier &vout, unsigned long long *qe_out, bool defer)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    constexpr int PER = kChunkMax / B;
+    constexpr int K = kBottomUpProbe;
+    static_assert(K == 2, "the hub pair supplies two probes");
+    const uint32_t *mask = s.mask;
+    uint32_t *mask_out = (s.mask == p.mask) ? p.mask_alt : p.mask;
+    int rs, re;
+    cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);  // rs is a multiple of kChunkGrain (so of 32)
+    unsigned long long found_acc = 0;  // defer: this thread's (count << 32 | degree) of discoveries
+    bool first = true;
+    for (int wb = rs; wb < re; wb += 32 * B) {
+        const int v0 = wb + 32 * tid;  // first vertex of this thread's word
+        unsigned w = 0xffffffffu;
+        if (v0 < re) w = ld_cg(mask + (v0 >> 5));
+        unsigned unv = v0 < re ? ~w : 0u;
+        if (v0 < re && re - v0 < 32) unv &= (1u << (re - v0)) - 1u;
+        s.win_word[tid] = w;
+        unsigned long long total;
+        const int pos = (int)cta_exclusive_scan<B>((unsigned long long)__popc(unv), s.scan_warp, &total);
+        const int U = (int)total;  // the scan's closing barrier also publishes win_word
+        for (int lo = 0; lo < U; lo += kChunkMax) {
+            const int n = min(U - lo, kChunkMax);
+            if (tid == 0) s.out_count = 0;
+            scatter_bits(unv, v0, pos, lo, n, s.stage);
+            __syncthreads();
+            if (first) stamp(p, pass, 0);
+            int r0[PER], r1[PER], parent[PER];
+            bool todo[PER];
+            int nb[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                const int j = t * B + tid;
+                todo[t] = j < n;
+                r0[t] = r1[t] = 0;
+                nb[t][0] = nb[t][1] = -1;
+                if (todo[t]) {
+                    const int v = s.stage[j];  // read again at the end (not kept in registers)
+                    r0[t] = ld_ro(p.row_offsets + v);
+                    r1[t] = ld_ro(p.row_offsets + v + 1);
+                    if (p.hub2) {
+                        // the vertex's two highest-degree neighbours (one 8-byte load)
+                        const int2 h = p.hub2[v];
+                        nb[t][0] = h.x;
+                        nb[t][1] = h.y;
+                    }
+                }
+            }
+            stamp_synced(p, pass, 1, first);
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                todo[t] = todo[t] && r1[t] > r0[t];
+                if (!p.hub2) {
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+                } else if (!todo[t]) {
+                    nb[t][0] = nb[t][1] = -1;
+                }
+            }
+            {
+                unsigned pw[PER][K];
+#pragma unroll
+                for (int t = 0; t < PER; t++)
+#pragma unroll
+                    for (int k = 0; k < K; k++) pw[t][k] = nb[t][k] >= 0 ? ld_mask(mask + (nb[t][k] >> 5)) : 0u;
+#pragma unroll
+                for (int t = 0; t < PER; t++) {
+                    parent[t] = -1;
+#pragma unroll
+                    for (int k = K - 1; k >= 0; k--)
+                        if (nb[t][k] >= 0 && ((pw[t][k] >> (nb[t][k] & 31)) & 1u)) parent[t] = nb[t][k];
+                }
+            }
+            stamp_synced(p, pass, 2, first);
+            if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
+                bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
+            else
+                bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
+            stamp_synced(p, pass, 3, first);
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                if (t * B >= n) break;  // CTA-uniform
+                const bool found = todo[t] && parent[t] >= 0;
+                const int v = found ? s.stage[t * B + tid] : 0;
+                {
+                    // the list is sorted, so a warp's discoveries share few words: one
+                    // shared atomic per word, with the bits OR-reduced over its lanes
+                    const int wi = (v - wb) >> 5;
+                    const unsigned grp = __match_any_sync(0xffffffffu, found ? wi : -1 - lane);
+                    const unsigned bits = __reduce_or_sync(grp, found ? 1u << (v & 31) : 0u);
+                    if (found && lane == __ffs(grp) - 1) atomicOr(&s.win_word[wi], bits);
+                }
+                if (found) {
+                    p.labels[v] = PRED ? parent[t] : level + 1;
+                    s.flag = 1;
+                }
+                if (defer) {
+                    if (found) found_acc += pack(1u, (unsigned)(r1[t] - r0[t]));
+                    continue;
+                }
+                const unsigned fb = __ballot_sync(0xffffffffu, found);
+                if (fb == 0) continue;
+                const int leader = __ffs(fb) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(&s.out_count, __popc(fb));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (found) {
+                    const int slot = base + __popc(fb & lanemask_lt());
+                    s.out[slot] = v;
+                    s.colstart[slot] = r0[t];
+                    s.rel[slot] = r1[t] - r0[t];
+                }
+            }
+            __syncthreads();  // the list is consumed; the batch's output and bits are complete
+            if (first) stamp(p, pass, 4);
+            if (!defer) {
+                emit_frontier<B>(p, s, pass, vout, qe_out);
+                __syncthreads();
+            }
+            if (first) stamp(p, pass, 5);
+            first = false;
+        }
+        if (v0 < re) mask_out[v0 >> 5] = s.win_word[tid];  // every word of the range, old bits | discoveries
+    }
+    if (defer) {
+        unsigned long long tot;
+        cta_exclusive_scan<B>(found_acc, s.scan_warp, &tot);
+        if (tid == 0 && tot != 0) atomicAdd(qe_out, tot);
+    }
+}
+
+// The vertex frontier of a bottom-up level that only counted its
+// discoveries: the vertices set in this pass's mask buffer and clear in the
+// other one (that level's input), emitted into `vout` like any level output,
+// slots from one packed atomic per batch on st->mat_ctr.  Every CTA takes its
+// range of vertex ids in windows of 32 * B (one word pair per thread); all
+// threads call it.
+template <int B, bool PRED>
+__device__ __forceinline__ void materialize_frontier(const BfsParams &p, ExpandSmem<B, PRED> &s,
+                                                     const VertexFrontier &vout)
+{
+    const int tid = threadIdx.x;
+    constexpr int PER = kChunkMax / B;
+    const uint32_t *cur = s.mask;
+    const uint32_t *prev = (s.mask == p.mask) ? p.mask_alt : p.mask;
+    int rs, re;
+    cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
+    for (int wb = rs; wb < re; wb += 32 * B) {
+        const int v0 = wb + 32 * tid;
+        unsigned fresh = 0u;
+        if (v0 < re) fresh = ld_cg(cur + (v0 >> 5)) & ~ld_cg(prev + (v0 >> 5));
+        if (v0 < re && re - v0 < 32) fresh &= (1u << (re - v0)) - 1u;
+        unsigned long long total;
+        const int pos = (int)cta_exclusive_scan<B>((unsigned long long)__popc(fresh), s.scan_warp, &total);
+        const int U = (int)total;
+        for (int lo = 0; lo < U; lo += kChunkMax) {
+            const int n = min(U - lo, kChunkMax);
+            scatter_bits(fresh, v0, pos, lo, n, s.out);
+            __syncthreads();
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                const int j = t * B + tid;
+                if (j < n) {
+                    const int v = s.out[j];
+                    const int a = ld_ro(p.row_offsets + v), b = ld_ro(p.row_offsets + v + 1);
+                    s.colstart[j] = a;
+                    s.rel[j] = b - a;  // > 0: a bottom-up level only discovers vertices with edges
+                }
+            }
+            if (tid == 0) s.out_count = n;
+            __syncthreads();
+            emit_frontier<B>(p, s, 0, vout, &p.st->mat_ctr, false);
+            __syncthreads();
+        }
     }
 }
 
@@ -1045,10 +1275,12 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
 // whether the level ran bottom-up and which mask buffer the next pass reads
 // (a bottom-up level writes the other one).
 __device__ __forceinline__ void record_direction(const BfsParams &p, unsigned long long visited_edges, int pass,
-                                                 bool bu, const uint32_t *pass_mask, int ul_in, int ul_n)
+                                                 bool bu, const uint32_t *pass_mask, int ul_in, int ul_n,
+                                                 bool deferred = false)
 {
     p.st->visited_edges[(pass + 1) % 3] = visited_edges;
-    p.st->dir[(pass + 1) % 3] = bu ? 1 : 0;
+    p.st->dir[(pass + 1) % 3] = bu ? (deferred ? 2 : 1) : 0;
+    if (deferred) p.st->mat_ctr = 0;
     p.st->mask_sel[(pass + 1) % 3] = (pass_mask == p.mask) == bu ? 1 : 0;
     if (p.ul[0]) {
         // a bottom-up level writes the next list (range mode into buffer 0,
@@ -1090,6 +1322,15 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         if (dl >= 0 && level >= dl) {
             limit_hit = true;
             break;
+        }
+        if (s.prev_bu == 2 &&
+            ((p.persistent && s.E <= p.small_edges) || !choose_bottom_up(p, true, s.q, s.E, s.visited_edges))) {
+            // the previous level ran bottom-up and only counted its discoveries:
+            // this top-down level (or solo phase) reads them as a vertex frontier
+            materialize_frontier<B, PRED>(p, s, p.vf[level & 1]);
+            if (!duty.barrier(p.st, generation, &s_ok)) break;
+            if (tid == 0 && ld_cg64(&p.st->mat_ctr) != ld_cg64(&p.st->qe[pass % 3]))
+                atomicOr(&p.st->error, kErrFrontier);
         }
         if (p.persistent && s.E <= p.small_edges) {
             // ---- small frontiers: CTA 0 alone, level after level ----------------------
@@ -1192,11 +1433,19 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
-        if (tid == 0 && blockIdx.x == 0) record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n);
+        const bool defer = !LISTS && bu && p.bu_defer && p.persistent;
+        if (tid == 0 && blockIdx.x == 0)
+            record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n, defer);
         if (LISTS && bu && s.ul_in >= 0)
             bottom_up_list<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        else if (bu && (LISTS || s.prev_bu == 0))
+            // the first bottom-up level of a run: most vertices are unvisited, so the
+            // chunks of vertex ids are walked directly
+            bottom_up_range<B, PRED, LISTS>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3],
+                                            defer);
         else if (bu)
-            bottom_up_range<B, PRED, LISTS>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+            // later bottom-up levels: the unvisited vertices of each window, compacted
+            bottom_up_windows<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], defer);
         else
             expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
                                                &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);

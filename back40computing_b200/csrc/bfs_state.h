@@ -60,13 +60,16 @@ struct alignas(128) SearchState {
     int32_t depth_limit;       // < 0: unlimited
     // direction-optimizing bookkeeping, rotating like qe: pass k reads [k % 3]
     // and block 0 writes [(k + 1) % 3]
-    int32_t dir[3];            // 1: the previous level ran bottom-up
+    int32_t dir[3];            // 1: the previous level ran bottom-up, 2: bottom-up with its frontier deferred
     int32_t mask_sel[3];       // which visited-mask buffer holds the visited set (0: mask, 1: mask_alt)
     unsigned long long visited_edges[3];  // degree sum of the vertices visited before the pass
     // level at which a persistent launch resumes after a small-frontier phase of
     // CTA 0, by phase parity (a slot is rewritten only two phases later, after
     // every CTA has read it)
     int32_t solo_resume[2];
+    // slots of a deferred bottom-up frontier built at the start of the next
+    // level (count << 32 | edge total; cleared when the bottom-up level starts)
+    unsigned long long mat_ctr;
 };
 
 __host__ __device__ inline int qe_count(unsigned long long x) { return (int)(x >> 32); }
@@ -131,6 +134,8 @@ struct BfsParams {
     int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
     int32_t small_edges;      // persistent launches: frontiers with at most this many edges run on CTA 0 alone
     int32_t bu_scan;          // bottom-up continuation: 1 per lane, 2 per CTA (edge-parallel worklist)
+    int32_t bu_defer;         // persistent bottom-up levels count their discoveries; the frontier is built
+                              // from the mask buffers only when a top-down level follows
     const uint32_t *iso;      // bit v: v has no edges in or out; a search starts with these bits visited (null: none)
     const int2 *hub2;         // per vertex its two highest-degree neighbours, probed first bottom-up (null: off)
     int32_t *ul[2];           // unvisited-vertex lists of bottom-up list mode (null: off; distance mode only)

@@ -19,6 +19,7 @@ constexpr unsigned kErrLookback = 4u;       // look-back wait expired
 constexpr unsigned kErrBulk = 8u;           // bulk-copy wait expired
 constexpr unsigned kErrInjected = 16u;      // test-only: a CTA skipped its barrier arrival
 constexpr unsigned kErrLevels = 32u;        // more levels than vertices: a captured loop was stopped
+constexpr unsigned kErrFrontier = 64u;      // a deferred bottom-up frontier did not match its counted size
 constexpr unsigned kSpinLimit = 1u << 22;   // polls before a wait gives up (~1-2 s with backoff)
 
 // ---- loads / stores ----------------------------------------------------------

@@ -130,6 +130,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.mask_alt = p->d_next;
     k.small_edges = pol.small_frontier_edges;
     k.bu_scan = pol.bottom_up_scan;
+    k.bu_defer = pol.bottom_up_defer_frontier > 0 ? 1 : 0;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
     k.arrive = p->instrument ? p->d_arrive : nullptr;
@@ -154,6 +155,7 @@ b40c_bfs_policy default_policy(int strategy)
     pol.bottom_up_scan = 1;
     pol.bottom_up_hub_probes = 1;
     pol.bottom_up_list = -1;
+    pol.bottom_up_defer_frontier = 1;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     if (strategy == B40C_DIRECTION_OPTIMIZING) {
         // measured on B200 over 16 sources: the kernel variant carrying the
@@ -186,6 +188,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->bottom_up_scan) d.bottom_up_scan = in->bottom_up_scan;
         if (in->bottom_up_hub_probes) d.bottom_up_hub_probes = in->bottom_up_hub_probes > 0 ? 1 : -1;
         if (in->bottom_up_list) d.bottom_up_list = in->bottom_up_list > 0 ? 1 : -1;
+        if (in->bottom_up_defer_frontier) d.bottom_up_defer_frontier = in->bottom_up_defer_frontier > 0 ? 1 : -1;
     }
     if (d.threads != kThreads)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: %d)", d.threads, kThreads);
@@ -275,6 +278,8 @@ int check_state_errors(b40c_bfs_problem *p)
                           "Frontier queue overflow.  Please increase queue-sizing factor.");
     if (e & dev::kErrLevels)
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a replayed search ran more levels than the graph has vertices");
+    if (e & dev::kErrFrontier)
+        return b40c::fail(B40C_ERROR_INTERNAL, "a deferred bottom-up frontier did not match its counted size");
     if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk | dev::kErrInjected))
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a bounded device-side wait expired (error bits 0x%x)", e);
     return B40C_SUCCESS;

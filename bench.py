@@ -393,8 +393,8 @@ def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=
 
 def lattice_extra():
     """grid2d-1000 from the corner and grid3d-256 from the centre: the persistent grid,
-    the whole-search CUDA graph and per-level launches."""
-    from back40computing_b200 import CsrProblem
+    the whole-search CUDA graph and per-level launches (expand-contract, tuned policy)."""
+    from back40computing_b200 import CsrProblem, autotune
     from back40computing_b200 import _native as N
     from back40computing_b200.bfs import ENACTORS
     out = {}
@@ -402,7 +402,7 @@ def lattice_extra():
         g, srcs = build_graph(name)
         ec = int(g.edges)  # lattices are connected: every edge is reached
         p = CsrProblem.from_graph(g)
-        e = ENACTORS[0]()
+        e = ENACTORS[0](policy=autotune.policy_for(g, "expand-contract"))
         N.check(p.Reset(e.GetFrontierType(), 1.3))
         res = {}
         for mode, mname in ((0, "fused persistent"), (2, "cuda graph"), (1, "per-level launches")):

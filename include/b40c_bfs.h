@@ -41,6 +41,7 @@ extern "C" {
 #define B40C_ERROR_NOT_READY                600  /* cudaErrorNotReady */
 #define B40C_ERROR_LAUNCH_TIMEOUT           702  /* cudaErrorLaunchTimeout: a bounded device-side wait expired */
 #define B40C_ERROR_NOT_SUPPORTED            801  /* cudaErrorNotSupported */
+#define B40C_ERROR_INTERNAL                 999  /* cudaErrorUnknown: a device-side consistency check failed */
 
 /* ---- enums ---------------------------------------------------------------- */
 
@@ -106,6 +107,10 @@ typedef struct b40c_bfs_policy {
                                       (testing neighbours on the labels; a kernel variant of its own):
                                       1 = on, -1 = off (default: measured slower overall on R-MAT and
                                       uniform graphs) */
+    int32_t bottom_up_defer_frontier; /* fused direction-optimizing searches: a bottom-up level only counts
+                                      its discoveries (and their edges); their vertex frontier is built
+                                      from the two visited-mask buffers only when a top-down level
+                                      follows: 1 = on (default), -1 = off */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

@@ -22,20 +22,26 @@ def _g(kind):
 
 
 def test_classify_builders():
-    assert autotune.classify(_g("grid2d")) == "lattice"
-    assert autotune.classify(_g("grid3d")) == "lattice"
+    assert autotune.classify(_g("grid2d")) == "lattice-narrow"
+    assert autotune.classify(_g("grid3d")) == "lattice-narrow"
+    wide = CsrGraph()
+    BuildGrid3dGraph(128, wide)  # levels of ~16k vertices
+    assert autotune.classify(wide) == "lattice-wide"
+    long2d = CsrGraph()
+    BuildGrid2dGraph(1000, long2d)  # levels of at most 1000 vertices
+    assert autotune.classify(long2d) == "lattice-narrow"
     assert autotune.classify(_g("rmat")) == "power-law"
     assert autotune.classify(_g("rr")) == "uniform"
 
 
 def test_policy_lookup(tmp_path):
     path = tmp_path / "cache.json"
-    path.write_text(json.dumps({"classes": {"lattice": {"direction-optimizing": {
+    path.write_text(json.dumps({"classes": {"lattice-narrow": {"direction-optimizing": {
         "policy": {"small_frontier_edges": 4096, "ctas_per_sm": 2}}}}}))
     pol = autotune.policy_for(_g("grid2d"), path=str(path))
     assert pol.small_frontier_edges == 4096 and pol.ctas_per_sm == 2 and pol.chunk_edges == 0
     assert autotune.policy_for("power-law", path=str(path)) is None
-    assert autotune.policy_for("lattice", kind="batched", path=str(path)) is None
+    assert autotune.policy_for("lattice-narrow", kind="batched", path=str(path)) is None
 
 
 def test_committed_cache_is_well_formed():

@@ -356,17 +356,20 @@ def test_source_without_edges(strategy, mode):
         assert e.GetStatistics()[1] == depth
 
 
-@pytest.mark.parametrize("scan,hub", [(1, 1), (1, -1)])
+@pytest.mark.parametrize("scan,hub,defer", [(1, 1, 1), (1, -1, 1), (1, 1, -1)])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 15, 12)), ("grid3d", (24,))])
 @pytest.mark.parametrize("preds", [False, True])
-def test_bottom_up_scan_variants(scan, hub, kind, args, preds):
-    """Bottom-up levels with and without the hub-pair probes give the oracle's
-    distances and valid predecessors; alpha 2 forces many bottom-up levels."""
+def test_bottom_up_scan_variants(scan, hub, defer, kind, args, preds):
+    """Bottom-up levels with and without the hub-pair probes, with the frontier
+    deferred (built from the mask buffers when a top-down level follows) or
+    emitted, give the oracle's distances and valid predecessors; alpha 2 forces
+    many bottom-up levels."""
     g = _graph(kind, *args)
     p = CsrProblem.from_graph(g, mark_predecessors=preds)
     pol = N.Policy()
     pol.bottom_up_scan = scan
     pol.bottom_up_hub_probes = hub
+    pol.bottom_up_defer_frontier = defer
     pol.bottom_up_alpha = 2
     for s in sample_sources(g, 3, seed=9):
         got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, policy=pol)
@@ -397,20 +400,23 @@ def test_batched_pull_hub_probes(hub, kind, args):
         assert depths[slot] == depth
 
 
-@pytest.mark.parametrize("lists", [1, -1])
+@pytest.mark.parametrize("lists,defer", [(1, 1), (-1, 1), (-1, -1)])
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("alpha,beta", [(2, 1), (2, 24), (2, 1000), (1, 2)])
 @pytest.mark.parametrize("kind,args", [("rmat", (1 << 15, 1 << 19)), ("rr", (1 << 14, 10)), ("grid3d", (20,))])
-def test_bottom_up_list_mode_and_alternation(lists, mode, alpha, beta, kind, args):
+def test_bottom_up_list_mode_and_alternation(lists, defer, mode, alpha, beta, kind, args):
     """Direction switches in every pattern (bottom-up runs, bottom-up -> top-down
     -> bottom-up with the unvisited list carried over and top-down levels
-    claiming on the labels) give the oracle's distances in every launch mode."""
+    claiming on the labels, deferred bottom-up frontiers built before a
+    top-down level or a solo phase) give the oracle's distances in every
+    launch mode."""
     g = _graph(kind, *args)
     p = CsrProblem.from_graph(g)
     pol = N.Policy()
     pol.bottom_up_alpha = alpha
     pol.bottom_up_beta = beta
     pol.bottom_up_list = lists
+    pol.bottom_up_defer_frontier = defer
     for s in sample_sources(g, 3, seed=21):
         got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, mode=mode, policy=pol)
         want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
