@@ -1334,6 +1334,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         }
         if (p.persistent && s.E <= p.small_edges) {
             // ---- small frontiers: CTA 0 alone, level after level ----------------------
+            const int solo_pass = pass;  // (instrumented searches stamp the arrivals under it)
             if (blockIdx.x == 0) {
                 int smem_n = -1;  // >= 0: this level's frontier is the run tables in shared memory (entries)
                 for (int solo = 0;; solo++) {
@@ -1411,6 +1412,11 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                         emit_frontier<B>(p, s, pass - 1, p.vf[level & 1], &p.st->qe[pass % 3]);
                         __syncthreads();
                         smem_n = -1;
+                        // the phase ends here unless only the one-sub-round limit stopped it
+                        // (the frontier's size is known: no read of the counter it went to)
+                        if (n == 0 || En > (unsigned long long)p.small_edges || (dl >= 0 && level >= dl) ||
+                            solo + 1 >= kSoloLevelCap)
+                            break;
                     }
                     if (tid == 0) {
                         const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
@@ -1426,6 +1432,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                 if (tid == 0) p.st->solo_resume[solo_phase & 1] = level;
             }
             worked = true;
+            stamp(p, solo_pass, kPhaseArrive);
             if (!duty.barrier(p.st, generation, &s_ok)) break;
             // not st->cur_level: CTA 0 may already have moved it on by the time a slow CTA reads
             level = ld_cg(&p.st->solo_resume[solo_phase & 1]) - 1;  // the loop increment brings it back

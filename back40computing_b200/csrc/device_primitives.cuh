@@ -101,7 +101,10 @@ __device__ __forceinline__ unsigned lanemask_lt()
 // trip less than a separate release flag).  The counter sits on its own cache
 // line, away from the frontier counters' atomics.  It is zeroed before each
 // persistent launch.  Requires every CTA to be resident (cooperative launch).
-// Returns false when the wait expired or another CTA reported an error.
+// Returns false when the wait expired or an error was seen while waiting; an
+// error reported just before the barrier completed is left to the callers'
+// next read of the error word (every caller reads it before its next step, the
+// same value in every CTA), which saves a round trip per barrier.
 __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word,
                                              int *s_flag)
 {
@@ -126,7 +129,6 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsign
             __nanosleep(spins < 64 ? 32 : 256);
         }
         __threadfence();
-        if (ok && ld_cg(error_word) != 0) ok = 0;
         *s_flag = ok;
     }
     __syncthreads();
