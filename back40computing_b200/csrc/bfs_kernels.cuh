@@ -666,6 +666,107 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
     }
 }
 
+// Bottom-up continuation with the warp's pending lists in a queue: the lists
+// (slot t, lane) still without a parent after the first probes, of length in
+// (MIN_LEN, kBottomUpLongList], are listed in the warp's region of q_lo / q_hi
+// (next position, end; 32 * PER entries per warp) and handed out to lanes as
+// they become free, so a warp keeps 32 scans in flight until its queue is
+// empty instead of waiting for the longest list of each slot in turn; each
+// step reads four neighbours and their visited words.  The parent found for
+// entry i lands in q_par[i] and goes back to its slot.  Longer lists are then
+// searched by the whole warp, 32 neighbours at a time.  The queue arrays are
+// shared memory the caller does not use until after a CTA barrier.
+template <int PER, int K, int MIN_LEN>
+__device__ __forceinline__ void bottom_up_queue(const BfsParams &p, const uint32_t *mask, const bool (&todo)[PER],
+                                                const int (&r0)[PER], const int (&r1)[PER], int (&parent)[PER],
+                                                int32_t *q_lo, int32_t *q_hi, int32_t *q_par)
+{
+    const int lane = threadIdx.x & 31;
+    const int wbase = (threadIdx.x >> 5) * 32 * PER;
+    q_lo += wbase;
+    q_hi += wbase;
+    q_par += wbase;
+    int n = 0;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const int len = r1[t] - r0[t];
+        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= kBottomUpLongList;
+        const unsigned bal = __ballot_sync(0xffffffffu, pend);
+        if (pend) {
+            const int i = n + __popc(bal & lanemask_lt());
+            q_lo[i] = r0[t] + K;
+            q_hi[i] = r1[t];
+            q_par[i] = -1;
+        }
+        n += __popc(bal);
+    }
+    __syncwarp();
+    int cur = -1, e = 0, hi = 0, handed = 0;
+    for (;;) {
+        const bool idle = cur < 0;
+        const unsigned ib = __ballot_sync(0xffffffffu, idle);
+        if (idle) {
+            const int i = handed + __popc(ib & lanemask_lt());
+            if (i < n) {
+                cur = i;
+                e = q_lo[i];
+                hi = q_hi[i];
+            }
+        }
+        handed += __popc(ib);
+        if (!__any_sync(0xffffffffu, cur >= 0)) break;
+        if (cur >= 0) {
+            int nb[4];
+            unsigned w[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) nb[k] = (e + k < hi) ? ld_stream(p.column_indices + e + k) : -1;
+#pragma unroll
+            for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
+            int found = -1;
+#pragma unroll
+            for (int k = 3; k >= 0; k--)
+                if (nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) found = nb[k];
+            e += 4;
+            if (found >= 0) q_par[cur] = found;
+            if (found >= 0 || e >= hi) cur = -1;
+        }
+    }
+    __syncwarp();
+    n = 0;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const int len = r1[t] - r0[t];
+        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= kBottomUpLongList;
+        const unsigned bal = __ballot_sync(0xffffffffu, pend);
+        if (pend) parent[t] = q_par[n + __popc(bal & lanemask_lt())];
+        n += __popc(bal);
+    }
+    // long lists: the whole warp, one list at a time
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const bool longlist = todo[t] && parent[t] < 0 && r1[t] - r0[t] > kBottomUpLongList;
+        unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+        while (lmask) {
+            const int owner = __ffs(lmask) - 1;
+            lmask &= lmask - 1;
+            const int lr0 = __shfl_sync(0xffffffffu, r0[t], owner) + K;
+            const int lr1 = __shfl_sync(0xffffffffu, r1[t], owner);
+            int found_u = -1;
+            for (int eb = lr0; eb < lr1; eb += 32) {
+                const int ee = eb + lane;
+                const int nb = ee < lr1 ? ld_stream(p.column_indices + ee) : -1;
+                const bool hit = nb >= 0 && ((ld_mask(mask + (nb >> 5)) >> (nb & 31)) & 1u);
+                const unsigned hb = __ballot_sync(0xffffffffu, hit);
+                if (hb) {
+                    found_u = __shfl_sync(0xffffffffu, nb, __ffs(hb) - 1);
+                    break;
+                }
+            }
+            if (lane == owner) parent[t] = found_u;
+        }
+    }
+}
+
 // Still-unvisited vertices of a bottom-up chunk, collected in s.stage (free
 // during bottom-up levels) and then appended to the next unvisited list with
 // one atomic per chunk.  Called by whole warps.
@@ -774,10 +875,19 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         }
         stamp_synced(p, pass, 2, first);
         // ---- continue the scan for candidates still without a parent ---------------
-        if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
-            bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
-        else
-            bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
+        if (LISTS) {
+            if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
+                bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
+            else
+                bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
+        } else {
+            // (s.colstart / s.rel / s.out are free until the discoveries are appended)
+            if (p.hub2)
+                bottom_up_queue<PER, 0, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
+            else
+                bottom_up_queue<PER, K, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
+            if (!defer) __syncthreads();  // every warp's queue is done before the appends
+        }
         stamp_synced(p, pass, 3, first);
         // ---- label, mark and append the discoveries --------------------------------
 #pragma unroll
@@ -933,10 +1043,13 @@ __device__ __forceinline__ void bottom_up_windows(const BfsParams &p, ExpandSmem
                 }
             }
             stamp_synced(p, pass, 2, first);
-            if (p.hub2)  // the pair came from anywhere in the list: longer lists are scanned from the start
-                bottom_up_lanes<PER, 0, K, false>(p, mask, level, todo, r0, r1, parent);
+            // the pair came from anywhere in the list: longer lists are scanned from the
+            // start (s.colstart / s.rel / s.out are free until the discoveries are appended)
+            if (p.hub2)
+                bottom_up_queue<PER, 0, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
             else
-                bottom_up_lanes<PER, K, K, false>(p, mask, level, todo, r0, r1, parent);
+                bottom_up_queue<PER, K, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
+            if (!defer) __syncthreads();  // every warp's queue is done before the appends
             stamp_synced(p, pass, 3, first);
 #pragma unroll
             for (int t = 0; t < PER; t++) {
