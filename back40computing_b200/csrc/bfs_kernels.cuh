@@ -612,7 +612,8 @@ __device__ __forceinline__ bool probe_hit(unsigned x, int u, int level)
     return LABELS ? ((int)x >= 0 && (int)x <= level) : (((x >> (u & 31)) & 1u) != 0);
 }
 
-// Bottom-up continuation, one lane per vertex: each lane scans its own list
+// Bottom-up continuation, one lane per vertex (list-mode levels; range levels
+// use bottom_up_queue): each lane scans its own list
 // on (K neighbours already probed at its start; lists of at most MIN_LEN are
 // finished), four neighbours at a time; lists longer than kBottomUpLongList
 // are searched by the whole warp, 32 neighbours at a time.
@@ -959,7 +960,7 @@ __device__ __forceinline__ void scatter_bits(unsigned bits, int v0, int pos, int
 // handled in batches of up to kChunkMax from a shared-memory list, so only
 // unvisited vertices take lanes and a mostly visited window costs one batch.
 // A batch: rows and hub pairs (independent loads, issued together), the
-// pair's probes, the per-lane (per-warp for long lists) scan of the rest,
+// pair's probes, the queued per-lane (per-warp for long lists) scan of the rest,
 // then labels; a discovery sets its bit in the window's shared copy of the
 // words (s.win_word), written whole to the other mask buffer when the window
 // ends.  With `defer` (CTA-uniform) discoveries are only counted (one packed
