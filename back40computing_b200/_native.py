@@ -155,6 +155,8 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_bfs_enact_limited": (C.c_int, [C.c_void_p, C.c_int, C.c_int, C.c_int32, C.c_int32, C.c_int,
                                          C.POINTER(Policy)]),
     "b40c_bfs_extract": (C.c_int, [C.c_void_p, _P_i32]),
+    "b40c_bfs_extract_async": (C.c_int, [C.c_void_p, _P_i32, C.c_int]),
+    "b40c_bfs_extract_wait": (C.c_int, [C.c_void_p, C.c_int]),
     "b40c_bfs_stats": (C.c_int, [C.c_void_p, _P_i64, _P_i32, C.POINTER(C.c_double)]),
     "b40c_bfs_problem_is_symmetric": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_set_instrument": (C.c_int, [C.c_void_p, C.c_int]),

@@ -109,6 +109,17 @@ class CsrProblem:
         assert h_labels.dtype == np.int32 and h_labels.size >= self.nodes
         return N.lib().b40c_bfs_extract(self.handle, N.i32p(h_labels))
 
+    def ExtractResultsAsync(self, h_labels: np.ndarray, slot: int) -> int:
+        """Starts the read-back of the last search's labels into h_labels through
+        staging slot 0 or 1 and returns at once (pinned memory overlaps the copy
+        with the next search); ExtractWait(slot) completes it.  h_labels must
+        stay alive and untouched until then."""
+        assert h_labels.dtype == np.int32 and h_labels.size >= self.nodes
+        return N.lib().b40c_bfs_extract_async(self.handle, N.i32p(h_labels), int(slot))
+
+    def ExtractWait(self, slot: int) -> int:
+        return N.lib().b40c_bfs_extract_wait(self.handle, int(slot))
+
     def labels(self) -> np.ndarray:
         out = np.empty(self.nodes, dtype=np.int32)
         N.check(self.ExtractResults(out), "ExtractResults")

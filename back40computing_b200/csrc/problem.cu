@@ -239,6 +239,9 @@ int64_t device_bytes(const b40c_bfs_problem *p)
     if (p->d_levels) t += a((int64_t)sizeof(LevelRecord) * kMaxLevelRecords);
     if (p->d_duty) t += a(4 * sizeof(unsigned long long));
     if (p->d_arrive) t += a((int64_t)sizeof(unsigned long long) * kMaxArrivePasses * kMaxArriveCtas * kPhaseStamps);
+    for (int i = 0; i < 2; i++)
+        if (p->d_stage[i]) t += a(4 * n);
+    if (p->d_stage_err) t += a(8);
     return t;
 }
 
@@ -270,9 +273,8 @@ int read_state(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
-int check_state_errors(b40c_bfs_problem *p)
+int error_status(unsigned e)
 {
-    const unsigned e = p->h_st->error;
     if (e & dev::kErrOverflow)
         return b40c::fail(B40C_ERROR_INVALID_CONFIGURATION,
                           "Frontier queue overflow.  Please increase queue-sizing factor.");
@@ -283,6 +285,23 @@ int check_state_errors(b40c_bfs_problem *p)
     if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk | dev::kErrInjected))
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a bounded device-side wait expired (error bits 0x%x)", e);
     return B40C_SUCCESS;
+}
+
+int check_state_errors(b40c_bfs_problem *p) { return error_status(p->h_st->error); }
+
+// Copies labels[n] into a staging slot (16-byte vectors; cudaMalloc'd buffers
+// are aligned) and the search's error word beside it.
+__global__ void stage_results_kernel(const int32_t *labels, int32_t *stage, int64_t n, const uint32_t *err,
+                                     uint32_t *err_out)
+{
+    const int64_t n4 = n / 4;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int4 *src4 = reinterpret_cast<const int4 *>(labels);
+    int4 *dst4 = reinterpret_cast<int4 *>(stage);
+    for (int64_t i = t0; i < n4; i += stride) dst4[i] = src4[i];
+    for (int64_t i = 4 * n4 + t0; i < n; i += stride) stage[i] = labels[i];
+    if (t0 == 0) *err_out = *err;
 }
 
 
@@ -778,6 +797,15 @@ int b40c_bfs_problem_destroy(b40c_bfs_problem *p)
     if (p->d_levels) cudaFree(p->d_levels);
     if (p->d_duty) cudaFree(p->d_duty);
     if (p->d_arrive) cudaFree(p->d_arrive);
+    if (p->copy_stream) cudaStreamSynchronize(p->copy_stream);
+    for (int i = 0; i < 2; i++) {
+        if (p->d_stage[i]) cudaFree(p->d_stage[i]);
+        if (p->staged_ev[i]) cudaEventDestroy(p->staged_ev[i]);
+        if (p->landed_ev[i]) cudaEventDestroy(p->landed_ev[i]);
+    }
+    if (p->d_stage_err) cudaFree(p->d_stage_err);
+    if (p->h_stage_err) cudaFreeHost(p->h_stage_err);
+    if (p->copy_stream) cudaStreamDestroy(p->copy_stream);
     for (int i = 0; i < 2; i++) {
         free_vf(p->vf[i]);
         free_ef(p->ef[i]);
@@ -1026,6 +1054,60 @@ int b40c_bfs_extract(b40c_bfs_problem *p, int32_t *h_labels)
     CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_labels, sizeof(int32_t) * p->nodes, cudaMemcpyDeviceToHost, p->stream),
              "label copy");
     CUDA_TRY(cudaStreamSynchronize(p->stream), "label copy synchronize");
+    return B40C_SUCCESS;
+}
+
+int b40c_bfs_extract_wait(b40c_bfs_problem *p, int slot)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    if (slot < 0 || slot > 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "staging slot %d (0 or 1)", slot);
+    if (!p->stage_pending[slot]) return B40C_SUCCESS;
+    DeviceGuard guard(p->device);
+    p->stage_pending[slot] = false;
+    CUDA_TRY(cudaEventSynchronize(p->landed_ev[slot]), "label copy synchronize");
+    return error_status(p->h_stage_err[slot]);
+}
+
+int b40c_bfs_extract_async(b40c_bfs_problem *p, int32_t *h_labels, int slot)
+{
+    b40c::clear_error();
+    if (!p || !h_labels) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    if (slot < 0 || slot > 1) return b40c::fail(B40C_ERROR_INVALID_VALUE, "staging slot %d (0 or 1)", slot);
+    DeviceGuard guard(p->device);
+    int rc;
+    if (p->stage_pending[slot]) {
+        // the slot's previous copy must land before its buffer is reused; its
+        // status belonged to an earlier search and was not asked for
+        p->stage_pending[slot] = false;
+        CUDA_TRY(cudaEventSynchronize(p->landed_ev[slot]), "label copy synchronize");
+    }
+    if (!p->copy_stream) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking), "copy stream");
+        for (int i = 0; i < 2; i++) {
+            CUDA_TRY(cudaEventCreateWithFlags(&p->staged_ev[i], cudaEventDisableTiming), "event");
+            CUDA_TRY(cudaEventCreateWithFlags(&p->landed_ev[i], cudaEventDisableTiming), "event");
+        }
+        if ((rc = alloc_dev((void **)&p->d_stage_err, 8, "staging error words"))) return rc;
+        CUDA_TRY(cudaHostAlloc((void **)&p->h_stage_err, 8, cudaHostAllocDefault), "pinned error words");
+    }
+    if (!p->d_stage[slot] &&
+        (rc = alloc_dev((void **)&p->d_stage[slot], sizeof(int32_t) * std::max<int64_t>(p->nodes, 1), "label staging")))
+        return rc;
+    const int64_t n = p->nodes;
+    const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((int64_t)p->sms * 8, (n / 4 + 255) / 256));
+    stage_results_kernel<<<blocks, 256, 0, p->stream>>>(p->d_labels, p->d_stage[slot], n, &p->st->error,
+                                                        p->d_stage_err + slot);
+    CUDA_TRY(cudaGetLastError(), "staging launch");
+    CUDA_TRY(cudaEventRecord(p->staged_ev[slot], p->stream), "event record");
+    CUDA_TRY(cudaStreamWaitEvent(p->copy_stream, p->staged_ev[slot], 0), "stream wait");
+    CUDA_TRY(cudaMemcpyAsync(h_labels, p->d_stage[slot], sizeof(int32_t) * n, cudaMemcpyDeviceToHost, p->copy_stream),
+             "label copy");
+    CUDA_TRY(cudaMemcpyAsync(p->h_stage_err + slot, p->d_stage_err + slot, sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                             p->copy_stream),
+             "error word copy");
+    CUDA_TRY(cudaEventRecord(p->landed_ev[slot], p->copy_stream), "event record");
+    p->stage_pending[slot] = true;
     return B40C_SUCCESS;
 }
 

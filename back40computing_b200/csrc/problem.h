@@ -91,6 +91,14 @@ struct b40c_bfs_problem {
     cudaGraphNode_t graph_copy_node[5] = {};  // the source-upload memcpy node of each graph
     b40c::BfsParams graph_params[5] = {};
     int graph_grid[5] = {};
+    // pipelined read-back (b40c_bfs_extract_async): two device staging slots,
+    // each with the search's error word, copied to the host on copy_stream
+    int32_t *d_stage[2] = {};
+    uint32_t *d_stage_err = nullptr;  // [2]
+    uint32_t *h_stage_err = nullptr;  // [2], pinned
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t staged_ev[2] = {}, landed_ev[2] = {};
+    bool stage_pending[2] = {};
 };
 
 namespace b40c {

@@ -190,6 +190,20 @@ int b40c_bfs_enact_limited(b40c_bfs_problem *problem, int strategy, int mode, in
 /* CsrProblem::ExtractResults (csr_problem.cuh:255-322): copies labels[n] to the host. */
 int b40c_bfs_extract(b40c_bfs_problem *problem, int32_t *h_labels);
 
+/* ExtractResults for pipelined searches (no reference counterpart: the
+ * reference reads results back synchronously).  Copies the labels of the
+ * search last enacted into device staging slot `slot` (0 or 1) in stream
+ * order, then starts their device-to-host copy into h_labels (labels[n]; pinned
+ * host memory lets it overlap) on a copy stream of the problem, and returns at
+ * once: the next search may be enacted right away, it waits only for the
+ * device-side copy.  A slot still in flight is waited for first.
+ * b40c_bfs_extract_wait(slot) blocks until that slot's labels are in host
+ * memory and returns the search's status (as b40c_bfs_extract would); it
+ * returns at once for a slot with nothing in flight.  h_labels must stay valid
+ * and untouched until then. */
+int b40c_bfs_extract_async(b40c_bfs_problem *problem, int32_t *h_labels, int slot);
+int b40c_bfs_extract_wait(b40c_bfs_problem *problem, int slot);
+
 /* Enactor*::GetStatistics (enactor_contract_expand.cuh:237-250 and peers):
  * total_queued = sum of the frontier-queue lengths the search processed,
  * search_depth = number of BFS levels (max distance + 1), avg_duty = mean

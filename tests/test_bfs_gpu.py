@@ -424,3 +424,36 @@ def test_bottom_up_list_mode_and_alternation(lists, defer, mode, alpha, beta, ki
         e = ENACTORS[DIRECTION_OPTIMIZING]()
         e._problem = p
         assert e.GetStatistics()[1] == depth
+
+
+@pytest.mark.parametrize("preds", [False, True])
+def test_pipelined_extract_matches_sync(preds):
+    """Read-back through the two staging slots while later searches run gives,
+    for every search, the labels the synchronous read-back gives."""
+    g = _graph("rmat", 1 << 14, 1 << 18)
+    p = CsrProblem.from_graph(g, mark_predecessors=preds)
+    e = ENACTORS[DIRECTION_OPTIMIZING]()
+    N.check(p.Reset(e.GetFrontierType(), 1.3))
+    srcs = [int(s) for s in sample_sources(g, 6, seed=4)]
+    bufs = [np.full(g.nodes, 7, np.int32) for _ in range(2)]
+    got = {}
+    for i, s in enumerate(srcs):
+        N.check(e._enact(p, s, N.ENACT_FUSED, 0))
+        slot = i & 1
+        if i >= 2:  # the slot's previous search: wait, then keep a copy before the buffer is reused
+            N.check(p.ExtractWait(slot))
+            got[srcs[i - 2]] = bufs[slot].copy()
+        N.check(p.ExtractResultsAsync(bufs[slot], slot))
+    for i in (len(srcs) - 2, len(srcs) - 1):
+        N.check(p.ExtractWait(i & 1))
+        got[srcs[i]] = bufs[i & 1].copy()
+    assert p.ExtractWait(0) == 0  # nothing in flight: returns at once
+    for s in srcs:
+        want, _ = oracle.bfs(g.row_offsets, g.column_indices, s)
+        if preds:
+            assert got[s][s] == -2
+            assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got[s]) == (-1, 0)
+        else:
+            assert oracle.compare_labels(got[s], want) == -1
+    with pytest.raises(B40cError):
+        N.check(p.ExtractResultsAsync(bufs[0], 2))
