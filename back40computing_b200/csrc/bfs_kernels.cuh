@@ -1406,6 +1406,9 @@ __device__ __forceinline__ void record_direction(const BfsParams &p, unsigned lo
 }
 
 constexpr int kSoloLevelCap = 4096;  // small levels CTA 0 runs alone before the grid resynchronises
+// bottom-up levels emit their frontier (rather than count it) once the unvisited
+// edges are under 1 / kDeferMinShare of the graph's
+constexpr unsigned long long kDeferMinShare = 512;
 
 // Expand-contract (vertex frontiers): one level per pass.  With
 // direction_opt, levels with a large frontier run bottom-up.  In a
@@ -1554,7 +1557,13 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
-        const bool defer = !LISTS && bu && p.bu_defer && p.persistent;
+        // a bottom-up level counts its discoveries instead of emitting them, unless
+        // the edges still unvisited (a bound on the next frontier's) are so few that
+        // emitting them costs less than building the frontier from the masks later
+        const unsigned long long unvisited =
+            (unsigned long long)p.edges - min((unsigned long long)p.edges, s.visited_edges);
+        const bool defer = !LISTS && bu && p.bu_defer && p.persistent &&
+                           unvisited * kDeferMinShare > (unsigned long long)p.edges;
         if (tid == 0 && blockIdx.x == 0)
             record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n, defer);
         if (LISTS && bu && s.ul_in >= 0)
