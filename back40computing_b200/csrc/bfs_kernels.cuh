@@ -215,10 +215,14 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
 // packed 64-bit atomicAdd on the pass's output counter (always with
 // lookback = false).  Each entry gets its slot, its degree prefix P and its
 // kChunkGrain boundaries in vout.cf.  The pass total accumulates in *qe_out.
-// All threads must call it.
+// A tile whose output ends past `skip_above` edges of the pass total only
+// counts: the caller passes the edge total beyond which the next level is
+// certain to run bottom-up (which never reads the frontier).  All threads must
+// call it.
 template <int B, typename Smem>
 __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int pass, const VertexFrontier &vout,
-                                              unsigned long long *qe_out, bool lookback = true)
+                                              unsigned long long *qe_out, bool lookback = true,
+                                              unsigned long long skip_above = ~0ull)
 {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int cnt = s.out_count;
@@ -259,6 +263,12 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
     const unsigned long long prefix = s.prefix;
     if (prefix == ~0ull) return;
     const unsigned g0 = (unsigned)(prefix >> 32), d0 = (unsigned)(prefix & 0xffffffffu);
+    if ((unsigned long long)d0 + (tot & 0xffffffffull) > skip_above) {
+        // counted above; the entries themselves are never read
+        if (tid == 0 && (unsigned long long)g0 + (tot >> 32) > (unsigned long long)p.vcap)
+            atomicOr(&p.st->error, kErrOverflow);
+        return;
+    }
     unsigned g = g0 + (unsigned)(excl >> 32);
     unsigned d = d0 + (unsigned)(excl & 0xffffffffu);
     bool long_run = false;
@@ -349,7 +359,8 @@ template <int B, bool PRED, bool FUSED_CULL, bool LISTS = false>
 __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFrontier &in, ExpandSmem<B, PRED> &s,
                                              int level, int pass, const VertexFrontier &vout,
                                              const EdgeFrontier &eout, unsigned long long *qe_out,
-                                             unsigned &bar_phase, int part, int parts, bool defer_emit = false)
+                                             unsigned &bar_phase, int part, int parts, bool defer_emit = false,
+                                             unsigned long long skip_above = ~0ull)
 {
     const int tid = threadIdx.x;
     const int q = s.q, E = s.E;
@@ -479,7 +490,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         __syncthreads();
         if (first) stamp(p, pass, 4);
         if (defer_emit) return;  // single sub-round (the caller checked): the output stays in s.out / colstart / rel
-        emit_frontier<B>(p, s, pass, vout, qe_out);
+        emit_frontier<B>(p, s, pass, vout, qe_out, true, skip_above);
         __syncthreads();
         if (first) stamp(p, pass, 5);
     }
@@ -1577,8 +1588,24 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             // later bottom-up levels: the unvisited vertices of each window, compacted
             bottom_up_windows<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], defer);
         else
+        {
+            // direction-optimizing: once this level's output passes E* edges, where
+            // E* * (alpha + 1) > the edges unvisited after this level's input, the
+            // next level runs bottom-up whatever the rest adds (the switch test is
+            // E * alpha > m - visited - E), so later tiles need not write entries.
+            // E* is at least the solo-phase threshold: a next level that small runs
+            // top-down on CTA 0 before any switch test.
+            unsigned long long skip_above = ~0ull;
+            if (p.direction_opt && !LISTS) {
+                const unsigned long long un =
+                    (unsigned long long)p.edges - min((unsigned long long)p.edges, s.visited_edges);
+                skip_above = max(un / (unsigned long long)(p.bu_alpha + 1),
+                                 (unsigned long long)max(p.small_edges, 0));
+            }
             expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
-                                               &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x);
+                                               &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x, false,
+                                               skip_above);
+        }
         __syncthreads();
         worked = true;
         if (s.flag) max_level_seen = level + 1;
