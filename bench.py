@@ -62,6 +62,8 @@ def parse():
                     help="0 expand-contract, 1 contract-expand, 2 two-phase, 3 hybrid, 4 direction-optimizing")
     ap.add_argument("--mode", type=int, default=0, help="0 fused (persistent), 1 per-level launches, 2 CUDA graph")
     ap.add_argument("--sources", type=int, default=64)
+    ap.add_argument("--levels", type=int, default=0,
+                    help="print the per-level records of this many instrumented searches (one JSON line) and exit")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound on the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
@@ -212,6 +214,36 @@ def cpu_baseline(g, srcs, deg, budget_s):
     return {"value": edges / t / 1e9, "unit": "GTEPS", "cores": 1, "kind": kind,
             "host_cores": os.cpu_count(), "wall_s": t, "user_cpu_s": user,
             "sample": f"{used} of {len(srcs)} sources, serial SimpleReferenceBfs, wall clock ({t:.1f} s)"}
+
+
+def level_report(problem, enact, srcs):
+    """Per-level records of instrumented searches: frontier vertices and edges,
+    direction, the level's duration (block 0's start of the level to its start
+    of the next) and the CTAs' barrier arrival times within it."""
+    problem.set_instrument(True)
+    out = []
+    for s in srcs:
+        enact(s)  # warm
+        problem.labels()
+        enact(s)
+        problem.labels()
+        recs = problem.level_records()
+        search_us = float(problem.recent_search_ms(1)[0]) * 1e3
+        arr = problem.cta_arrivals(64)
+        levels = []
+        for r in recs:
+            k, t0 = r["pass_"], int(r["t_ns"])
+            row = arr[k].astype(np.int64) if k < arr.shape[0] else np.zeros(0, np.int64)
+            got = row[row > 0] - t0
+            lv = {"pass": k, "vertices": int(r["vertices"]), "edges": int(r["edges"]),
+                  "bottom_up": bool(r["bottom_up"]), "us": round(r.get("ns", 0) / 1e3, 2)}
+            if got.size > 1:
+                lv["arrive_us"] = {"median": round(float(np.median(got)) / 1e3, 2),
+                                   "max": round(float(got.max()) / 1e3, 2), "ctas": int(got.size)}
+            levels.append(lv)
+        out.append({"source": int(s), "search_us": round(search_us, 2), "levels": levels})
+    problem.set_instrument(False)
+    return out
 
 
 def max_over_ranks(x, dist=None, device="cuda"):
@@ -467,6 +499,15 @@ def main():
 
     def enact(s):
         N.check(enactor._enact(problem, int(s), args.mode, 0), "enact")
+
+    if args.levels:
+        if rank == 0:
+            print(json.dumps({"workload": CONFIGS[args.config]["workload"], "strategy": kind,
+                              "searches": level_report(problem, enact, srcs[:args.levels])}), flush=True)
+        problem.Destroy()
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     # untimed pass: per-source reached vertices/edges, and parity with the oracle on one source
     ec, vc = [], []
