@@ -210,128 +210,85 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
     for (int cs = rs; cs < re; cs += kChunkMax) {
         if (tid == 0) s.out_count = 0;
         __syncthreads();
-        // two vertices per lane at a time (slots t and t + 1), so each lane keeps
-        // two independent probe chains in flight
 #pragma unroll 1
-        for (int t = 0; t < PER; t += 2) {
-            constexpr int V2 = 2, U2 = U / V2;
-            int v[V2], r0[V2], r1[V2];
-            bool act[V2], inr[V2];
-            unsigned long long vold[V2], missing[V2], acc[V2];
-#pragma unroll
-            for (int u = 0; u < V2; u++) {
-                const int vb = cs + (t + u) * B + (tid & ~31);
-                act[u] = vb < re;  // warp-uniform
-                v[u] = vb + lane;
-                inr[u] = act[u] && v[u] < re;
-                vold[u] = inr[u] ? ld_cg64(m.visited + v[u]) : 0ull;
-            }
-            if (!act[0]) break;  // warp-uniform; slot t + 1 lies further on
-#pragma unroll
-            for (int u = 0; u < V2; u++) {
-                missing[u] = inr[u] ? (active & ~vold[u]) : 0ull;
-                acc[u] = 0;
-                r0[u] = r1[u] = 0;
-                if (missing[u]) {
-                    r0[u] = ld_ro(p.row_offsets + v[u]);
-                    r1[u] = ld_ro(p.row_offsets + v[u] + 1);
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * B + (tid & ~31);
+            if (vb >= re) break;  // warp-uniform
+            const int v = vb + lane;
+            const bool inr = v < re;
+            unsigned long long vold = 0, missing = 0;
+            int r0 = 0, r1 = 0;
+            if (inr) {
+                vold = ld_cg64(m.visited + v);
+                missing = active & ~vold;
+                if (missing) {
+                    r0 = ld_ro(p.row_offsets + v);
+                    r1 = ld_ro(p.row_offsets + v + 1);
                 }
             }
-            if (p.hub2) {
-                // each vertex's two highest-degree neighbours first (one coalesced load)
-                int2 h[V2];
-#pragma unroll
-                for (int u = 0; u < V2; u++) h[u] = missing[u] ? p.hub2[v[u]] : make_int2(-1, -1);
-#pragma unroll
-                for (int u = 0; u < V2; u++) {
-                    if (h[u].x >= 0) acc[u] |= ld_cg64(fcur + h[u].x) & missing[u];
-                    if (h[u].y >= 0) acc[u] |= ld_cg64(fcur + h[u].y) & missing[u];
-                }
-#pragma unroll
-                for (int u = 0; u < V2; u++)
-                    if (missing[u] && (acc[u] == missing[u] || r1[u] - r0[u] <= 2)) missing[u] = 0;  // done
+            unsigned long long acc = 0;
+            if (missing && p.hub2) {
+                // the vertex's two highest-degree neighbours first (one coalesced load)
+                const int2 h = p.hub2[v];
+                if (h.x >= 0) acc |= ld_cg64(fcur + h.x) & missing;
+                if (h.y >= 0) acc |= ld_cg64(fcur + h.y) & missing;
+                if (acc == missing || r1 - r0 <= 2) missing = 0;  // nothing left to look for
             }
-            bool longlist[V2];
-            int e[V2];
+            const bool longlist = missing && (r1 - r0) > kPullLongList;
+            if (missing && !longlist) {
+                for (int e = r0; e < r1 && acc != missing; e += U) {
+                    int nb[U];
 #pragma unroll
-            for (int u = 0; u < V2; u++) {
-                longlist[u] = missing[u] && (r1[u] - r0[u]) > kPullLongList;
-                e[u] = (missing[u] && !longlist[u]) ? r0[u] : r1[u];
-            }
-            // both short lists scanned together, U2 neighbours of each per step (as many
-            // loads in flight as one list U at a time)
-            while ((e[0] < r1[0] && acc[0] != missing[0]) || (e[1] < r1[1] && acc[1] != missing[1])) {
-                int nb[V2][U2];
+                    for (int k = 0; k < U; k++) nb[k] = (e + k < r1) ? ld_stream(p.column_indices + e + k) : -1;
+                    unsigned long long fm[U];
 #pragma unroll
-                for (int u = 0; u < V2; u++) {
-                    const bool go = e[u] < r1[u] && acc[u] != missing[u];
+                    for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_cg64(fcur + nb[k]) : 0ull;
 #pragma unroll
-                    for (int k = 0; k < U2; k++)
-                        nb[u][k] = (go && e[u] + k < r1[u]) ? ld_stream(p.column_indices + e[u] + k) : -1;
-                }
-                unsigned long long fm[V2][U2];
-#pragma unroll
-                for (int u = 0; u < V2; u++)
-#pragma unroll
-                    for (int k = 0; k < U2; k++) fm[u][k] = nb[u][k] >= 0 ? ld_cg64(fcur + nb[u][k]) : 0ull;
-#pragma unroll
-                for (int u = 0; u < V2; u++) {
-                    if (e[u] < r1[u] && acc[u] != missing[u]) {
-#pragma unroll
-                        for (int k = 0; k < U2; k++) acc[u] |= fm[u][k] & missing[u];
-                        e[u] += U2;
-                    }
+                    for (int k = 0; k < U; k++) acc |= fm[k] & missing;
                 }
             }
-#pragma unroll
-            for (int u = 0; u < V2; u++) {
-                unsigned lmask = __ballot_sync(0xffffffffu, longlist[u]);
-                while (lmask) {
-                    const int owner = __ffs(lmask) - 1;
-                    lmask &= lmask - 1;
-                    const int lr0 = __shfl_sync(0xffffffffu, r0[u], owner), lr1 = __shfl_sync(0xffffffffu, r1[u], owner);
-                    const unsigned long long miss = __shfl_sync(0xffffffffu, missing[u], owner);
-                    unsigned long long a = 0;
-                    for (int eb = lr0; eb < lr1; eb += 32) {
-                        const int ee = eb + lane;
-                        if (ee < lr1) a |= ld_cg64(fcur + ld_stream(p.column_indices + ee)) & miss;
-                        for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
-                        if (a == miss) break;
-                    }
-                    if (lane == owner) acc[u] = a;
+            unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+            while (lmask) {
+                const int owner = __ffs(lmask) - 1;
+                lmask &= lmask - 1;
+                const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
+                const unsigned long long miss = __shfl_sync(0xffffffffu, missing, owner);
+                unsigned long long a = 0;
+                for (int eb = lr0; eb < lr1; eb += 32) {
+                    const int ee = eb + lane;
+                    if (ee < lr1) a |= ld_cg64(fcur + ld_stream(p.column_indices + ee)) & miss;
+                    for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
+                    if (a == miss) break;
                 }
+                if (lane == owner) acc = a;
             }
-#pragma unroll
-            for (int u = 0; u < V2; u++) {
-                if (!act[u]) break;  // warp-uniform
-                found |= acc[u];
-                if (acc[u]) {
-                    m.visited[v[u]] = vold[u] | acc[u];
-                    fnext[v[u]] = acc[u];
-                    s.flag = 1;
-                }
-                // labels, source by source: one coalesced store per warp
-                const unsigned long long wor_lo = __reduce_or_sync(0xffffffffu, (unsigned)(acc[u] & 0xffffffffull));
-                const unsigned long long wor_hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc[u] >> 32));
-                unsigned long long wor = wor_lo | (wor_hi << 32);
-                while (wor) {
-                    const int src = __ffsll((long long)wor) - 1;
-                    wor &= wor - 1;
-                    if ((acc[u] >> src) & 1ull) m.labels[(long long)src * n + v[u]] = level + 1;
-                }
-                const bool push = acc[u] && r1[u] > r0[u];
-                const unsigned bal = __ballot_sync(0xffffffffu, push);
-                if (bal) {
-                    const int leader = __ffs(bal) - 1;
-                    int base = 0;
-                    if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
-                    base = __shfl_sync(0xffffffffu, base, leader);
-                    if (push) {
-                        const int slot = base + __popc(bal & lanemask_lt());
-                        s.out[slot] = v[u];
-                        s.colstart[slot] = r0[u];
-                        s.rel[slot] = r1[u] - r0[u];
-                    }
+            found |= acc;
+            if (acc) {
+                m.visited[v] = vold | acc;
+                fnext[v] = acc;
+                s.flag = 1;
+            }
+            // labels, source by source: one coalesced store per warp
+            const unsigned long long wor_lo = __reduce_or_sync(0xffffffffu, (unsigned)(acc & 0xffffffffull));
+            const unsigned long long wor_hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc >> 32));
+            unsigned long long wor = wor_lo | (wor_hi << 32);
+            while (wor) {
+                const int src = __ffsll((long long)wor) - 1;
+                wor &= wor - 1;
+                if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1;
+            }
+            const bool push = acc && r1 > r0;
+            const unsigned bal = __ballot_sync(0xffffffffu, push);
+            if (bal) {
+                const int leader = __ffs(bal) - 1;
+                int base = 0;
+                if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
+                base = __shfl_sync(0xffffffffu, base, leader);
+                if (push) {
+                    const int slot = base + __popc(bal & lanemask_lt());
+                    s.out[slot] = v;
+                    s.colstart[slot] = r0;
+                    s.rel[slot] = r1 - r0;
                 }
             }
         }
