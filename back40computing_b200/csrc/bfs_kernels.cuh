@@ -1727,7 +1727,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
 template <bool PRED, bool VERTEX_FRONTIER, bool FULL>
 __global__ void init_kernel(BfsParams p)
 {
-    const int src = p.st->src;
+    const int src = p.src_by_value ? p.src_arg : p.st->src;
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int src_label = PRED ? -2 : 0;
@@ -1751,6 +1751,10 @@ __global__ void init_kernel(BfsParams p)
     }
     if (t0 == 0) {
         SearchState *st = p.st;
+        if (p.src_by_value) {
+            st->src = p.src_arg;
+            st->depth_limit = p.depth_arg;
+        }
         const int r0 = p.row_offsets[src], r1 = p.row_offsets[src + 1];
         st->tile_ctr[0] = st->tile_ctr[1] = st->tile_ctr[2] = 0;
         st->cur_level = 0;

@@ -145,6 +145,11 @@ struct BfsParams {
     unsigned long long *duty; // [0] sum over CTAs of busy ns, [1] sum of lifetime ns (instrumented)
     unsigned long long *arrive;  // [pass][cta] %globaltimer at the end-of-level barrier (instrumented)
     unsigned long long cond_handle;  // cudaGraphConditionalHandle (graph mode), 0 = none
+    // 1: the init kernel takes the source and depth limit from src_arg /
+    // depth_arg (and stores them in the state); 0: they were copied into the
+    // state before it runs (CUDA-graph replays re-point that copy per launch)
+    int32_t src_by_value;
+    int32_t src_arg, depth_arg;
 };
 
 }  // namespace b40c

@@ -45,7 +45,11 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
         if ((rc = run_graph(p, slot, init, body, 1))) return rc;
         return finish_timing(p);
     }
-    if ((rc = upload_source(p))) return rc;
+    // the source and depth limit travel as kernel arguments of the init kernel
+    // (no host-to-device copy in the search's stream)
+    k.src_by_value = 1;
+    k.src_arg = src;
+    k.depth_arg = depth_limit;
     if ((rc = launch_init<PRED>(p, k, true, p->needs_init))) return rc;
     if ((rc = mark_search_start(p))) return rc;
     if (mode == B40C_ENACT_FUSED) {

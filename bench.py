@@ -561,14 +561,19 @@ def main():
     # of search i (two staging slots) overlaps search i + 1 on the device
     hosts = [torch.empty(g.nodes, dtype=torch.int32, pin_memory=True) for _ in range(2)]
     hviews = [h.numpy() for h in hosts]
+
+    def e2e_pass(steps):
+        for _ in range(steps):
+            for i, s in enumerate(srcs):
+                enact(s)
+                N.check(problem.ExtractResultsAsync(hviews[i & 1], i & 1), "ExtractResultsAsync")
+        for slot in (0, 1):
+            N.check(problem.ExtractWait(slot), "ExtractWait")
+
+    e2e_pass(1)  # untimed: staging buffers, copy stream and host pages warmed
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        for i, s in enumerate(srcs):
-            enact(s)
-            N.check(problem.ExtractResultsAsync(hviews[i & 1], i & 1), "ExtractResultsAsync")
-    for slot in (0, 1):
-        N.check(problem.ExtractWait(slot), "ExtractWait")
+    e2e_pass(args.steps)
     e2e_s = time.perf_counter() - t0
     if world > 1:
         e2e_s = max_over_ranks(e2e_s, dist)
