@@ -1732,7 +1732,24 @@ __global__ void init_kernel(BfsParams p)
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int src_label = PRED ? -2 : 0;
     if (FULL) {
-        for (long long i = t0; i < p.nodes; i += stride) p.labels[i] = (VERTEX_FRONTIER && i == src) ? src_label : -1;
+        // 16-byte stores when the labels array is 16-byte aligned (a caller's
+        // array given to the allocation-free search may not be); the source's
+        // label is set by the thread that stores its vector
+        const long long n4 = (reinterpret_cast<uintptr_t>(p.labels) & 15) == 0 ? p.nodes / 4 : 0;
+        int4 *labels4 = reinterpret_cast<int4 *>(p.labels);
+        for (long long i = t0; i < n4; i += stride) {
+            int4 x = make_int4(-1, -1, -1, -1);
+            if (VERTEX_FRONTIER && (src >> 2) == i) {
+                const int r = src & 3;
+                x.x = r == 0 ? src_label : -1;
+                x.y = r == 1 ? src_label : -1;
+                x.z = r == 2 ? src_label : -1;
+                x.w = r == 3 ? src_label : -1;
+            }
+            labels4[i] = x;
+        }
+        for (long long i = 4 * n4 + t0; i < p.nodes; i += stride)
+            p.labels[i] = (VERTEX_FRONTIER && i == src) ? src_label : -1;
         for (long long w = t0; w < p.mask_words; w += stride) {
             // edgeless vertices start visited; the source's bit is set for a vertex
             // frontier and clear for an edge frontier (whose contraction labels it)

@@ -57,3 +57,21 @@ def test_noalloc_rejects_graphs_beyond_its_scratch():
     rc = _noalloc(ro, ci, g, 0, labels)
     assert rc == N.ERROR_INVALID_VALUE
     assert "exceeds its fixed scratch" in N.lib().b40c_last_error_string().decode()
+
+
+def test_noalloc_labels_at_an_unaligned_address():
+    """A caller's labels array need not be 16-byte aligned: the reset falls back
+    to 4-byte stores and the neighbouring words stay untouched."""
+    import torch
+    g = CsrGraph()
+    BuildGrid2dGraph(97, g)  # 9,409 vertices: not a multiple of 4
+    ro, ci, _ = _device_csr(g)
+    buf = torch.full((g.nodes + 2,), 7, dtype=torch.int32, device="cuda")
+    labels = buf[1:1 + g.nodes]  # 4 bytes past a 256-byte aligned allocation
+    assert labels.data_ptr() % 16 == 4
+    N.check(_noalloc(ro, ci, g, 5, labels), "b40c_bfs_search_noalloc")
+    y, x = np.divmod(np.arange(g.nodes), 97)
+    want = np.abs(x - 5) + y  # L1 distance from vertex 5 on row 0
+    got = buf.cpu().numpy()
+    assert got[0] == 7 and got[-1] == 7
+    assert np.array_equal(got[1:-1], want.astype(np.int32))
