@@ -65,6 +65,7 @@ struct ExpandSmem {
     int32_t ul_n;                      // entries of that list
     int32_t ul_base;                   // where this chunk's still-unvisited vertices go in the next list
     int32_t solo_stop;                 // the solo phase writes its frontier out (CTA-uniform decision)
+    int32_t run_count;                 // expand: runs of a sub-round that spans more than B entries
     uint32_t win_word[B];              // bottom-up windows: the window's visited words, discoveries OR'ed in
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
@@ -375,25 +376,53 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         const int len = ce - cs;
         const bool first = FUSED_CULL && cs == rs;
         // ---- load the runs of entries i_cur.. that start before ce ----------------
-        if (tid == 0) s.out_count = 0;
-        int k = 0;
-        for (int base = i_cur;; base += B) {
-            const int i = base + tid;
+        if (tid == 0) {
+            s.out_count = 0;
+            s.run_count = B;
+        }
+        int k;
+        {
+            const int i = i_cur + tid;
             bool inside = false;
             if (i < q) {
                 const int Pi = ld_cg(in.P + i);
-                if (Pi < ce && i - i_cur <= kChunkMax) {
+                if (Pi < ce) {
                     inside = true;
-                    const int j = i - i_cur;
                     const int start = max(Pi, cs);
-                    s.rel[j] = start - cs;
-                    s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
-                    if (PRED) s.vert[j] = ld_cg(in.v + i);
+                    s.rel[tid] = start - cs;
+                    s.colstart[tid] = ld_cg(in.col + i) + (start - Pi);
+                    if (PRED) s.vert[tid] = ld_cg(in.v + i);
                 }
             }
-            const int c = __syncthreads_count(inside);
-            k += c;
-            if (c < B) break;
+            k = __syncthreads_count(inside);
+        }
+        if (k == B) {
+            // the sub-round spans more than B entries (short lists): the rest, at
+            // most kChunkMax + 1 - B (every entry has an edge), are loaded at once
+            // rather than B at a time; the entries inside form a prefix
+            constexpr int R = (kChunkMax + B) / B - 1;
+            int Pr[R];
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                const int i = i_cur + (r + 1) * B + tid;
+                Pr[r] = (i < q && i - i_cur <= kChunkMax) ? ld_cg(in.P + i) : INT_MAX;
+            }
+            int last = 0;
+#pragma unroll
+            for (int r = 0; r < R; r++) {
+                if (Pr[r] < ce) {
+                    const int i = i_cur + (r + 1) * B + tid;
+                    const int j = (r + 1) * B + tid;
+                    const int start = max(Pr[r], cs);
+                    s.rel[j] = start - cs;
+                    s.colstart[j] = ld_cg(in.col + i) + (start - Pr[r]);
+                    if (PRED) s.vert[j] = ld_cg(in.v + i);
+                    last = j + 1;
+                }
+            }
+            if (last) atomicMax(&s.run_count, last);
+            __syncthreads();
+            k = s.run_count;
         }
         if (tid == 0) s.rel[k] = len;
         if (first) stamp(p, pass, 1);
