@@ -47,6 +47,7 @@ class Policy(C.Structure):
         ("bottom_up_hub_probes", C.c_int32),
         ("bottom_up_list", C.c_int32),
         ("bottom_up_defer_frontier", C.c_int32),
+        ("subgrid_frontier_edges", C.c_int32),
     ]
 
 

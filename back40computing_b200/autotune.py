@@ -47,13 +47,14 @@ SEARCH_SPACE = {
     "bottom_up_beta": [12, 24, 48],
     "bitmask_precheck": [1, -1],
     "warp_cull": [1, -1],
+    "subgrid_frontier_edges": [-1, 4096, 16384, 65536],
 }
 # knobs that matter to each kind of search
 KNOBS = {
-    "direction-optimizing": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "bottom_up_alpha",
-                             "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck"],
-    "expand-contract": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "warp_gather_threshold",
-                        "cta_gather_threshold", "bitmask_precheck", "warp_cull"],
+    "direction-optimizing": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
+                             "bottom_up_alpha", "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck"],
+    "expand-contract": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
+                        "warp_gather_threshold", "cta_gather_threshold", "bitmask_precheck", "warp_cull"],
     "batched": ["ctas_per_sm", "bottom_up_alpha"],
 }
 

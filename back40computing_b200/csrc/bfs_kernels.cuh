@@ -38,6 +38,11 @@ namespace dev {
 
 constexpr int kChunkMax = 2048;   // edges (or edge-frontier items) per sub-round
 constexpr int kChunkGrain = 256;  // CTA ranges start at multiples of this; granularity of the cf index
+// With a sub-grid threshold (p.subgrid_edges), mid-size top-down levels (more
+// edges than a solo level, at most the threshold) of a persistent search run on
+// the first kSubgridCtas CTAs, which synchronise among themselves; the rest of
+// the grid waits at the grid barrier.
+constexpr int kSubgridCtas = 16;
 
 // emit_frontier: output entries whose degree spans more chunks than this have
 // their cf runs written by the whole CTA.
@@ -1456,7 +1461,7 @@ constexpr unsigned long long kDeferMinShare = 512;
 // p.small_edges edges is processed by CTA 0 alone, separated by CTA-level
 // barriers only, while the other CTAs wait at the grid barrier; while those
 // levels fit one sub-round their frontier stays in shared memory.
-template <int B, bool PRED, bool LISTS>
+template <int B, bool PRED, bool LISTS, bool SUBGRID = false>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1469,6 +1474,8 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, worked = false;
     int solo_phase = 0;  // small-frontier phases so far (the same count in every CTA)
+    int sub_phase = 0;   // sub-grid phases so far (the same count in every CTA)
+    unsigned sub_generation = 0;  // barriers of sub-grid phases this CTA took part in
     DutyClock duty(p);
     __syncthreads();
     for (int iter = 0; iter < p.max_levels; iter++, level++) {
@@ -1594,6 +1601,45 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             // not st->cur_level: CTA 0 may already have moved it on by the time a slow CTA reads
             level = ld_cg(&p.st->solo_resume[solo_phase & 1]) - 1;  // the loop increment brings it back
             solo_phase++;
+            continue;
+        }
+        // (a kernel variant of its own: the code would cost the other paths registers)
+        if (SUBGRID && p.persistent && p.subgrid_edges > 0 && s.E <= p.subgrid_edges &&
+            (int)gridDim.x >= 4 * kSubgridCtas &&
+            !choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges)) {
+            // ---- mid-size top-down levels: the first kSubgridCtas CTAs, level after
+            // level, with a barrier of their own; the others wait at the grid barrier
+            if ((int)blockIdx.x < kSubgridCtas) {
+                for (int sub = 0;; sub++) {
+                    if (tid == 0 && blockIdx.x == 0)
+                        record_direction(p, s.visited_edges, pass, false, s.mask, s.ul_in, s.ul_n);
+                    expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1],
+                                                       p.ef[0], &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x,
+                                                       kSubgridCtas);
+                    __syncthreads();
+                    if (s.flag) max_level_seen = level + 1;
+                    // (a wait that expires sets the error word: the test below then
+                    // ends the phase in every CTA of it)
+                    grid_barrier(&p.st->sub_barrier, sub_generation, &p.st->error, &s_ok, kSubgridCtas);
+                    level++;
+                    pass = level;
+                    // the level's frontier is counted once, by the pass that processes it
+                    begin_pass<B, PRED>(p, s, pass, false);
+                    if (tid == 0)
+                        s.solo_stop = s.q == 0 || s.E > p.subgrid_edges || s.E <= p.small_edges ||
+                                      (dl >= 0 && level >= dl) || sub + 1 >= kSoloLevelCap ||
+                                      ld_cg(&p.st->error) != 0 ||
+                                      choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
+                    __syncthreads();
+                    if (s.solo_stop) break;
+                    if (tid == 0 && blockIdx.x == 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
+                }
+                if (tid == 0 && blockIdx.x == 0) p.st->sub_resume[sub_phase & 1] = level;
+            }
+            worked = true;
+            if (!duty.barrier(p.st, generation, &s_ok)) break;
+            level = ld_cg(&p.st->sub_resume[sub_phase & 1]) - 1;  // the loop increment brings it back
+            sub_phase++;
             continue;
         }
         const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
@@ -1806,6 +1852,7 @@ __global__ void init_kernel(BfsParams p)
         st->cur_level = 0;
         st->epoch += 1ull << 24;
         st->barrier = 0;
+        st->sub_barrier = 0;
         st->error = 0;
         st->max_level = 0;
         st->done = 0;

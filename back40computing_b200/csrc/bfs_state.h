@@ -67,9 +67,14 @@ struct alignas(128) SearchState {
     // CTA 0, by phase parity (a slot is rewritten only two phases later, after
     // every CTA has read it)
     int32_t solo_resume[2];
+    // the same for a phase of mid-size top-down levels run by the first
+    // kSubgridCtas CTAs alone
+    int32_t sub_resume[2];
     // slots of a deferred bottom-up frontier built at the start of the next
     // level (count << 32 | edge total; cleared when the bottom-up level starts)
     unsigned long long mat_ctr;
+    // arrival counter of the barrier among the CTAs of a sub-grid phase (its own line)
+    alignas(128) unsigned long long sub_barrier;
 };
 
 __host__ __device__ inline int qe_count(unsigned long long x) { return (int)(x >> 32); }
@@ -133,6 +138,8 @@ struct BfsParams {
     int32_t bu_alpha;         // switch to bottom-up when frontier edges > unvisited edges / alpha
     int32_t bu_beta;          // switch back to top-down when frontier vertices < n / beta
     int32_t small_edges;      // persistent launches: frontiers with at most this many edges run on CTA 0 alone
+    int32_t subgrid_edges;    // persistent launches: top-down frontiers with more than small_edges and at most
+                              // this many edges run on the first kSubgridCtas CTAs alone (0: off)
     int32_t bu_scan;          // bottom-up continuation: 1 per lane, 2 per CTA (edge-parallel worklist)
     int32_t bu_defer;         // persistent bottom-up levels count their discoveries; the frontier is built
                               // from the mask buffers only when a top-down level follows

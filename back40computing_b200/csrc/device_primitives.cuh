@@ -105,13 +105,15 @@ __device__ __forceinline__ unsigned lanemask_lt()
 // error reported just before the barrier completed is left to the callers'
 // next read of the error word (every caller reads it before its next step, the
 // same value in every CTA), which saves a round trip per barrier.
+// `count` CTAs take part (the whole grid unless given: a sub-grid barrier has
+// its own counter).
 __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word,
-                                             int *s_flag)
+                                             int *s_flag, unsigned count = 0)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
         generation++;
-        const unsigned long long target = (unsigned long long)generation * gridDim.x;
+        const unsigned long long target = (unsigned long long)generation * (count ? count : gridDim.x);
         __threadfence();
         atomicAdd(counter, 1ull);
         unsigned spins = 0;

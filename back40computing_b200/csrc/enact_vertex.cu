@@ -30,8 +30,12 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     // distance searches with unvisited lists run the kernel variant that
     // carries list mode; the others keep the leaner code
     const bool lists_kernel = direction_opt && !PRED && pol.bottom_up_list > 0;
-    const void *kern = lists_kernel ? (const void *)dev::ec_kernel<kThreads, false, true>
-                                    : (const void *)dev::ec_kernel<kThreads, PRED, false>;
+    // fused searches with a sub-grid threshold run the variant that carries the
+    // sub-grid phase (not combined with list mode)
+    const bool subgrid_kernel = !lists_kernel && mode == B40C_ENACT_FUSED && pol.subgrid_frontier_edges > 0;
+    const void *kern = lists_kernel     ? (const void *)dev::ec_kernel<kThreads, false, true>
+                       : subgrid_kernel ? (const void *)dev::ec_kernel<kThreads, PRED, false, true>
+                                        : (const void *)dev::ec_kernel<kThreads, PRED, false>;
     const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;

@@ -111,6 +111,10 @@ typedef struct b40c_bfs_policy {
                                       its discoveries (and their edges); their vertex frontier is built
                                       from the two visited-mask buffers only when a top-down level
                                       follows: 1 = on (default), -1 = off */
+    int32_t subgrid_frontier_edges; /* fused searches: runs of top-down levels with more than
+                                      small_frontier_edges and at most this many edges run on 16 CTAs
+                                      with a barrier of their own while the rest of the grid waits (the
+                                      mid-size levels of high-diameter graphs); -1 = off (default) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

@@ -457,3 +457,32 @@ def test_pipelined_extract_matches_sync(preds):
             assert oracle.compare_labels(got[s], want) == -1
     with pytest.raises(B40cError):
         N.check(p.ExtractResultsAsync(bufs[0], 2))
+
+
+@pytest.mark.parametrize("threshold", [4096, 65536])
+@pytest.mark.parametrize("kind,args,strategy", [("grid2d", (300,), EXPAND_CONTRACT), ("grid3d", (40,), EXPAND_CONTRACT),
+                                                 ("rmat", (1 << 15, 1 << 19), DIRECTION_OPTIMIZING),
+                                                 ("rr", (1 << 15, 12), EXPAND_CONTRACT)])
+@pytest.mark.parametrize("preds", [False, True])
+def test_subgrid_phase(threshold, kind, args, strategy, preds):
+    """Runs of mid-size top-down levels on 16 CTAs with their own barrier (the
+    sub-grid phase, entered and left level by level between solo phases and
+    whole-grid levels) give the oracle's distances, valid predecessors and the
+    search depth."""
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g, mark_predecessors=preds)
+    pol = N.Policy()
+    pol.subgrid_frontier_edges = threshold
+    pol.ctas_per_sm = 1  # 148 CTAs: the phase needs at least 64
+    srcs = [0] if kind.startswith("grid") else [int(s) for s in sample_sources(g, 2, seed=17)]
+    for s in srcs:
+        got = search(p, s, strategy=strategy, policy=pol)
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, s)
+        if preds:
+            assert got[s] == -2
+            assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+        else:
+            assert oracle.compare_labels(got, want) == -1
+            e = ENACTORS[strategy]()
+            e._problem = p
+            assert e.GetStatistics()[1] == depth
