@@ -147,9 +147,12 @@ __device__ __forceinline__ bool warp_cull(bool valid, int v)
 // the winners) so each thread keeps all of its memory operations in flight.
 // A winner is labelled and, when it has edges, appended to the sub-round's
 // output (s.out = vertex, s.colstart = row start, s.rel = degree; the run
-// tables are consumed by then).  All threads of the CTA call it with
-// CTA-uniform `active`.
-template <int B, bool PRED, int U, bool LISTS = false>
+// tables are consumed by then).  With LEAVES (vertex-frontier searches) the
+// winners without edges, which never enter a frontier, are added to the
+// search's total_queued: the reference's expand-contract queues every
+// discovered vertex (expand_contract_atomic/cta.cuh:432-466).  All threads of
+// the CTA call it with CTA-uniform `active`.
+template <int B, bool PRED, int U, bool LISTS = false, bool LEAVES = false>
 __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B, PRED> &s, const int (&v)[U],
                                                const int (&u)[U], const bool (&valid)[U], const bool (&active)[U],
                                                int label_value, bool precheck = true)
@@ -197,6 +200,10 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
         if (!active[t]) continue;
         if (found[t]) s.flag = 1;  // benign race: every writer stores 1
         const bool push = found[t] && r1[t] > r0[t];
+        if (LEAVES) {
+            const unsigned leaf = __ballot_sync(0xffffffffu, found[t] && !push);
+            if (leaf && lane == __ffs(leaf) - 1) atomicAdd(&p.st->total_queued, (unsigned long long)__popc(leaf));
+        }
         const unsigned bal = __ballot_sync(0xffffffffu, push);
         if (bal == 0) continue;
         const int leader = __ffs(bal) - 1;
@@ -258,7 +265,7 @@ __device__ __forceinline__ void emit_frontier(const BfsParams &p, Smem &s, int p
                 if (lane == 0) lookback_publish(&p.slots[0], epoch, kFlagInclusive, tot);
             } else {
                 if (lane == 0) lookback_publish(&p.slots[tile], epoch, kFlagAggregate, tot);
-                prefix = lookback_exclusive(p.slots, (unsigned)tile, epoch, &p.st->error);
+                prefix = lookback_exclusive(p.slots, (unsigned)tile, epoch, &p.st->error, p.spin_limit);
                 if (lane == 0 && prefix != ~0ull) lookback_publish(&p.slots[tile], epoch, kFlagInclusive, prefix + tot);
             }
             if (lane == 0 && prefix != ~0ull) atomicAdd(qe_out, tot);  // pass totals
@@ -434,13 +441,17 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         const int j_last = k - 1;  // its run may continue into the next sub-round
 
         // ---- CTA-cooperative gather: a sub-round inside one adjacency list is
-        // staged into shared memory with one bulk copy of its aligned body ----------
-        const bool single = (k == 1) && (len >= p.cta_thresh);
+        // staged into shared memory with one bulk copy of its 16-byte aligned
+        // body (aligned by address, so any 4-byte aligned column array works) --
+        const bool single = p.bulk_ok && (k == 1) && (len >= p.cta_thresh);
         int b0 = 0, b1 = 0;
+        bool staged = true;  // false: this thread's wait for the bulk copy ran out
         if (single) {
             const int c0 = s.colstart[0];
-            b0 = (c0 + 3) & ~3;
-            b1 = (c0 + len) & ~3;
+            // column index i sits at a 16-byte boundary when (i + mis) % 4 == 0
+            const int mis = (int)((reinterpret_cast<uintptr_t>(p.column_indices) >> 2) & 3u);
+            b0 = ((c0 + mis + 3) & ~3) - mis;
+            b1 = ((c0 + len + mis) & ~3) - mis;
             if (b1 > b0) {
                 if (tid == 0) {
                     fence_proxy_async_smem();
@@ -448,16 +459,12 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
                     bulk_g2s(s.stage, p.column_indices + b0, (unsigned)(b1 - b0) * 4u, &s.bar);
                 }
                 unsigned spins = 0;
-                bool ok = true;
                 while (!mbar_try_wait(&s.bar, bar_phase)) {
-                    if (++spins > kSpinLimit) {
-                        atomicOr(&p.st->error, kErrBulk);
-                        ok = false;
+                    if (++spins > p.spin_limit) {
+                        staged = false;
                         break;
                     }
                 }
-                bar_phase ^= 1u;
-                if (!ok) b1 = b0;  // an expired wait leaves the staged words undefined: read global
             }
         } else {
             // ---- owner map: thread t resolves positions [t*PER, t*PER + PER)
@@ -485,7 +492,19 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
                 }
             }
         }
-        __syncthreads();
+        if (!__syncthreads_and(staged)) {
+            // the copy did not land in time: report it, give the copy still in
+            // flight one more bounded wait (so it cannot land in shared memory
+            // the CTA reuses) and stop; every caller reads the error word next
+            if (tid == 0) {
+                atomicOr(&p.st->error, kErrBulk);
+                unsigned spins = 0;
+                while (!mbar_try_wait(&s.bar, bar_phase) && ++spins <= p.spin_limit) __nanosleep(256);
+            }
+            __syncthreads();
+            return;
+        }
+        if (single && b1 > b0) bar_phase ^= 1u;
 
         if (first) stamp(p, pass, 2);
         // ---- gather: thread t takes positions t, t + B, ...: a warp reads 32
@@ -520,7 +539,7 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         }
         __syncthreads();  // run tables consumed: they now collect the sub-round's output
         if (first) stamp(p, pass, 3);
-        discover_batch<B, PRED, PER, LISTS>(p, s, v, u, valid, active, level + 1);
+        discover_batch<B, PRED, PER, LISTS, true>(p, s, v, u, valid, active, level + 1);
         __syncthreads();
         if (first) stamp(p, pass, 4);
         if (defer_emit) return;  // single sub-round (the caller checked): the output stays in s.out / colstart / rel
@@ -583,7 +602,7 @@ __device__ __forceinline__ void solo_level_smem(const BfsParams &p, ExpandSmem<B
         }
     }
     __syncthreads();  // run tables consumed: they now collect the level's output
-    discover_batch<B, PRED, PER, LISTS>(p, s, v, u, valid, active, level + 1, false);
+    discover_batch<B, PRED, PER, LISTS, true>(p, s, v, u, valid, active, level + 1, false);
     __syncthreads();
 }
 
@@ -1339,7 +1358,7 @@ struct DutyClock {
     {
         unsigned long long a = 0;
         if (p.duty && threadIdx.x == 0) a = globaltimer_ns();
-        const bool ok = grid_barrier(&st->barrier, generation, &st->error, s_flag);
+        const bool ok = grid_barrier(&st->barrier, generation, &st->error, s_flag, 0, p.spin_limit);
         if (p.duty && threadIdx.x == 0) waited += globaltimer_ns() - a;
         return ok;
     }
@@ -1401,7 +1420,9 @@ __device__ __forceinline__ void begin_pass(const BfsParams &p, ExpandSmem<B, PRE
         if (blockIdx.x == 0) {
             p.st->qe[(pass + 2) % 3] = 0;
             p.st->tile_ctr[(pass + 1) % 3] = 0;
-            if (count_queue) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
+            // (the reference counts the queues after the source's: kernel_runtime_stats
+            // aggregates from iteration 1 on, contract_expand_atomic/kernel.cuh:333-345)
+            if (count_queue && pass > 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
         }
         s.visited_edges = ld_cg64(&p.st->visited_edges[pass % 3]) + (unsigned long long)s.E;
         s.prev_bu = ld_cg(&p.st->dir[pass % 3]);
@@ -1448,6 +1469,21 @@ __device__ __forceinline__ void record_direction(const BfsParams &p, unsigned lo
         if (!bu) p.st->ul_count[(pass + 1) % 3] = (uint32_t)ul_n;
     }
     if (bu && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
+}
+
+// A phase of levels run by part of the grid (CTA 0 alone, or the first
+// kSubgridCtas CTAs) starts at a pass whose state slots (qe[pass % 3] and the
+// direction slots) every CTA reads in begin_pass; the CTAs outside the phase
+// then wait at the grid barrier.  Block 0 reuses those slots two passes on, so
+// before its second level it waits (thread 0, bounded) until the `outside` CTAs
+// have arrived at that barrier, which they do right after their read -- a late
+// CTA (one launched last, at kernel start) must not read a cleared slot.
+template <int B, bool PRED>
+__device__ __forceinline__ void outside_arrived(const BfsParams &p, ExpandSmem<B, PRED> &s, unsigned generation,
+                                                unsigned outside)
+{
+    if (threadIdx.x == 0) wait_outside_arrivals(&p.st->barrier, generation, outside, &p.st->error, p.spin_limit);
+    __syncthreads();
 }
 
 constexpr int kSoloLevelCap = 4096;  // small levels CTA 0 runs alone before the grid resynchronises
@@ -1536,6 +1572,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                                           (dl >= 0 && level >= dl) || solo + 1 >= kSoloLevelCap ||
                                           ld_cg(&p.st->error) != 0;
                         __syncthreads();
+                        if (!s.solo_stop && solo == 0) outside_arrived(p, s, generation, gridDim.x - 1);
                         if (!s.solo_stop) {
 #pragma unroll
                             for (int k = 0; k < PER; k++) {
@@ -1591,6 +1628,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                     const bool stop = s.q == 0 || s.E > p.small_edges || (dl >= 0 && level >= dl) ||
                                       solo + 1 >= kSoloLevelCap || ld_cg(&p.st->error) != 0;
                     if (stop) break;
+                    if (solo == 0) outside_arrived(p, s, generation, gridDim.x - 1);
                     begin_pass<B, PRED>(p, s, pass, true);
                 }
                 if (tid == 0) p.st->solo_resume[solo_phase & 1] = level;
@@ -1620,9 +1658,11 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                     if (s.flag) max_level_seen = level + 1;
                     // (a wait that expires sets the error word: the test below then
                     // ends the phase in every CTA of it)
-                    grid_barrier(&p.st->sub_barrier, sub_generation, &p.st->error, &s_ok, kSubgridCtas);
+                    grid_barrier(&p.st->sub_barrier, sub_generation, &p.st->error, &s_ok, kSubgridCtas,
+                                 p.spin_limit);
                     level++;
                     pass = level;
+                    if (sub == 0 && blockIdx.x == 0) outside_arrived(p, s, generation, gridDim.x - kSubgridCtas);
                     // the level's frontier is counted once, by the pass that processes it
                     begin_pass<B, PRED>(p, s, pass, false);
                     if (tid == 0)
@@ -1687,10 +1727,8 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         if (!p.persistent) break;
         stamp(p, pass, kPhaseArrive);
         if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
-        if ((int)blockIdx.x == p.skip_arrival_cta) {
-            if (tid == 0) atomicOr(&p.st->error, kErrInjected);
-            return;  // never arrives: the others' bounded waits must expire
-        }
+        if ((int)blockIdx.x == p.skip_arrival_cta)
+            return;  // test-only: never arrives, so the others' bounded waits must run out
         if (!duty.barrier(p.st, generation, &s_ok)) break;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
@@ -1731,20 +1769,19 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
         const int out_idx = p.edge_pingpong ? ((level + 1) & 1) : 0;
         if (p.phase_mask & 1) {
             const int pass = 2 * level;
-            begin_pass<B, PRED>(p, s, pass, true);
+            begin_pass<B, PRED>(p, s, pass, false);
             if (ld_cg(&p.st->error) != 0 || s.q == 0) break;
             if (p.hybrid && p.persistent && s.q > (int)gridDim.x * p.saturation) {
-                saturated = true;
+                saturated = true;  // the two-phase launches take this pass over (and count it)
                 break;
             }
+            if (tid == 0 && blockIdx.x == 0 && pass > 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
             contract_range<B, PRED>(p, s, p.ef[in_idx], level, pass, &p.st->qe[(pass + 1) % 3]);
             __syncthreads();
             if (s.flag) max_level_seen = max(max_level_seen, level);
             if (p.persistent) {
-                if ((int)blockIdx.x == p.skip_arrival_cta) {
-                    if (tid == 0) atomicOr(&p.st->error, kErrInjected);
-                    return;
-                }
+                if ((int)blockIdx.x == p.skip_arrival_cta)
+                    return;  // test-only: never arrives, so the others' bounded waits must run out
                 if (!duty.barrier(p.st, generation, &s_ok)) break;
             }
         }

@@ -130,6 +130,9 @@ struct BfsParams {
     int32_t saturation;       // hybrid: leave the fused kernel when items > gridDim * saturation
     int32_t persistent;       // 1: loop over levels with the grid barrier
     int32_t skip_arrival_cta; // test-only fault injection: this CTA never arrives (-1 = off)
+    uint32_t spin_limit;      // polls before a device-side wait gives up (dev::kSpinLimit; tests pass less)
+    int32_t bulk_ok;          // 1: a sub-round inside one adjacency list may be staged by cp.async.bulk
+                              // (column_indices is device memory; 0 for a host-mapped CSR)
     int32_t edge_pingpong;    // edge strategies: 1 = two edge frontiers (EDGE_FRONTIERS), 0 = one (MIXED)
     int32_t phase_mask;       // edge kernel: 1 = contract, 2 = expand, 3 = both per level (persistent)
     int32_t hybrid;           // edge kernel: leave the persistent loop when the frontier saturates

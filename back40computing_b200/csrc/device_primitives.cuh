@@ -17,7 +17,6 @@ constexpr unsigned kErrOverflow = 1u;       // a frontier queue would overflow
 constexpr unsigned kErrBarrier = 2u;        // grid barrier wait expired
 constexpr unsigned kErrLookback = 4u;       // look-back wait expired
 constexpr unsigned kErrBulk = 8u;           // bulk-copy wait expired
-constexpr unsigned kErrInjected = 16u;      // test-only: a CTA skipped its barrier arrival
 constexpr unsigned kErrLevels = 32u;        // more levels than vertices: a captured loop was stopped
 constexpr unsigned kErrFrontier = 64u;      // a deferred bottom-up frontier did not match its counted size
 constexpr unsigned kSpinLimit = 1u << 22;   // polls before a wait gives up (~1-2 s with backoff)
@@ -106,9 +105,10 @@ __device__ __forceinline__ unsigned lanemask_lt()
 // next read of the error word (every caller reads it before its next step, the
 // same value in every CTA), which saves a round trip per barrier.
 // `count` CTAs take part (the whole grid unless given: a sub-grid barrier has
-// its own counter).
+// its own counter).  `spin_limit` polls bound the wait (kSpinLimit in
+// production; tests pass a short limit to make a wait run out quickly).
 __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsigned &generation, unsigned *error_word,
-                                             int *s_flag, unsigned count = 0)
+                                             int *s_flag, unsigned count = 0, unsigned spin_limit = kSpinLimit)
 {
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -119,7 +119,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsign
         unsigned spins = 0;
         int ok = 1;
         while (ld_acquire(counter) < target) {
-            if (++spins > kSpinLimit) {
+            if (++spins > spin_limit) {
                 atomicOr(error_word, kErrBarrier);
                 ok = 0;
                 break;
@@ -135,6 +135,31 @@ __device__ __forceinline__ bool grid_barrier(unsigned long long *counter, unsign
     }
     __syncthreads();
     return *s_flag != 0;
+}
+
+// For a CTA that runs levels while `outside` other CTAs of the grid wait at the
+// next grid barrier (generation `generation` + 1): called by thread 0 before the
+// CTA first overwrites state those CTAs read at the start of the pass.  They
+// arrive right after that read, so once the counter shows their `outside`
+// arrivals (the barrier's own count starts at generation * gridDim.x: no CTA
+// can pass it while this one has not arrived) the state is free.  Bounded like
+// grid_barrier; returns false with kErrBarrier set when the wait expired, or
+// when another error was seen.
+__device__ __forceinline__ bool wait_outside_arrivals(const unsigned long long *counter, unsigned generation,
+                                                      unsigned outside, unsigned *error_word,
+                                                      unsigned spin_limit = kSpinLimit)
+{
+    const unsigned long long target = (unsigned long long)generation * gridDim.x + outside;
+    unsigned spins = 0;
+    while (ld_acquire(counter) < target) {
+        if (++spins > spin_limit) {
+            atomicOr(error_word, kErrBarrier);
+            return false;
+        }
+        if ((spins & 7) == 0 && ld_cg(error_word) != 0) return false;
+        __nanosleep(spins < 64 ? 32 : 256);
+    }
+    return true;
 }
 
 // ---- mbarrier + bulk copy (cp.async.bulk, global -> this CTA's shared) ----------
@@ -207,7 +232,8 @@ __device__ __forceinline__ void lookback_publish(LookbackSlot *slot, unsigned lo
 // (sum of the values of chunks 0..chunk-1); chunk 0 must not call it.  On
 // a wait that expires it sets kErrLookback and returns ~0ull.
 __device__ __forceinline__ unsigned long long lookback_exclusive(LookbackSlot *slots, unsigned chunk,
-                                                                 unsigned long long epoch, unsigned *error_word)
+                                                                 unsigned long long epoch, unsigned *error_word,
+                                                                 unsigned spin_limit = kSpinLimit)
 {
     const unsigned lane = threadIdx.x & 31;
     unsigned long long prefix = 0;
@@ -226,7 +252,7 @@ __device__ __forceinline__ unsigned long long lookback_exclusive(LookbackSlot *s
                                                      : ld_relaxed(&slots[j].aggregate);
                     break;
                 }
-                if (++spins > kSpinLimit) {
+                if (++spins > spin_limit) {
                     atomicOr(error_word, kErrLookback);
                     flag = kFlagInclusive;
                     value = ~0ull;

@@ -76,9 +76,11 @@ inline int launch_plain(b40c_bfs_problem *p, const void *kern, int grid, size_t 
 }
 
 // Test-only fault injection: B40C_TEST_SKIP_ARRIVAL_CTA=<cta> makes that CTA
-// of a persistent launch leave without arriving at the grid barrier, so the
-// other CTAs' bounded waits expire and the search reports
-// B40C_ERROR_LAUNCH_TIMEOUT.
+// of a persistent launch leave at its first whole-grid end-of-level barrier
+// without arriving (and without reporting anything), so the other CTAs'
+// bounded waits must run out; the search then reports
+// B40C_ERROR_LAUNCH_TIMEOUT.  B40C_TEST_SPIN_LIMIT (make_params) shortens
+// those waits.
 inline int injected_skip_cta()
 {
     const char *inj = getenv("B40C_TEST_SKIP_ARRIVAL_CTA");

@@ -55,7 +55,9 @@ static DeviceSetup g_setup[kMaxDevices];
 static std::mutex g_setup_mutex;
 
 // Once per device, with that device current: the scratch's device address,
-// the kernel's shared-memory attribute and its cooperative grid size.
+// the kernel's shared-memory attribute and its cooperative grid size.  These
+// belong to the device's primary context: after a cudaDeviceReset in the same
+// process they are stale, so the entry point must not be used after one.
 static int set_up(int device, DeviceSetup **out)
 {
     std::lock_guard<std::mutex> lock(g_setup_mutex);
@@ -104,6 +106,10 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
                           "(at most %lld vertices and %lld edges); use b40c_bfs_problem_create instead",
                           (long long)nodes, (long long)edges, (long long)kMaxNodes, (long long)kMaxEdges);
     if (src < 0 || src >= nodes) return b40c::fail(B40C_ERROR_INVALID_VALUE, "source %d out of range", src);
+    // int32 arrays: anything but a 4-byte aligned address would fault on the device
+    if ((reinterpret_cast<uintptr_t>(d_row_offsets) | reinterpret_cast<uintptr_t>(d_column_indices) |
+         reinterpret_cast<uintptr_t>(d_labels)) & 3u)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "b40c_bfs_search_noalloc: device arrays must be 4-byte aligned");
     int device = 0;
     if (cudaGetDevice(&device) != cudaSuccess || device >= kMaxDevices) {
         cudaGetLastError();
@@ -150,6 +156,8 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
     k.saturation = 512;
     k.persistent = 1;
     k.skip_arrival_cta = -1;
+    k.spin_limit = dev::kSpinLimit;
+    k.bulk_ok = 1;  // device memory; the kernel aligns each bulk copy by address
     k.alloc_lookback = 0;  // one packed atomic per tile: no look-back slots needed
     k.direction_opt = 0;
     k.bu_alpha = 14;

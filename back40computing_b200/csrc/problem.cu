@@ -92,6 +92,16 @@ int ensure_slots(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
+// Test-only: B40C_TEST_SPIN_LIMIT=<polls> shortens every device-side wait of
+// the searches enacted from then on, so a test can make one run out quickly.
+uint32_t test_spin_limit()
+{
+    const char *s = getenv("B40C_TEST_SPIN_LIMIT");
+    if (!s) return dev::kSpinLimit;
+    const long v = atol(s);
+    return v > 0 && v < (long)dev::kSpinLimit ? (uint32_t)v : dev::kSpinLimit;
+}
+
 BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
 {
     BfsParams k{};
@@ -123,6 +133,9 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.saturation = pol.saturation_quit;
     k.persistent = 0;
     k.skip_arrival_cta = -1;
+    k.spin_limit = test_spin_limit();
+    // a host-mapped CSR (stream_from_host) is read with plain loads only
+    k.bulk_ok = p->stream_from_host ? 0 : 1;
     k.alloc_lookback = pol.queue_allocation == 1 ? 1 : 0;
     k.direction_opt = 0;
     k.bu_alpha = pol.bottom_up_alpha;
@@ -285,7 +298,7 @@ int error_status(unsigned e)
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a replayed search ran more levels than the graph has vertices");
     if (e & dev::kErrFrontier)
         return b40c::fail(B40C_ERROR_INTERNAL, "a deferred bottom-up frontier did not match its counted size");
-    if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk | dev::kErrInjected))
+    if (e & (dev::kErrBarrier | dev::kErrLookback | dev::kErrBulk))
         return b40c::fail(B40C_ERROR_LAUNCH_TIMEOUT, "a bounded device-side wait expired (error bits 0x%x)", e);
     return B40C_SUCCESS;
 }
@@ -720,6 +733,10 @@ int b40c_bfs_problem_create(const int32_t *h_ro, const int32_t *h_ci, int64_t no
         return b40c::fail(B40C_ERROR_INVALID_VALUE,
                           "invalid CSR (nodes %lld, edges %lld; need 0 < nodes < 2^30, edges < 2^31)", (long long)nodes,
                           (long long)edges);
+    // int32 arrays at an address that is not 4-byte aligned cannot be read by
+    // the kernels when mapped zero-copy (and are not int32 arrays in C anyway)
+    if ((reinterpret_cast<uintptr_t>(h_ro) | reinterpret_cast<uintptr_t>(h_ci)) & 3u)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "row_offsets and column_indices must be 4-byte aligned");
     if (h_ro[0] != 0 || h_ro[nodes] != edges)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "row_offsets must start at 0 and end at edges");
     // the kernels index labels and the mask by column value: reject malformed CSR up front

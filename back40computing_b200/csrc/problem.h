@@ -138,6 +138,7 @@ int create_problem(int64_t nodes, int64_t edges, int mark_pred, int stream_from_
 int64_t planned_bytes(int64_t n, int64_t m, int k, double qs);
 int ensure_slots(b40c_bfs_problem *p);
 BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol);
+uint32_t test_spin_limit();
 b40c_bfs_policy default_policy(int strategy);
 int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out);
 int read_state(b40c_bfs_problem *p);

@@ -310,7 +310,7 @@ def run_reference(args, rank):
 def batched_extra(steps, warmup):
     """64-source batched search on the random 2^21 x 16 symmetrised graph against 64
     one-at-a-time plain searches (direction-optimizing and expand-contract) on the
-    same GPU; labels and search depths of two slots are checked against the oracle.
+    same GPU; every slot's labels and search depth are checked against the oracle.
     Algorithmic bytes of a batch: 4 * sum_v deg(v) * L_v + 4 * sum_s V_c(s), L_v =
     the number of distinct levels at which v is in some source's frontier."""
     import oracle
@@ -327,17 +327,15 @@ def batched_extra(steps, warmup):
     depths = p.msbfs_depths()
     ec, vc = [], []
     levels = np.zeros(g.nodes, np.uint64)
-    for slot in range(64):
+    for slot, (s, want, depth) in enumerate(oracle.bfs_many(g.row_offsets, g.column_indices, srcs)):
         lab = p.labels_of(slot)
         v, e = visited(deg, lab)
         ec.append(e)
         vc.append(v)
         m = lab >= 0
         levels[m] |= np.left_shift(np.uint64(1), lab[m].astype(np.uint64))
-        if slot in (0, 37):
-            want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
-            if oracle.compare_labels(lab, want) != -1 or depths[slot] != depth:
-                raise SystemExit("batched parity failure against the oracle")
+        if oracle.compare_labels(lab, want) != -1 or depths[slot] != depth:
+            raise SystemExit(f"batched parity failure against the oracle (slot {slot}, source {s})")
     lv = np.bitwise_count(levels).astype(np.int64)
     balg = 4.0 * float((deg * lv).sum()) + 4.0 * float(sum(vc))
     for _ in range(warmup):
@@ -453,11 +451,20 @@ def lattice_extra():
         p = CsrProblem.from_graph(g)
         e = ENACTORS[0](policy=autotune.policy_for(g, "expand-contract"))
         N.check(p.Reset(e.GetFrontierType(), 1.3))
+        # lattice BFS distance = L1 distance from the source (no wraparound)
+        w, dims = CONFIGS[name]["width"], (2 if name.startswith("grid2d") else 3)
+        idx = np.arange(g.nodes, dtype=np.int64)
+        want = np.zeros(g.nodes, np.int64)
+        for k in range(dims):
+            want += np.abs(idx // w ** k % w - int(srcs[0]) // w ** k % w)
+        want = want.astype(np.int32)
         res = {}
         for mode, mname in ((0, "fused persistent"), (2, "cuda graph"), (1, "per-level launches")):
             for _ in range(2):
                 N.check(e._enact(p, int(srcs[0]), mode, 0))
             ms = float(p.recent_search_ms(1)[0])
+            if not np.array_equal(p.labels(), want):
+                raise SystemExit(f"{name}: {mname} distances differ from the lattice distances")
             res[mname] = {"ms": ms, "gteps": ec / (ms * 1e-3) / 1e9}
         out[name] = res
         p.Destroy()
@@ -509,19 +516,25 @@ def main():
             dist.destroy_process_group()
         return
 
-    # untimed pass: per-source reached vertices/edges, and parity with the oracle on one source
+    # untimed pass: per-source reached vertices/edges; on rank 0 every source's
+    # labels are checked against the oracle (the reference's SimpleReferenceBfs
+    # in parallel host threads) before anything is timed
     ec, vc = [], []
-    for i, s in enumerate(srcs):
+    checks = None
+    if rank == 0:
+        import oracle
+        checks = oracle.bfs_many(g.row_offsets, g.column_indices, srcs)
+    for s in srcs:
         enact(s)
         labels = problem.labels()
         v, e = visited(deg, labels)
         vc.append(v)
         ec.append(e)
-        if i == 0 and rank == 0:
-            import oracle
-            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        if checks is not None:
+            ref_src, want, _ = next(checks)
+            assert ref_src == int(s)
             if oracle.compare_labels(labels, want) != -1:
-                raise SystemExit("parity failure against the oracle")
+                raise SystemExit(f"parity failure against the oracle (source {s})")
     ec, vc = np.array(ec, np.int64), np.array(vc, np.int64)
 
     def step():
@@ -580,14 +593,20 @@ def main():
     e2e = {"value": replica_gteps(float(ec.sum()) * args.steps, world, e2e_s), "unit": "GTEPS",
            "h2d_bytes_per_step": 8 * len(srcs), "d2h_bytes_per_step": 4 * g.nodes * len(srcs)}
 
-    # the same searches through the reference-faithful top-down strategy, for comparison
+    # the same searches through the reference's top-down strategies (what its
+    # drop-in callers reach), for comparison: device time per search
     topdown = None
     if args.strategy == 4 and rank == 0:
-        td = ENACTORS[0]()
-        for s in srcs:
-            N.check(td._enact(problem, int(s), args.mode, 0))
-        tk = problem.recent_search_ms(len(srcs))
-        topdown = {"gteps": float(ec.sum() / (tk.sum() * 1e-3) / 1e9), "kernel_ms_per_search": float(tk.mean())}
+        topdown = {}
+        for st in (0, 1, 3):
+            td = ENACTORS[st]()
+            N.check(problem.Reset(td.GetFrontierType(), 1.3), "Reset")
+            for s in srcs:
+                N.check(td._enact(problem, int(s), args.mode, 0))
+            tk = problem.recent_search_ms(len(srcs))
+            topdown[STRATEGY_NAMES[st]] = {"gteps": float(ec.sum() / (tk.sum() * 1e-3) / 1e9),
+                                           "kernel_ms_per_search": float(tk.mean()),
+                                           "roofline_frac": float(balg.mean() / (tk.mean() * 1e-3) / 1e9 / peak)}
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
@@ -608,7 +627,6 @@ def main():
                        "vertices": g.nodes, "edges": g.edges, "searches_per_step": len(srcs),
                        "strategy": STRATEGY_NAMES[args.strategy],
                        "policy": f"autotuned for class {graph_class}" if policy is not None else "library defaults",
-                       "topdown_expand_contract": topdown,
                        "mode": ["fused persistent", "per-level launches", "cuda graph"][args.mode],
                        "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6),
                        "parallelism": f"replicas x{world}"},
@@ -617,7 +635,7 @@ def main():
                          "traffic": (traffic or {}).get("dram_bytes_per_search"),
                          "bytes_per_search_alg": float(balg.mean()),
                          "kernel_ms_per_search": float(kernel_ms.mean())},
-            "cpu_baseline": cpu, "e2e": e2e,
+            "cpu_baseline": cpu, "e2e": e2e, "topdown": topdown,
             "gpu_launches": 2 * len(srcs) * args.steps,
             "clocks": clk,
             **extras,

@@ -7,6 +7,14 @@
  * cudaError_t results.  graph_slices[0] exposes the device arrays
  * (d_row_offsets, d_column_indices, d_labels, d_visited_mask: bit v & 7 of
  * byte v >> 3, as in the reference).  Only num_gpus == 1 is supported.
+ *
+ * The device arrays hold 32-bit ids and offsets (SizeT must be 32-bit).  A
+ * 64-bit VertexId (the reference driver's "g500" graphs, test_bfs.cu:1066-1090)
+ * is accepted on the host: FromHostProblem narrows the column indices into
+ * an int32 copy the problem keeps (the one mapped zero-copy with
+ * stream_from_host), ExtractResults widens the labels back, and
+ * graph_slices[0]->d_column_indices / d_labels are then NULL (the device
+ * copies are int32: b40c_bfs_device_view_get gives them).
  */
 #pragma once
 #include <stdio.h>
@@ -37,9 +45,10 @@ struct CsrProblem {
     typedef unsigned char VisitedMask;
     typedef unsigned char ValidFlag;
 
-    // the library's device arrays are 32-bit
-    typedef char vertex_id_must_be_32_bit[sizeof(VertexId) == 4 ? 1 : -1];
+    // the library's device arrays are 32-bit (ids of a 64-bit VertexId are narrowed on the host)
+    typedef char vertex_id_must_be_32_or_64_bit[sizeof(VertexId) == 4 || sizeof(VertexId) == 8 ? 1 : -1];
     typedef char size_t_must_be_32_bit[sizeof(SizeT) == 4 ? 1 : -1];
+    enum { NARROW_IDS = sizeof(VertexId) != 4 };
 
     /* Per-GPU device state (csr_problem.cuh:99-173); one slice on one GPU here. */
     struct GraphSlice {
@@ -61,6 +70,7 @@ struct CsrProblem {
     SizeT edges;
     std::vector<GraphSlice *> graph_slices;
     b40c_bfs_problem *handle;  // the library problem
+    std::vector<int32_t> narrow_ids;  // 64-bit VertexId: the int32 column indices (outlive the handle)
 
     CsrProblem() : num_gpus(0), nodes(0), edges(0), handle(NULL) {}
 
@@ -80,9 +90,20 @@ struct CsrProblem {
                                     __LINE__);
         if (handle) b40c_bfs_problem_destroy(handle);
         handle = NULL;
-        int rc = b40c_bfs_problem_create((const int32_t *)h_row_offsets, (const int32_t *)h_column_indices, nodes,
-                                         edges, MARK_PREDECESSORS ? 1 : 0, stream_from_host ? 1 : 0,
-                                         -1 /* the caller's current device */, &handle);
+        const int32_t *ids = (const int32_t *)h_column_indices;
+        if (NARROW_IDS) {
+            narrow_ids.resize(edges > 0 ? (size_t)edges : 1);
+            for (SizeT e = 0; e < edges; e++) {
+                const long long u = (long long)h_column_indices[e];
+                if (u < 0 || u >= (long long)nodes)
+                    return util::B40CPerror(cudaErrorInvalidValue, "CsrProblem: column index out of range", __FILE__,
+                                            __LINE__);
+                narrow_ids[e] = (int32_t)u;
+            }
+            ids = narrow_ids.data();
+        }
+        int rc = b40c_bfs_problem_create((const int32_t *)h_row_offsets, ids, nodes, edges, MARK_PREDECESSORS ? 1 : 0,
+                                         stream_from_host ? 1 : 0, -1 /* the caller's current device */, &handle);
         if (rc) return util::B40CPerror(util::AsCudaError(rc), "CsrProblem FromHostProblem failed", __FILE__, __LINE__);
         this->nodes = nodes;
         this->edges = edges;
@@ -93,8 +114,8 @@ struct CsrProblem {
         b40c_bfs_device_view_get(handle, &view);
         GraphSlice *slice = new GraphSlice(view.device);
         slice->d_row_offsets = (SizeT *)view.d_row_offsets;
-        slice->d_column_indices = (VertexId *)view.d_column_indices;
-        slice->d_labels = (VertexId *)view.d_labels;
+        slice->d_column_indices = NARROW_IDS ? NULL : (VertexId *)view.d_column_indices;
+        slice->d_labels = NARROW_IDS ? NULL : (VertexId *)view.d_labels;
         slice->d_visited_mask = (VisitedMask *)view.d_visited_mask;
         slice->nodes = nodes;
         slice->edges = edges;
@@ -115,7 +136,15 @@ struct CsrProblem {
     cudaError_t ExtractResults(VertexId *h_label)
     {
         if (!handle) return cudaErrorInvalidValue;
-        int rc = b40c_bfs_extract(handle, (int32_t *)h_label);
+        int rc;
+        if (NARROW_IDS) {
+            std::vector<int32_t> narrow(nodes > 0 ? (size_t)nodes : 1);
+            rc = b40c_bfs_extract(handle, narrow.data());
+            if (!rc)
+                for (SizeT v = 0; v < nodes; v++) h_label[v] = (VertexId)narrow[v];  // -1 / -2 sign-extend
+        } else {
+            rc = b40c_bfs_extract(handle, (int32_t *)h_label);
+        }
         return rc ? util::B40CPerror(util::AsCudaError(rc), "CsrProblem ExtractResults failed", __FILE__, __LINE__)
                   : cudaSuccess;
     }

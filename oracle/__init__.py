@@ -176,3 +176,24 @@ def ref_bfs(row_offsets, column_indices, src):
     L.ref_simple_bfs(n, column_indices.size, _p32(row_offsets), _p32(ci), int(src), _p32(labels), C.byref(depth),
                      C.byref(ms))
     return labels, int(depth.value), float(ms.value)
+
+
+def bfs_many(row_offsets, column_indices, sources, threads=None):
+    """Distances from each source, computed by independent serial searches in
+    parallel threads (ctypes releases the GIL during each call): the
+    reference's own SimpleReferenceBfs when its harness was built, else the C
+    restatement.  Yields (source, labels, search_depth) in source order;
+    search_depth = max label + 1 (what SimpleReferenceBfs reports)."""
+    from concurrent.futures import ThreadPoolExecutor
+    use_ref = have_ref()
+
+    def one(s):
+        if use_ref:
+            labels = ref_bfs(row_offsets, column_indices, int(s))[0]
+        else:
+            labels = bfs(row_offsets, column_indices, int(s))[0]
+        return int(s), labels, int(labels.max()) + 1
+
+    threads = threads or max(1, min(len(sources), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        yield from ex.map(one, list(sources))

@@ -1,6 +1,6 @@
 #!/usr/bin/env bash
 # Builds oracle/_ref/libb40c_ref.so from the reference's own sources, where
-# they lie in the read-only reference tree (default /root/reference, or $1).
+# they lie in the read-only reference tree given as $1.
 # Outputs go only to oracle/_ref/ (git-ignored).  Used to pin the C oracle and
 # the host builders against the reference, and as the reference CPU baseline.
 #
@@ -10,7 +10,7 @@
 # cut out of that file at build time into oracle/_ref/ and compiled by
 # oracle/ref_harness.cpp together with the reference's builder headers.
 set -euo pipefail
-REF="${1:-/root/reference}"
+REF="${1:?usage: build_ref.sh <reference tree>}"
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
 OUT="$HERE/_ref"
 CUDA_HOME="${CUDA_HOME:-/usr/local/cuda}"

@@ -80,3 +80,22 @@ def test_server_plan_bytes_arithmetic():
     assert csr + 4 * n + 3 * 8 * n < b1 < csr + 88 * n + m // 8
     with pytest.raises(N.B40cError):
         BfsServer.plan_bytes(n, m, 65)
+
+
+def test_unaligned_int32_arrays_are_rejected_before_any_device_call():
+    """int32 arrays must start on a 4-byte boundary: the no-allocation search
+    and problem creation refuse other addresses up front (no GPU touched)."""
+    import numpy as np
+    lib = N.lib()
+    good, odd = ctypes.c_void_p(1 << 20), ctypes.c_void_p((1 << 20) + 2)
+    for args in ((odd, good, good), (good, odd, good), (good, good, odd)):
+        rc = lib.b40c_bfs_search_noalloc(args[0], args[1], 100, 400, 0, args[2], None)
+        assert rc == N.ERROR_INVALID_VALUE
+        assert "4-byte aligned" in lib.b40c_last_error_string().decode()
+    raw = np.zeros(16, np.uint8)
+    base = (-raw.ctypes.data) % 4
+    ro = ctypes.cast(ctypes.c_void_p(raw.ctypes.data + base + 2),  # 2 bytes past a 4-byte boundary
+                     ctypes.POINTER(ctypes.c_int32))
+    h = ctypes.c_void_p()
+    rc = lib.b40c_bfs_problem_create(ro, ro, 1, 0, 0, 1, 0, ctypes.byref(h))
+    assert rc == N.ERROR_INVALID_VALUE and not h.value

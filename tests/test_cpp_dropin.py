@@ -105,3 +105,33 @@ def test_file_readers_through_cpp_headers(exes, tmp_path):
         g = CsrGraph()
         assert fn(g) == 0
         assert np.array_equal(ro, g.row_offsets) and np.array_equal(ci, g.column_indices), args[0]
+
+
+REF_DRIVER = os.path.join(ROOT, "oracle", "_ref", "test_bfs_dropin")
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not os.path.exists(REF_DRIVER), reason="reference driver not built (oracle/build_dropin.sh)")
+@pytest.mark.parametrize("args,strategies", [
+    (["grid2d", "300", "--src=0"], 5),
+    (["grid3d", "40", "--src=0", "--mark-pred"], 4),
+    (["rmat", "65536", "1048576", "--undirected", "--src=randomize", "--i=2"], 4),
+    (["rmat", "65536", "1048576", "--undirected", "--src=randomize", "--mark-pred"], 4),
+    (["rmat", "32768", "262144", "--undirected", "--src=randomize", "--stream-from-host"], 5),
+    (["g500", "32768", "--src=randomize"], 5),
+    (["random", "20000", "100000", "--undirected", "--src=randomize"], 4),
+    (["rr", "20000", "6", "--src=randomize", "--queue-sizing=2.0"], 4),
+])
+def test_reference_driver_unchanged_validates_on_gpu(args, strategies):
+    """The reference's own driver (test/bfs/test_bfs.cu: RunTests and main),
+    compiled unchanged against include/ by oracle/build_dropin.sh, runs every
+    enactor it knows (expand-contract, contract-expand, two-phase, hybrid and,
+    on one GPU, the multi-GPU one) and checks each against its own CPU BFS:
+    every GPU search prints CORRECT.  Covers 64-bit vertex ids (g500) and the
+    zero-copy --stream-from-host mode."""
+    strat = ",".join(str(s) for s in range(strategies))
+    r = subprocess.run([REF_DRIVER, *args, f"--strategy={strat}"], capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-2000:]
+    iters = 2 if "--i=2" in args else 1
+    assert "INCORRECT" not in r.stdout, r.stdout[-3000:]
+    assert r.stdout.count("CORRECT") == strategies * iters, r.stdout[-3000:]

@@ -32,11 +32,16 @@ def _noalloc(ro, ci, g, src, labels):
                                            int(src), C.c_void_p(labels.data_ptr()), C.c_void_p(stream))
 
 
-@pytest.mark.parametrize("kind", ["rmat", "grid2d"])
+@pytest.mark.parametrize("kind", ["rmat", "grid2d", "rmat_at_limits"])
 def test_noalloc_matches_expand_contract_twice(kind):
     g = CsrGraph()
     if kind == "rmat":
         BuildRmatGraph(1 << 16, 1 << 20, g, True, 0.57, 0.19, 0.19, seed=4, permute=True)
+    elif kind == "rmat_at_limits":
+        # 262,144 vertices and 4,194,302 edges: the largest graph the scratch
+        # takes (a level's chunk index may then span almost all of its entries)
+        BuildRmatGraph(1 << 18, (1 << 21) - 1, g, True, 0.57, 0.19, 0.19, seed=4, permute=True)
+        assert g.nodes == 1 << 18 and g.edges == (1 << 22) - 2
     else:
         BuildGrid2dGraph(300, g)
     problem = CsrProblem.from_graph(g)
