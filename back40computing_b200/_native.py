@@ -48,6 +48,7 @@ class Policy(C.Structure):
         ("bottom_up_list", C.c_int32),
         ("bottom_up_defer_frontier", C.c_int32),
         ("subgrid_frontier_edges", C.c_int32),
+        ("bottom_up_long_list", C.c_int32),
     ]
 
 

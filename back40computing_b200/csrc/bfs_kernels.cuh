@@ -643,7 +643,6 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
 // ------------------------------------------------------------------------------------
 // Bottom-up step (direction-optimizing levels, undirected graphs only)
 // ------------------------------------------------------------------------------------
-constexpr int kBottomUpLongList = 256;  // lists longer than this are searched warp-cooperatively
 
 // Level `level` run bottom-up over the CTA's share of vertex ids: every
 // unvisited vertex with edges looks for a neighbour whose visited bit is set
@@ -679,7 +678,7 @@ __device__ __forceinline__ bool probe_hit(unsigned x, int u, int level)
 // Bottom-up continuation, one lane per vertex (list-mode levels; range levels
 // use bottom_up_queue): each lane scans its own list
 // on (K neighbours already probed at its start; lists of at most MIN_LEN are
-// finished), four neighbours at a time; lists longer than kBottomUpLongList
+// finished), four neighbours at a time; lists longer than p.bu_long
 // are searched by the whole warp, 32 neighbours at a time.
 template <int PER, int K, int MIN_LEN, bool LABELS>
 __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32_t *mask, int level,
@@ -691,7 +690,7 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
     for (int t = 0; t < PER; t++) {
         const bool more = todo[t] && parent[t] < 0 && r1[t] - r0[t] > MIN_LEN;
         if (!__any_sync(0xffffffffu, more)) continue;
-        const bool longlist = more && (r1[t] - r0[t]) > kBottomUpLongList;
+        const bool longlist = more && (r1[t] - r0[t]) > p.bu_long;
         bool scan = more && !longlist;
         int e = r0[t] + K;
         while (__any_sync(0xffffffffu, scan)) {
@@ -733,7 +732,7 @@ __device__ __forceinline__ void bottom_up_lanes(const BfsParams &p, const uint32
 
 // Bottom-up continuation with the warp's pending lists in a queue: the lists
 // (slot t, lane) still without a parent after the first probes, of length in
-// (MIN_LEN, kBottomUpLongList], are listed in the warp's region of q_lo / q_hi
+// (MIN_LEN, p.bu_long], are listed in the warp's region of q_lo / q_hi
 // (next position, end; 32 * PER entries per warp) and handed out to lanes as
 // they become free, so a warp keeps 32 scans in flight until its queue is
 // empty instead of waiting for the longest list of each slot in turn; each
@@ -755,7 +754,7 @@ __device__ __forceinline__ void bottom_up_queue(const BfsParams &p, const uint32
 #pragma unroll
     for (int t = 0; t < PER; t++) {
         const int len = r1[t] - r0[t];
-        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= kBottomUpLongList;
+        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= p.bu_long;
         const unsigned bal = __ballot_sync(0xffffffffu, pend);
         if (pend) {
             const int i = n + __popc(bal & lanemask_lt());
@@ -801,7 +800,7 @@ __device__ __forceinline__ void bottom_up_queue(const BfsParams &p, const uint32
 #pragma unroll
     for (int t = 0; t < PER; t++) {
         const int len = r1[t] - r0[t];
-        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= kBottomUpLongList;
+        const bool pend = todo[t] && parent[t] < 0 && len > MIN_LEN && len <= p.bu_long;
         const unsigned bal = __ballot_sync(0xffffffffu, pend);
         if (pend) parent[t] = q_par[n + __popc(bal & lanemask_lt())];
         n += __popc(bal);
@@ -809,7 +808,7 @@ __device__ __forceinline__ void bottom_up_queue(const BfsParams &p, const uint32
     // long lists: the whole warp, one list at a time
 #pragma unroll
     for (int t = 0; t < PER; t++) {
-        const bool longlist = todo[t] && parent[t] < 0 && r1[t] - r0[t] > kBottomUpLongList;
+        const bool longlist = todo[t] && parent[t] < 0 && r1[t] - r0[t] > p.bu_long;
         unsigned lmask = __ballot_sync(0xffffffffu, longlist);
         while (lmask) {
             const int owner = __ffs(lmask) - 1;
@@ -1497,7 +1496,9 @@ constexpr unsigned long long kDeferMinShare = 512;
 // p.small_edges edges is processed by CTA 0 alone, separated by CTA-level
 // barriers only, while the other CTAs wait at the grid barrier; while those
 // levels fit one sub-round their frontier stays in shared memory.
-template <int B, bool PRED, bool LISTS, bool SUBGRID = false>
+// BU = false builds a top-down-only variant (plain expand-contract searches):
+// without the bottom-up code the kernel needs fewer registers.
+template <int B, bool PRED, bool LISTS, bool SUBGRID = false, bool BU = true>
 __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1523,7 +1524,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             limit_hit = true;
             break;
         }
-        if (s.prev_bu == 2 &&
+        if (BU && s.prev_bu == 2 &&
             ((p.persistent && s.E <= p.small_edges) || !choose_bottom_up(p, true, s.q, s.E, s.visited_edges))) {
             // the previous level ran bottom-up and only counted its discoveries:
             // this top-down level (or solo phase) reads them as a vertex frontier
@@ -1644,7 +1645,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
         // (a kernel variant of its own: the code would cost the other paths registers)
         if (SUBGRID && p.persistent && p.subgrid_edges > 0 && s.E <= p.subgrid_edges &&
             (int)gridDim.x >= 4 * kSubgridCtas &&
-            !choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges)) {
+            !(BU && choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges))) {
             // ---- mid-size top-down levels: the first kSubgridCtas CTAs, level after
             // level, with a barrier of their own; the others wait at the grid barrier
             if ((int)blockIdx.x < kSubgridCtas) {
@@ -1669,7 +1670,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
                         s.solo_stop = s.q == 0 || s.E > p.subgrid_edges || s.E <= p.small_edges ||
                                       (dl >= 0 && level >= dl) || sub + 1 >= kSoloLevelCap ||
                                       ld_cg(&p.st->error) != 0 ||
-                                      choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
+                                      (BU && choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges));
                     __syncthreads();
                     if (s.solo_stop) break;
                     if (tid == 0 && blockIdx.x == 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
@@ -1682,7 +1683,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
             sub_phase++;
             continue;
         }
-        const bool bu = choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
+        const bool bu = BU && choose_bottom_up(p, s.prev_bu != 0, s.q, s.E, s.visited_edges);
         // a bottom-up level counts its discoveries instead of emitting them, unless
         // the edges still unvisited (a bound on the next frontier's) are so few that
         // emitting them costs less than building the frontier from the masks later

@@ -98,7 +98,7 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
     if ((rc = begin_instrumented(p))) return rc;
-    const int init_blocks = std::max(1, std::min<int>(p->sms * 8, (int)(((long long)p->nodes * k + 255) / 256)));
+    const int init_blocks = std::max(1, std::min<int>(p->sms * 8, (int)(((long long)p->nodes + 255) / 256)));
     dev::msbfs_init_kernel<<<init_blocks, kThreads, 0, p->stream>>>(bp, m);
     CUDA_TRY(cudaGetLastError(), "batch init launch");
     dev::msbfs_seed_kernel<<<1, 32, 0, p->stream>>>(bp, m, p->d_ms_src, seed);

@@ -33,9 +33,13 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
     // fused searches with a sub-grid threshold run the variant that carries the
     // sub-grid phase (not combined with list mode)
     const bool subgrid_kernel = !lists_kernel && mode == B40C_ENACT_FUSED && pol.subgrid_frontier_edges > 0;
+    // plain expand-contract searches (and directed graphs) never go bottom-up:
+    // they run the top-down-only variants
     const void *kern = lists_kernel     ? (const void *)dev::ec_kernel<kThreads, false, true>
-                       : subgrid_kernel ? (const void *)dev::ec_kernel<kThreads, PRED, false, true>
-                                        : (const void *)dev::ec_kernel<kThreads, PRED, false>;
+                       : subgrid_kernel ? (direction_opt ? (const void *)dev::ec_kernel<kThreads, PRED, false, true>
+                                                         : (const void *)dev::ec_kernel<kThreads, PRED, false, true, false>)
+                       : direction_opt  ? (const void *)dev::ec_kernel<kThreads, PRED, false>
+                                        : (const void *)dev::ec_kernel<kThreads, PRED, false, false, false>;
     const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;

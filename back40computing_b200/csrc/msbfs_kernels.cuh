@@ -218,7 +218,9 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             const bool inr = v < re;
             unsigned long long vold = 0, missing = 0;
             int r0 = 0, r1 = 0;
-            if (inr) {
+            // vertices without edges are never reached (their labels are set at the end)
+            const bool iso = inr && p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u);
+            if (inr && !iso) {
                 vold = ld_cg64(m.visited + v);
                 missing = active & ~vold;
                 if (missing) {
@@ -378,22 +380,42 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
         }
         if (!duty.barrier(p.st, generation, &s_ok)) break;
     }
+    // The (source, vertex) pairs no level reached get label -1 here; every
+    // other label was written by the level that reached the pair, so each
+    // entry is written once (no fill of the k label rows before the search).
+    // The loop above ends after a grid barrier, so every level's writes are done.
+    {
+        const unsigned long long kmask = m.k >= 64 ? ~0ull : ((1ull << m.k) - 1ull);
+        const int lane = tid & 31;
+        const long long n = p.nodes, warps = (long long)gridDim.x * (B / 32);
+        for (long long vb = ((long long)blockIdx.x * (B / 32) + (tid >> 5)) * 32; vb < n; vb += warps * 32) {
+            const long long v = vb + lane;
+            const unsigned long long miss = v < n ? ~ld_cg64(m.visited + v) & kmask : 0ull;
+            const unsigned lo = __reduce_or_sync(0xffffffffu, (unsigned)(miss & 0xffffffffull));
+            const unsigned hi = __reduce_or_sync(0xffffffffu, (unsigned)(miss >> 32));
+            unsigned long long wor = ((unsigned long long)hi << 32) | lo;
+            while (wor) {
+                const int src = __ffsll((long long)wor) - 1;
+                wor &= wor - 1;
+                if ((miss >> src) & 1ull) m.labels[(long long)src * n + v] = -1;
+            }
+        }
+    }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
     duty.finish();
     if (tid == 0 && blockIdx.x == 0) p.st->done = 1;
 }
 
-// Batch set-up: labels <- -1, masks <- 0 (grid-stride) and the search state.
+// Batch set-up: masks <- 0 (grid-stride) and the search state.  The label
+// rows are not filled: the search writes every entry once (reached pairs by
+// their level, the rest at its end).
 template <int DUMMY = 0>
 __global__ void msbfs_init_kernel(BfsParams p, MsParams m)
 {
     const long long stride = (long long)gridDim.x * blockDim.x;
     const long long t0 = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = (long long)m.k * p.nodes;
-    for (long long i = t0; i < total; i += stride) m.labels[i] = -1;
     for (long long v = t0; v < p.nodes; v += stride) {
-        // vertices without edges count as visited by every source: pull levels skip them
-        m.visited[v] = (p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u)) ? ~0ull : 0ull;
+        m.visited[v] = 0;
         m.fmask[0][v] = 0;
         m.fmask[1][v] = 0;
     }

@@ -8,6 +8,14 @@
  * are kept.  Random numbers come from libc rand() in the reference's order
  * (one draw per quadrant choice, then per parameter a sign draw and a
  * magnitude draw), so the same srand() seed gives the same graph.
+ *
+ * One difference: the walk starts at id 1, so a walk that takes the last
+ * quadrant's half at every level ends at id `nodes`, one past the last vertex
+ * (the reference keeps it: its CSR then ends short of `edges` and indexes past
+ * its arrays).  Such an id wraps to 0 here, as in the library's native
+ * builder, so every graph is a valid CSR.  It happens about once per
+ * (c + d)^log2(nodes) draws: never in practice at the Graph500 parameters
+ * (.57/.19/.19), now and then at the GTGraph defaults (.45/.15/.15).
  */
 #pragma once
 #include "utils.cuh"
@@ -77,6 +85,8 @@ int BuildRmatGraph(SizeT nodes, SizeT edges, CsrGraph<VertexId, Value, SizeT> &c
             ChoosePartition(&u, &v, step, a, b, c, d);
             VaryParams(&a, &b, &c, &d);
         }
+        if (u == (VertexId)nodes) u = 0;
+        if (v == (VertexId)nodes) v = 0;
         coo[i] = EdgeTupleType(u, v, 1);
         if (undirected) coo[edges + i] = EdgeTupleType(v, u, 1);
     }

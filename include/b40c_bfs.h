@@ -17,8 +17,12 @@
  *  - A handle is used by one host thread at a time; its work is ordered on
  *    the handle's CUDA stream (b40c_bfs_set_stream), default: a stream the
  *    handle creates.
- *  - Vertex ids, row offsets and labels are int32 (the reference's
- *    VertexId = SizeT = int for every graph type its driver builds).
+ *  - Vertex ids, row offsets and labels are int32 on the device (the
+ *    reference driver's graphs use SizeT = int; its one 64-bit VertexId graph
+ *    type, "g500", is narrowed to int32 ids by the C++ CsrProblem).
+ *  - b40c_bfs_policy grows at its end between versions: callers pass the
+ *    struct of the header they were built with, so rebuild against this
+ *    header (a caller built against an older one passes a shorter struct).
  */
 #ifndef B40C_BFS_H
 #define B40C_BFS_H
@@ -115,6 +119,10 @@ typedef struct b40c_bfs_policy {
                                       small_frontier_edges and at most this many edges run on 16 CTAs
                                       with a barrier of their own while the rest of the grid waits (the
                                       mid-size levels of high-diameter graphs); -1 = off (default) */
+    int32_t bottom_up_long_list;   /* bottom-up levels: a vertex whose list is longer than this (and whose
+                                      first probes found no parent) is searched by its whole warp, 32
+                                      neighbours at a time; shorter lists are scanned by one lane, four at
+                                      a time (>= 4; 0 = default 256) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */
