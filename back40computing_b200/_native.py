@@ -92,7 +92,8 @@ class ServerOptions(C.Structure):
         ("max_batch", C.c_int32),
         ("single_strategy", C.c_int32),
         ("max_in_flight", C.c_int32),
-        ("reserved", C.c_int32 * 5),
+        ("ctas_per_sm", C.c_int32),
+        ("reserved", C.c_int32 * 4),
     ]
 
 
@@ -108,12 +109,15 @@ class ServerResult(C.Structure):
         ("arrival_ns", C.c_int64),
         ("launch_ns", C.c_int64),
         ("finish_ns", C.c_int64),
+        ("gpu_start_ns", C.c_int64),
+        ("gpu_end_ns", C.c_int64),
     ]
 
 
 SERVER_RESULT_DTYPE = np.dtype([("ticket", "<i8"), ("graph", "<i4"), ("source", "<i4"), ("depth_limit", "<i4"),
                                 ("status", "<i4"), ("search_depth", "<i4"), ("batch_size", "<i4"),
-                                ("arrival_ns", "<i8"), ("launch_ns", "<i8"), ("finish_ns", "<i8")])
+                                ("arrival_ns", "<i8"), ("launch_ns", "<i8"), ("finish_ns", "<i8"),
+                                ("gpu_start_ns", "<i8"), ("gpu_end_ns", "<i8")])
 
 
 class ServerCounters(C.Structure):
@@ -127,7 +131,8 @@ class ServerCounters(C.Structure):
         ("memory_used_bytes", C.c_int64),
         ("memory_budget_bytes", C.c_int64),
         ("graphs", C.c_int32),
-        ("reserved", C.c_int32 * 3),
+        ("reserved", C.c_int32),
+        ("joined_queries", C.c_int64),
     ]
 
 
@@ -169,6 +174,8 @@ SIGNATURES: dict[str, tuple] = {
     "b40c_bfs_device_view_get": (C.c_int, [C.c_void_p, C.POINTER(DeviceView)]),
     "b40c_msbfs_enact": (C.c_int, [C.c_void_p, _P_i32, _P_i32, C.c_int, C.c_int, C.POINTER(Policy)]),
     "b40c_msbfs_extract": (C.c_int, [C.c_void_p, C.c_int, _P_i32]),
+    "b40c_msbfs_join": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, C.c_int32]),
+    "b40c_msbfs_joined": (C.c_int, [C.c_void_p, _P_i32, _P_i32]),
     "b40c_msbfs_stats": (C.c_int, [C.c_void_p, _P_i32]),
     "b40c_bfs_problem_device_bytes": (C.c_int, [C.c_void_p, C.POINTER(C.c_int64)]),
     "b40c_msbfs_device_labels": (C.c_int, [C.c_void_p, C.POINTER(C.c_void_p), _P_i32]),

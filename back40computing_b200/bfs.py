@@ -173,6 +173,18 @@ class CsrProblem:
                                          int(src.size), int(max_grid_size), pol), "msbfs")
         self._ms_k = int(src.size)
 
+    def msbfs_join(self, slot: int, source: int, depth_limit: int = -1) -> None:
+        """Adds `source` in slot `slot` to the batch in flight (taken at its next
+        level boundary; see msbfs_joined)."""
+        N.check(N.lib().b40c_msbfs_join(self.handle, int(slot), int(source), int(depth_limit)), "b40c_msbfs_join")
+
+    def msbfs_joined(self) -> tuple[int, np.ndarray]:
+        """(join requests the last batch took, every slot's search depth [64])."""
+        taken = C.c_int32(0)
+        depths = np.zeros(64, np.int32)
+        N.check(N.lib().b40c_msbfs_joined(self.handle, C.byref(taken), N.i32p(depths)), "b40c_msbfs_joined")
+        return taken.value, depths
+
     def labels_of(self, slot: int) -> np.ndarray:
         """Labels of source `slot` of the last batch."""
         out = np.empty(self.nodes, dtype=np.int32)

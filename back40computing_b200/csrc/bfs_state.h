@@ -104,6 +104,19 @@ constexpr int kMaxArriveCtas = 2048;
 constexpr int kPhaseStamps = 8;
 constexpr int kPhaseArrive = 7;
 
+// Sources added to a batched search while it runs (b40c_msbfs_join): the
+// host copies request j into src/slot/limit[j] and then raises `count`; at
+// the end of each level block 0 takes the requests up to count, seeds them as
+// sources of the next level and sets `taken`.  A slot's labels count from the
+// level it was seeded at, so they are the distances of a search from that
+// source alone.  Device memory, reset by the batch's seed kernel.
+struct MsJoin {
+    int32_t count;              // requests written by the host
+    int32_t taken;              // requests the search has taken (block 0)
+    unsigned long long used;    // slots in use: the batch's k plus the joined ones
+    int32_t src[64], slot[64], limit[64];
+};
+
 // Kernel parameter block.
 struct BfsParams {
     const int32_t *row_offsets;

@@ -20,11 +20,23 @@ void free_batch(b40c_bfs_problem *p)
     if (p->d_ms_labels) cudaFree(p->d_ms_labels);
     if (p->d_ms_src) cudaFree(p->d_ms_src);
     if (p->d_ms_depth) cudaFree(p->d_ms_depth);
+    if (p->d_ms_off) cudaFree(p->d_ms_off);
+    if (p->join_stream) cudaStreamSynchronize(p->join_stream);
+    if (p->d_ms_join) cudaFree(p->d_ms_join);
+    if (p->h_ms_join) cudaFreeHost(p->h_ms_join);
+    if (p->h_ms_seq) cudaFreeHost(p->h_ms_seq);
+    p->h_ms_seq = nullptr;
+    if (p->ms_seeded_ev) cudaEventDestroy(p->ms_seeded_ev);
+    if (p->join_stream) cudaStreamDestroy(p->join_stream);
     p->d_ms_visited = nullptr;
     p->d_ms_fmask[0] = p->d_ms_fmask[1] = nullptr;
     p->d_ms_labels = nullptr;
     p->d_ms_src = nullptr;
     p->d_ms_depth = nullptr;
+    p->d_ms_off = nullptr;
+    p->d_ms_join = p->h_ms_join = nullptr;
+    p->ms_seeded_ev = nullptr;
+    p->join_stream = nullptr;
     p->ms_labels_k = 0;
 }
 
@@ -39,6 +51,14 @@ int ensure_batch(b40c_bfs_problem *p, int k)
                 return rc;
         if ((rc = alloc_dev((void **)&p->d_ms_src, sizeof(int32_t) * 64, "batch depth limits"))) return rc;
         if ((rc = alloc_dev((void **)&p->d_ms_depth, sizeof(int32_t) * 64, "batch search depths"))) return rc;
+        if ((rc = alloc_dev((void **)&p->d_ms_off, sizeof(int32_t) * 64, "batch level offsets"))) return rc;
+        if ((rc = alloc_dev((void **)&p->d_ms_join, sizeof(MsJoin), "batch join requests"))) return rc;
+        CUDA_TRY(cudaMallocHost((void **)&p->h_ms_join, sizeof(MsJoin)), "pinned join requests");
+        memset(p->h_ms_join, 0, sizeof(MsJoin));
+        CUDA_TRY(cudaMallocHost((void **)&p->h_ms_seq, sizeof(int32_t) * 65), "pinned join counts");
+        for (int i = 0; i <= 64; i++) p->h_ms_seq[i] = i;
+        CUDA_TRY(cudaStreamCreateWithFlags(&p->join_stream, cudaStreamNonBlocking), "join stream");
+        CUDA_TRY(cudaEventCreateWithFlags(&p->ms_seeded_ev, cudaEventDisableTiming), "event");
     }
     if (p->ms_labels_k < k) {
         if (p->d_ms_labels) cudaFree(p->d_ms_labels);
@@ -90,7 +110,10 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     m.labels = p->d_ms_labels;
     m.depth_limit = p->d_ms_src;
     m.depth = p->d_ms_depth;
+    m.level_off = p->d_ms_off;
+    m.join = p->d_ms_join;
     m.k = k;
+    m.rows = p->ms_labels_k;
     m.pull_ok = p->symmetric == 1 ? 1 : 0;
     const void *kern = (const void *)dev::msbfs_kernel<kThreads>;
     const size_t smem = sizeof(dev::MsSmem<kThreads>);
@@ -98,11 +121,18 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
     if ((rc = begin_instrumented(p))) return rc;
+    // join requests still being copied for an earlier batch land before this
+    // batch's seed kernel resets the request block, and their pinned staging
+    // entries are read before this batch's requests rewrite them
+    if (p->ms_joins > 0) CUDA_TRY(cudaStreamSynchronize(p->join_stream), "join copies");
     const int init_blocks = std::max(1, std::min<int>(p->sms * 8, (int)(((long long)p->nodes + 255) / 256)));
     dev::msbfs_init_kernel<<<init_blocks, kThreads, 0, p->stream>>>(bp, m);
     CUDA_TRY(cudaGetLastError(), "batch init launch");
-    dev::msbfs_seed_kernel<<<1, 32, 0, p->stream>>>(bp, m, p->d_ms_src, seed);
+    dev::msbfs_seed_kernel<<<1, 32, 0, p->stream>>>(bp, m, seed);
     CUDA_TRY(cudaGetLastError(), "batch seed launch");
+    // requests for this batch are copied only after its seed kernel
+    CUDA_TRY(cudaEventRecord(p->ms_seeded_ev, p->stream), "event record");
+    p->ms_joins = 0;
     if ((rc = mark_search_start(p))) return rc;
     void *args[] = {&bp, &m};
     CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream),
@@ -140,11 +170,68 @@ int b40c_msbfs_enact(b40c_bfs_problem *p, const int32_t *sources, const int32_t 
     return enact_batch(p, sources, depth_limits, k, max_grid_size, pol);
 }
 
+int b40c_msbfs_join(b40c_bfs_problem *p, int32_t slot, int32_t source, int32_t depth_limit)
+{
+    b40c::clear_error();
+    if (!p) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null problem");
+    if (p->ms_k < 1 || !p->d_ms_join) return b40c::fail(B40C_ERROR_NOT_READY, "no batch has been enacted");
+    if (source < 0 || source >= p->nodes) return b40c::fail(B40C_ERROR_INVALID_VALUE, "source %d out of range", source);
+    if (slot < p->ms_k || slot >= std::min(64, (int)p->ms_labels_k))
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "join slot %d: must be in [%d, %d) (the batch's k .. label rows)",
+                          slot, p->ms_k, std::min(64, (int)p->ms_labels_k));
+    if (p->ms_joins >= 64) return b40c::fail(B40C_ERROR_INVALID_VALUE, "at most 64 join requests per batch");
+    DeviceGuard guard(p->device);
+    // request j's pinned staging entries are written once per batch (the next
+    // batch waits for these copies before rewriting them) and the count comes
+    // from a constant table, so no copy reads a value changed after it was issued
+    MsJoin *h = p->h_ms_join;
+    const int j = p->ms_joins;
+    h->src[j] = source;
+    h->slot[j] = slot;
+    h->limit[j] = depth_limit < 0 ? -1 : depth_limit;
+    CUDA_TRY(cudaStreamWaitEvent(p->join_stream, p->ms_seeded_ev, 0), "stream wait");
+    // the request first, then the count that makes it visible (stream order)
+    CUDA_TRY(cudaMemcpyAsync(&p->d_ms_join->src[j], &h->src[j], sizeof(int32_t), cudaMemcpyHostToDevice,
+                             p->join_stream),
+             "join request copy");
+    CUDA_TRY(cudaMemcpyAsync(&p->d_ms_join->slot[j], &h->slot[j], sizeof(int32_t), cudaMemcpyHostToDevice,
+                             p->join_stream),
+             "join request copy");
+    CUDA_TRY(cudaMemcpyAsync(&p->d_ms_join->limit[j], &h->limit[j], sizeof(int32_t), cudaMemcpyHostToDevice,
+                             p->join_stream),
+             "join request copy");
+    CUDA_TRY(cudaMemcpyAsync(&p->d_ms_join->count, p->h_ms_seq + j + 1, sizeof(int32_t), cudaMemcpyHostToDevice,
+                             p->join_stream),
+             "join count copy");
+    p->ms_joins = j + 1;
+    return B40C_SUCCESS;
+}
+
+int b40c_msbfs_joined(b40c_bfs_problem *p, int32_t *taken, int32_t *search_depths)
+{
+    b40c::clear_error();
+    if (!p || !taken) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
+    if (p->ms_k < 1 || !p->d_ms_join) return b40c::fail(B40C_ERROR_NOT_READY, "no batch has run");
+    DeviceGuard guard(p->device);
+    int rc = read_state(p);
+    if (rc) return rc;
+    if ((rc = check_state_errors(p))) return rc;
+    CUDA_TRY(cudaMemcpyAsync(taken, &p->d_ms_join->taken, sizeof(int32_t), cudaMemcpyDeviceToHost, p->stream),
+             "join count read");
+    if (search_depths)
+        CUDA_TRY(cudaMemcpyAsync(search_depths, p->d_ms_depth, sizeof(int32_t) * 64, cudaMemcpyDeviceToHost, p->stream),
+                 "batch depth copy");
+    CUDA_TRY(cudaStreamSynchronize(p->stream), "join read synchronize");
+    return B40C_SUCCESS;
+}
+
 int b40c_msbfs_extract(b40c_bfs_problem *p, int slot, int32_t *h_labels)
 {
     b40c::clear_error();
     if (!p || !h_labels) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
-    if (slot < 0 || slot >= p->ms_k) return b40c::fail(B40C_ERROR_INVALID_VALUE, "no source %d in the last batch", slot);
+    // slots past k hold the sources that joined the batch (b40c_msbfs_join)
+    if (slot < 0 || slot >= std::max(p->ms_k, std::min(64, (int)p->ms_labels_k)))
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "no source %d in the last batch", slot);
     DeviceGuard guard(p->device);
     int rc = read_state(p);
     if (rc) return rc;

@@ -29,10 +29,13 @@ namespace dev {
 struct MsParams {
     unsigned long long *visited;     // V[n]
     unsigned long long *fmask[2];    // F[2][n]
-    int32_t *labels;                 // [k][n], source-major
-    const int32_t *depth_limit;      // [k]; < 0 unlimited
-    int32_t *depth;                  // [k]; search depth of each source (max label + 1)
+    int32_t *labels;                 // [rows][n], source-major
+    int32_t *depth_limit;            // [64]; < 0 unlimited
+    int32_t *depth;                  // [64]; search depth of each source (max label + 1)
+    int32_t *level_off;              // [64]; level at which each slot's source was seeded
+    MsJoin *join;                    // sources joining the running batch (null: none)
     int32_t k;
+    int32_t rows;                    // label rows allocated (joined slots must be below)
     int32_t pull_ok;                 // 1: the graph is symmetric, dense levels may pull
 };
 
@@ -44,6 +47,9 @@ struct MsSmem {
     uint16_t own[kChunkMax];
     int32_t out[kChunkMax];
     int32_t limits[64];
+    int32_t off[64];                 // level_off of each slot
+    int32_t jn0, jn1;                // join requests taken at this level end: [jn0, jn1)
+    unsigned long long used;         // slots in use
     int32_t out_count;
     int32_t flag;
     int32_t q, E;
@@ -149,7 +155,7 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
                 while (bits) {
                     const int src = __ffsll((long long)bits) - 1;
                     bits &= bits - 1;
-                    m.labels[(long long)src * n + w[t]] = level + 1;
+                    m.labels[(long long)src * n + w[t]] = level + 1 - s.off[src];
                 }
                 first[t] = atomicOr(fnext + w[t], set[t]) == 0ull;
             }
@@ -277,7 +283,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             while (wor) {
                 const int src = __ffsll((long long)wor) - 1;
                 wor &= wor - 1;
-                if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1;
+                if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1 - s.off[src];
             }
             const bool push = acc && r1 > r0;
             const unsigned bal = __ballot_sync(0xffffffffu, push);
@@ -300,6 +306,74 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
     }
 }
 
+// Block 0, between the grid barriers that end level `level` (no CTA touches the
+// masks or the next frontier then): takes the join requests the host has
+// raised since the last level end and seeds each as a source of level + 1 --
+// label 0 in its slot's row, its visited bit, its bit in the next frontier
+// mask and, if no other source put it there, an entry in the next frontier
+// queue (emitted like any discovery, so the level's counters include it).
+template <int B>
+__device__ __forceinline__ void take_joins(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
+                                           const VertexFrontier &vout, unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x, lane = tid & 31;
+    if (tid == 0) {
+        const int c = min((int)ld_acquire((const unsigned *)&m.join->count), 64);
+        const int t = m.join->taken;  // written by block 0 only
+        s.jn0 = t;
+        s.jn1 = max(c, t);
+        s.out_count = 0;
+    }
+    __syncthreads();
+    const int t0 = s.jn0, t1 = s.jn1;
+    if (t1 == t0) return;  // CTA-uniform
+    unsigned long long *fnext = m.fmask[(level + 1) & 1];
+    const long long n = p.nodes;
+    for (int jb = t0; jb < t1; jb += B) {
+        const int j = jb + tid;
+        bool push = false;
+        int v = 0, r0 = 0, r1 = 0;
+        if (j < t1) {
+            v = ld_cg(&m.join->src[j]);
+            const int slot = ld_cg(&m.join->slot[j]);
+            if (v >= 0 && v < p.nodes && slot >= 0 && slot < min(m.rows, 64)) {  // checked by the host too
+                const unsigned long long bit = 1ull << slot;
+                m.depth_limit[slot] = ld_cg(&m.join->limit[j]);
+                m.level_off[slot] = level + 1;
+                m.depth[slot] = 1;
+                m.labels[(long long)slot * n + v] = 0;
+                atomicOr(m.visited + v, bit);
+                atomicOr(&m.join->used, bit);
+                if (atomicOr(fnext + v, bit) == 0ull) {  // not yet in the next frontier
+                    r0 = ld_ro(p.row_offsets + v);
+                    r1 = ld_ro(p.row_offsets + v + 1);
+                    push = r1 > r0;
+                }
+            }
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, push);
+        if (bal) {
+            const int leader = __ffs(bal) - 1;
+            int base = 0;
+            if (lane == leader) base = atomicAdd(&s.out_count, __popc(bal));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (push) {
+                const int slot_i = base + __popc(bal & lanemask_lt());
+                s.out[slot_i] = v;
+                s.colstart[slot_i] = r0;
+                s.rel[slot_i] = r1 - r0;
+            }
+        }
+    }
+    __syncthreads();
+    emit_frontier<B>(p, s, level, vout, qe_out);
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        m.join->taken = t1;
+    }
+}
+
 // Whole batched search in one persistent cooperative grid.
 template <int B>
 __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
@@ -308,13 +382,18 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
     MsSmem<B> &s = *reinterpret_cast<MsSmem<B> *>(smem_raw);
     __shared__ int s_ok;
     const int tid = threadIdx.x;
-    if (tid < 64) s.limits[tid] = tid < m.k ? m.depth_limit[tid] : 0;
     unsigned generation = 0;
     int max_level_seen = -1;
     DutyClock duty(p);
-    __syncthreads();
     for (int level = 0;; level++) {
         const int pass = level;
+        // the slots' depth limits and level offsets (sources may have joined at the last level end)
+        if (tid < 64) {
+            s.limits[tid] = ld_cg(m.depth_limit + tid);
+            s.off[tid] = ld_cg(m.level_off + tid);
+        }
+        if (tid == 0) s.used = m.join ? ld_cg64(&m.join->used) : (m.k >= 64 ? ~0ull : ((1ull << m.k) - 1ull));
+        __syncthreads();
         if (tid == 0) {
             const unsigned long long x = ld_cg64(&p.st->qe[pass % 3]);
             s.q = qe_count(x);
@@ -326,8 +405,9 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             }
             s.found = 0;
             unsigned long long act = 0;
-            for (int src = 0; src < m.k; src++)
-                if (s.limits[src] < 0 || level < s.limits[src]) act |= 1ull << src;
+            for (int src = 0; src < 64; src++)
+                if (((s.used >> src) & 1ull) && (s.limits[src] < 0 || level - s.off[src] < s.limits[src]))
+                    act |= 1ull << src;
             s.active = act;
             if (blockIdx.x == 0) {
                 p.st->qe[(pass + 2) % 3] = 0;
@@ -368,7 +448,7 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             while (bits) {
                 const int src = __ffsll((long long)bits) - 1;
                 bits &= bits - 1;
-                atomicMax(m.depth + src, level + 2);
+                atomicMax(m.depth + src, level + 2 - s.off[src]);
             }
         }
         if (!duty.barrier(p.st, generation, &s_ok)) break;
@@ -378,6 +458,7 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             unsigned long long *fcur = m.fmask[level & 1];
             for (int i = blockIdx.x * B + tid; i < s.q; i += gridDim.x * B) fcur[ld_cg(in.v + i)] = 0ull;
         }
+        if (m.join && blockIdx.x == 0) take_joins<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
         if (!duty.barrier(p.st, generation, &s_ok)) break;
     }
     // The (source, vertex) pairs no level reached get label -1 here; every
@@ -385,7 +466,8 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
     // entry is written once (no fill of the k label rows before the search).
     // The loop above ends after a grid barrier, so every level's writes are done.
     {
-        const unsigned long long kmask = m.k >= 64 ? ~0ull : ((1ull << m.k) - 1ull);
+        const unsigned long long kmask =
+            m.join ? ld_cg64(&m.join->used) : (m.k >= 64 ? ~0ull : ((1ull << m.k) - 1ull));
         const int lane = tid & 31;
         const long long n = p.nodes, warps = (long long)gridDim.x * (B / 32);
         for (long long vb = ((long long)blockIdx.x * (B / 32) + (tid >> 5)) * 32; vb < n; vb += warps * 32) {
@@ -446,12 +528,18 @@ struct MsSeed {
 // masks and search depths, and the level-0 frontier queue of the distinct
 // source vertices; one thread.
 template <int DUMMY = 0>
-__global__ void msbfs_seed_kernel(BfsParams p, MsParams m, int32_t *limits_out, MsSeed seed)
+__global__ void msbfs_seed_kernel(BfsParams p, MsParams m, MsSeed seed)
 {
     if (threadIdx.x == 0) {
-        for (int s = 0; s < m.k; s++) {
-            limits_out[s] = seed.limit[s];
+        for (int s = 0; s < 64; s++) {
+            m.depth_limit[s] = s < m.k ? seed.limit[s] : 0;
+            m.level_off[s] = 0;
             m.depth[s] = 1;
+        }
+        if (m.join) {
+            m.join->count = 0;
+            m.join->taken = 0;
+            m.join->used = m.k >= 64 ? ~0ull : ((1ull << m.k) - 1ull);
         }
         int g = 0, d = 0;
         for (int i = 0; i < seed.n_distinct; i++) {

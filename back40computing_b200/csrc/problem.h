@@ -53,7 +53,16 @@ struct b40c_bfs_problem {
     int32_t ms_labels_k = 0;       // sources the label array is sized for
     int32_t *d_ms_src = nullptr;   // [64] depth limit of each source slot
     int32_t *d_ms_depth = nullptr; // [64] search depth of each source slot
+    int32_t *d_ms_off = nullptr;   // [64] level at which each slot's source was seeded
     int32_t ms_k = 0;              // sources of the last batch
+    // sources joining the batch in flight (b40c_msbfs_join): the device request
+    // block, its pinned host staging, the stream the requests are copied on and
+    // the event after which they may be (the batch's seed kernel)
+    b40c::MsJoin *d_ms_join = nullptr, *h_ms_join = nullptr;
+    int32_t *h_ms_seq = nullptr;   // pinned 0..64: request counts copied from here (never rewritten)
+    cudaStream_t join_stream = nullptr;
+    cudaEvent_t ms_seeded_ev = nullptr;
+    int32_t ms_joins = 0;          // requests sent to the batch in flight
     // instrumentation (per-pass records, CTA duty)
     bool instrument = false;
     b40c::LevelRecord *d_levels = nullptr;

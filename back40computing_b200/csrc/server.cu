@@ -1,19 +1,24 @@
 // BFS query server: resident graphs, continuous batching, a device-memory
 // budget (include/b40c_server.h).
 //
-// One dispatcher thread owns all GPU work of a server.  Its loop:
+// One dispatcher thread owns all GPU work of a server.  Each in-flight slot
+// has a CUDA stream of its own, so batches of different graphs (and the label
+// read-back of one with the search of another) overlap on the device; a
+// batch's persistent grid takes a share of every SM (ctas_per_sm), so several
+// grids are resident side by side.  The dispatcher's loop:
 //   1. queries whose arrival time has come move from the arrival heap to their
 //      graph's FIFO;
-//   2. finished batches are retired in issue order (one CUDA stream, so they
-//      finish in that order): results, latencies, labels already copied;
-//   3. while fewer than max_in_flight batches are queued and some graph with
-//      waiting queries has no batch in flight, the graph whose oldest waiting
-//      query arrived first gets a batch of up to its width: the batched kernel
-//      for two or more queries, the plain search for one;
+//   2. finished batches (any slot, in whatever order they finish) are retired:
+//      results, latencies, labels already copied;
+//   3. while a slot is free and some graph with waiting queries has no batch in
+//      flight, the graph whose oldest waiting query arrived first gets a batch
+//      of up to its width on that slot's stream: the batched kernel for two or
+//      more queries, the plain search for one;
 //   4. it spins (yielding) while batches are in flight, otherwise sleeps until
 //      the next arrival or a submit.
 // Queries for a graph that already has a batch in flight wait and gather into
-// its next batch: that is the continuous batching.
+// its next batch: that is the continuous batching.  Removing a graph returns
+// its bytes to the budget and widens the other graphs' batches again.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -72,11 +77,14 @@ struct Landing {
     int32_t depth[64];
     uint32_t error;
     int32_t max_level;
+    int32_t taken;  // join requests the batched search took
 };
 
 struct Batch {
     int graph;
-    std::vector<Query> queries;
+    std::vector<Query> queries;  // the batch's own k, then the ones sent to join it
+    std::vector<int64_t> join_ns;  // when each joining query was sent
+    int k = 0;                   // queries the batch was launched with
     bool single;
     int slot;
     int64_t launch_ns;
@@ -91,8 +99,9 @@ using namespace b40c::server;
 struct b40c_server {
     int device = 0;
     int32_t max_batch = 64, single_strategy = B40C_DIRECTION_OPTIMIZING, max_in_flight = 2;
+    int32_t ctas_per_sm = 0;  // of each batch's persistent grid (0: the policy's)
     int64_t budget = 0, used = 0;
-    cudaStream_t stream = nullptr;
+    cudaStream_t *streams = nullptr;  // [max_in_flight]: one per in-flight slot
     std::chrono::steady_clock::time_point t0;
     std::vector<Graph *> graphs;
     std::mutex mu;
@@ -103,8 +112,11 @@ struct b40c_server {
     std::deque<Batch> in_flight;
     Landing *landing = nullptr;               // [max_in_flight], page-locked
     cudaEvent_t *done_ev = nullptr;           // [max_in_flight]
+    cudaEvent_t *gpu_ev = nullptr;            // [2 * max_in_flight]: timing events around each slot's search
+    cudaEvent_t base_ev = nullptr;            // device-clock origin (recorded at creation)
     std::vector<int> free_slots;
     int64_t submitted = 0, completed = 0, failed = 0, batches = 0, batched_queries = 0, single_queries = 0;
+    int64_t joined_queries = 0;  // queries answered by joining a batch in flight
     bool stop = false;
     int thread_error = 0;
     std::thread worker;
@@ -117,19 +129,38 @@ struct b40c_server {
 
 namespace {
 
-// Marks every query of a batch finished (called with the lock held).
+// Marks the queries of a batch finished (called with the lock held): its own
+// and the joining ones the search took; joining queries it did not take go
+// back to the head of their graph's queue, in order.
 void finish_batch(b40c_server *s, Batch &b, int status, int64_t finish_ns)
 {
     Graph &g = *s->graphs[b.graph];
     const Landing &l = s->landing[b.slot];
+    const int joined = (int)b.queries.size() - b.k;
+    const int taken = (status == B40C_SUCCESS && joined > 0) ? std::max(0, std::min(joined, l.taken)) : 0;
+    if (status == B40C_SUCCESS && taken < joined) {
+        for (int i = (int)b.queries.size() - 1; i >= b.k + taken; i--) g.ready.push_front(b.queries[i]);
+        b.queries.resize(b.k + taken);
+    }
+    s->joined_queries += taken;
+    s->batched_queries += taken;
+    float t0 = 0.f, t1 = 0.f;
+    if (status == B40C_SUCCESS &&
+        (cudaEventElapsedTime(&t0, s->base_ev, s->gpu_ev[2 * b.slot]) != cudaSuccess ||
+         cudaEventElapsedTime(&t1, s->base_ev, s->gpu_ev[2 * b.slot + 1]) != cudaSuccess)) {
+        cudaGetLastError();
+        t0 = t1 = 0.f;
+    }
     for (size_t i = 0; i < b.queries.size(); i++) {
         const Query &q = b.queries[i];
         b40c_server_result &r = s->results[q.ticket];
         r.status = status;
         r.search_depth = status ? 0 : (b.single ? l.max_level + 1 : l.depth[i]);
         r.batch_size = (int32_t)b.queries.size();
-        r.launch_ns = b.launch_ns;
+        r.launch_ns = i < (size_t)b.k ? b.launch_ns : b.join_ns[i - b.k];
         r.finish_ns = finish_ns;
+        r.gpu_start_ns = (int64_t)((double)t0 * 1e6);
+        r.gpu_end_ns = (int64_t)((double)t1 * 1e6);
         g.pending--;
         s->completed++;
         if (status) s->failed++;
@@ -138,24 +169,40 @@ void finish_batch(b40c_server *s, Batch &b, int status, int64_t finish_ns)
     s->free_slots.push_back(b.slot);
 }
 
-// Issues one batch on the server stream (lock held; the calls only queue work).
+// The policy of one batch: the graph's (or the library default) with the
+// grid share of the server applied.
+const b40c_bfs_policy *batch_policy(const b40c_server *s, const Graph &g, bool single, b40c_bfs_policy *buf)
+{
+    const bool has = single ? g.has_single : g.has_batch;
+    if (!has && s->ctas_per_sm == 0) return nullptr;
+    *buf = has ? (single ? g.single : g.batch) : b40c_bfs_policy{};
+    if (s->ctas_per_sm > 0 && (buf->ctas_per_sm == 0 || buf->ctas_per_sm > s->ctas_per_sm))
+        buf->ctas_per_sm = s->ctas_per_sm;
+    return buf;
+}
+
+// Issues one batch on its slot's stream (lock held; the calls only queue work).
 int issue(b40c_server *s, Batch &b)
 {
     Graph &g = *s->graphs[b.graph];
     b40c_bfs_problem *p = g.p;
     Landing *l = s->landing + b.slot;
+    cudaStream_t st = s->streams[b.slot];
+    p->stream = st;  // a graph has at most one batch in flight: its buffers are this stream's alone
     const int k = (int)b.queries.size();
+    b40c_bfs_policy pol;
     int rc;
+    CUDA_TRY(cudaEventRecord(s->gpu_ev[2 * b.slot], st), "event record");
     if (b.single) {
         const Query &q = b.queries[0];
         rc = b40c_bfs_enact_limited(p, s->single_strategy, B40C_ENACT_FUSED, q.source, q.depth_limit, 0,
-                                    g.has_single ? &g.single : nullptr);
+                                    batch_policy(s, g, true, &pol));
         if (rc) return rc;
-        CUDA_TRY(cudaMemcpyAsync(&l->max_level, &p->st->max_level, sizeof(int32_t), cudaMemcpyDeviceToHost, s->stream),
+        CUDA_TRY(cudaEventRecord(s->gpu_ev[2 * b.slot + 1], st), "event record");
+        CUDA_TRY(cudaMemcpyAsync(&l->max_level, &p->st->max_level, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
                  "depth copy");
         if (q.h_labels)
-            CUDA_TRY(cudaMemcpyAsync(q.h_labels, p->d_labels, sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost,
-                                     s->stream),
+            CUDA_TRY(cudaMemcpyAsync(q.h_labels, p->d_labels, sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, st),
                      "label copy");
     } else {
         int32_t src[64], lim[64];
@@ -163,20 +210,62 @@ int issue(b40c_server *s, Batch &b)
             src[i] = b.queries[i].source;
             lim[i] = b.queries[i].depth_limit;
         }
-        rc = b40c_msbfs_enact(p, src, lim, k, 0, g.has_batch ? &g.batch : nullptr);
+        rc = b40c_msbfs_enact(p, src, lim, k, 0, batch_policy(s, g, false, &pol));
         if (rc) return rc;
-        CUDA_TRY(cudaMemcpyAsync(l->depth, p->d_ms_depth, sizeof(int32_t) * k, cudaMemcpyDeviceToHost, s->stream),
+        CUDA_TRY(cudaEventRecord(s->gpu_ev[2 * b.slot + 1], st), "event record");
+        CUDA_TRY(cudaMemcpyAsync(l->depth, p->d_ms_depth, sizeof(int32_t) * 64, cudaMemcpyDeviceToHost, st),
                  "depth copy");
+        CUDA_TRY(cudaMemcpyAsync(&l->taken, &p->d_ms_join->taken, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
+                 "join count copy");
         for (int i = 0; i < k; i++)
             if (b.queries[i].h_labels)
                 CUDA_TRY(cudaMemcpyAsync(b.queries[i].h_labels, p->d_ms_labels + (size_t)i * (size_t)g.nodes,
-                                         sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, s->stream),
+                                         sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, st),
                          "label copy");
     }
-    CUDA_TRY(cudaMemcpyAsync(&l->error, &p->st->error, sizeof(uint32_t), cudaMemcpyDeviceToHost, s->stream),
+    CUDA_TRY(cudaMemcpyAsync(&l->error, &p->st->error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st),
              "error word copy");
-    CUDA_TRY(cudaEventRecord(s->done_ev[b.slot], s->stream), "event record");
+    CUDA_TRY(cudaEventRecord(s->done_ev[b.slot], st), "event record");
     return B40C_SUCCESS;
+}
+
+// Sends the waiting queries of a graph whose batched search is in flight to
+// join it, while it has free slots (lock held).  Each joining query's labels
+// are copied from its slot after the search (queued on the batch's stream
+// behind the search), then the batch's depths, join count and error word are
+// copied again and its completion event re-recorded, so the batch retires
+// only after all of them.  Returns true when any query was sent.
+bool join_waiting(b40c_server *s, Batch &b)
+{
+    if (b.single) return false;
+    Graph &g = *s->graphs[b.graph];
+    b40c_bfs_problem *p = g.p;
+    Landing *l = s->landing + b.slot;
+    cudaStream_t st = s->streams[b.slot];
+    const int rows = std::min(64, (int)std::min<int64_t>(g.width, p->ms_labels_k));
+    bool sent = false;
+    while (!g.ready.empty() && (int)b.queries.size() < rows) {
+        const Query q = g.ready.front();
+        const int slot = (int)b.queries.size();
+        if (b40c_msbfs_join(p, slot, q.source, q.depth_limit) != B40C_SUCCESS) break;
+        g.ready.pop_front();
+        b.queries.push_back(q);
+        b.join_ns.push_back(s->now());
+        if (q.h_labels &&
+            cudaMemcpyAsync(q.h_labels, p->d_ms_labels + (size_t)slot * (size_t)g.nodes, sizeof(int32_t) * g.nodes,
+                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            cudaGetLastError();  // the query then reports the batch's status with stale labels: not expected
+        sent = true;
+    }
+    if (sent) {
+        if (cudaMemcpyAsync(l->depth, p->d_ms_depth, sizeof(int32_t) * 64, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaMemcpyAsync(&l->taken, &p->d_ms_join->taken, sizeof(int32_t), cudaMemcpyDeviceToHost, st) !=
+                cudaSuccess ||
+            cudaMemcpyAsync(&l->error, &p->st->error, sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+            cudaEventRecord(s->done_ev[b.slot], st) != cudaSuccess)
+            cudaGetLastError();
+    }
+    return sent;
 }
 
 // The graph whose oldest waiting query arrived first among graphs without a
@@ -213,12 +302,15 @@ void dispatcher(b40c_server *s)
             s->arrivals.pop();
             s->graphs[q.graph]->ready.push_back(q);
         }
-        // 2. retire finished batches in issue order
+        // 2. retire finished batches (slots run on their own streams: any order)
         bool retired = false;
-        while (!s->in_flight.empty()) {
-            Batch &b = s->in_flight.front();
+        for (auto it = s->in_flight.begin(); it != s->in_flight.end();) {
+            Batch &b = *it;
             const cudaError_t e = cudaEventQuery(s->done_ev[b.slot]);
-            if (e == cudaErrorNotReady) break;
+            if (e == cudaErrorNotReady) {
+                ++it;
+                continue;
+            }
             int status = B40C_SUCCESS;
             if (e != cudaSuccess) {
                 cudaGetLastError();
@@ -231,7 +323,7 @@ void dispatcher(b40c_server *s)
                     status = B40C_ERROR_LAUNCH_TIMEOUT;
             }
             finish_batch(s, b, status, s->now());
-            s->in_flight.pop_front();
+            it = s->in_flight.erase(it);
             retired = true;
         }
         // a dispatcher without a device fails what is waiting instead of issuing it
@@ -251,7 +343,11 @@ void dispatcher(b40c_server *s)
             }
         }
         if (retired) s->cv_done.notify_all();
-        // 3. issue batches
+        // 3. waiting queries of a graph whose batch is running join it (its free
+        // slots), the rest wait for a batch of their own
+        if (!s->thread_error)
+            for (Batch &b : s->in_flight) join_waiting(s, b);
+        // 4. issue batches
         while ((int)s->in_flight.size() < s->max_in_flight && !s->free_slots.empty() && !s->thread_error) {
             const int gi = next_graph(s);
             if (gi < 0) break;
@@ -265,6 +361,7 @@ void dispatcher(b40c_server *s)
                 b.queries.push_back(g.ready.front());
                 g.ready.pop_front();
             }
+            b.k = k;
             b.single = (k == 1 && s->single_strategy >= 0);
             b.launch_ns = s->now();
             g.busy = true;
@@ -281,7 +378,7 @@ void dispatcher(b40c_server *s)
                 s->batched_queries += k;
             s->in_flight.push_back(std::move(b));
         }
-        // 4. wait
+        // 5. wait
         bool waiting = false;
         for (Graph *g : s->graphs)
             if (g && !g->ready.empty()) waiting = true;
@@ -384,6 +481,9 @@ int b40c_server_create(int device, const b40c_server_options *options, b40c_serv
     s->max_batch = o.max_batch ? o.max_batch : 64;
     s->single_strategy = o.single_strategy;
     s->max_in_flight = o.max_in_flight ? o.max_in_flight : 2;
+    // by default the slots split each SM evenly (the kernels are resident at 4 CTAs per SM)
+    s->ctas_per_sm = o.ctas_per_sm > 0 ? o.ctas_per_sm : std::max(1, 4 / s->max_in_flight);
+    if (o.ctas_per_sm < 0) s->ctas_per_sm = 0;  // -1: every batch takes the whole device
     s->t0 = std::chrono::steady_clock::now();
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
@@ -392,25 +492,41 @@ int b40c_server_create(int device, const b40c_server_options *options, b40c_serv
         return b40c::fail(B40C_ERROR_NO_DEVICE, "cudaMemGetInfo failed");
     }
     s->budget = o.memory_budget_bytes ? o.memory_budget_bytes : (int64_t)(0.9 * (double)free_b);
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaMallocHost((void **)&s->landing, sizeof(Landing) * s->max_in_flight) != cudaSuccess) {
-        cudaGetLastError();
-        if (s->stream) cudaStreamDestroy(s->stream);
-        delete s;
-        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server stream or landing area allocation failed");
-    }
+    s->streams = new cudaStream_t[s->max_in_flight]();
     s->done_ev = new cudaEvent_t[s->max_in_flight]();
+    s->gpu_ev = new cudaEvent_t[2 * s->max_in_flight]();
+    auto undo = [s]() {
+        for (int j = 0; j < s->max_in_flight; j++) {
+            if (s->done_ev[j]) cudaEventDestroy(s->done_ev[j]);
+            if (s->gpu_ev[2 * j]) cudaEventDestroy(s->gpu_ev[2 * j]);
+            if (s->gpu_ev[2 * j + 1]) cudaEventDestroy(s->gpu_ev[2 * j + 1]);
+            if (s->streams[j]) cudaStreamDestroy(s->streams[j]);
+        }
+        if (s->base_ev) cudaEventDestroy(s->base_ev);
+        delete[] s->done_ev;
+        delete[] s->gpu_ev;
+        delete[] s->streams;
+        if (s->landing) cudaFreeHost(s->landing);
+        cudaGetLastError();
+        delete s;
+    };
+    if (cudaMallocHost((void **)&s->landing, sizeof(Landing) * s->max_in_flight) != cudaSuccess) {
+        s->landing = nullptr;
+        undo();
+        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server landing area allocation failed");
+    }
     for (int i = 0; i < s->max_in_flight; i++) {
-        if (cudaEventCreateWithFlags(&s->done_ev[i], cudaEventDisableTiming) != cudaSuccess) {
-            cudaGetLastError();
-            for (int j = 0; j < i; j++) cudaEventDestroy(s->done_ev[j]);
-            delete[] s->done_ev;
-            cudaFreeHost(s->landing);
-            cudaStreamDestroy(s->stream);
-            delete s;
-            return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server event creation failed");
+        if (cudaStreamCreateWithFlags(&s->streams[i], cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&s->done_ev[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreate(&s->gpu_ev[2 * i]) != cudaSuccess || cudaEventCreate(&s->gpu_ev[2 * i + 1]) != cudaSuccess) {
+            undo();
+            return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server stream or event creation failed");
         }
         s->free_slots.push_back(s->max_in_flight - 1 - i);
+    }
+    if (cudaEventCreate(&s->base_ev) != cudaSuccess || cudaEventRecord(s->base_ev, s->streams[0]) != cudaSuccess) {
+        undo();
+        return b40c::fail(B40C_ERROR_MEMORY_ALLOCATION, "server event creation failed");
     }
     s->worker = std::thread(dispatcher, s);
     *out = s;
@@ -438,15 +554,22 @@ int b40c_server_destroy(b40c_server *s)
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
     rt::DeviceGuard guard(s->device);
-    cudaStreamSynchronize(s->stream);
+    for (int i = 0; i < s->max_in_flight; i++) cudaStreamSynchronize(s->streams[i]);
     for (Graph *g : s->graphs) {
         if (g && g->p) b40c_bfs_problem_destroy(g->p);
         delete g;
     }
-    for (int i = 0; i < s->max_in_flight; i++) cudaEventDestroy(s->done_ev[i]);
+    for (int i = 0; i < s->max_in_flight; i++) {
+        cudaEventDestroy(s->done_ev[i]);
+        cudaEventDestroy(s->gpu_ev[2 * i]);
+        cudaEventDestroy(s->gpu_ev[2 * i + 1]);
+        cudaStreamDestroy(s->streams[i]);
+    }
+    cudaEventDestroy(s->base_ev);
     delete[] s->done_ev;
+    delete[] s->gpu_ev;
+    delete[] s->streams;
     cudaFreeHost(s->landing);
-    cudaStreamDestroy(s->stream);
     cudaGetLastError();
     delete s;
     return B40C_SUCCESS;
@@ -484,7 +607,7 @@ int b40c_server_add_graph(b40c_server *s, const int32_t *row_offsets, const int3
         b40c_bfs_problem_destroy(p);
         return code;
     };
-    p->stream = s->stream;
+    p->stream = s->streams[0];  // set-up only; each batch runs on its slot's stream
     p->queue_sizing = kQueueSizing;
     // allocate everything a batch of full width and a single search use, now
     // rather than while serving; the searches also run the symmetry test once
@@ -495,7 +618,7 @@ int b40c_server_add_graph(b40c_server *s, const int32_t *row_offsets, const int3
         return bail(rc);
     // charged by the plan whether or not searches use them
     if ((rc = rt::ensure_hubs(p)) || (rc = rt::ensure_unvisited_lists(p))) return bail(rc);
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess) {
+    if (cudaStreamSynchronize(s->streams[0]) != cudaSuccess) {
         const cudaError_t e = cudaGetLastError();
         return bail(b40c::fail((int)e, "graph warm-up failed: %s", cudaGetErrorString(e)));
     }
@@ -529,6 +652,21 @@ int b40c_server_remove_graph(b40c_server *s, int32_t graph_id)
         s->used -= g->bytes;
         p = g->p;
         g->p = nullptr;
+        // the freed bytes widen the other graphs' batches again (oldest graph
+        // first, up to max_batch), charged at the new width's plan; the extra
+        // label rows are allocated by their next batch
+        for (Graph *o : s->graphs) {
+            if (!o || o->removed || o->width >= s->max_batch) continue;
+            int w = o->width;
+            while (w * 2 <= s->max_batch &&
+                   rt::planned_bytes(o->nodes, o->edges, w * 2, kQueueSizing) - o->bytes <= s->budget - s->used)
+                w *= 2;
+            if (w == o->width) continue;
+            const int64_t nb = rt::planned_bytes(o->nodes, o->edges, w, kQueueSizing);
+            s->used += nb - o->bytes;
+            o->bytes = nb;
+            o->width = w;
+        }
     }
     rt::DeviceGuard guard(s->device);
     return b40c_bfs_problem_destroy(p);
@@ -661,6 +799,7 @@ int b40c_server_counters_get(b40c_server *s, b40c_server_counters *out)
     c.batches = s->batches;
     c.batched_queries = s->batched_queries;
     c.single_queries = s->single_queries;
+    c.joined_queries = s->joined_queries;
     c.memory_used_bytes = s->used;
     c.memory_budget_bytes = s->budget;
     for (Graph *g : s->graphs)

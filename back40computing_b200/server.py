@@ -25,12 +25,13 @@ class BfsServer:
     """
 
     def __init__(self, device: int = 0, memory_budget_bytes: int = 0, max_batch: int = 0,
-                 single_strategy: int = N.DIRECTION_OPTIMIZING, max_in_flight: int = 0):
+                 single_strategy: int = N.DIRECTION_OPTIMIZING, max_in_flight: int = 0, ctas_per_sm: int = 0):
         o = N.ServerOptions()
         o.memory_budget_bytes = int(memory_budget_bytes)
         o.max_batch = int(max_batch)
         o.single_strategy = int(single_strategy)
         o.max_in_flight = int(max_in_flight)
+        o.ctas_per_sm = int(ctas_per_sm)
         self._h = C.c_void_p(None)
         N.check(N.lib().b40c_server_create(int(device), C.byref(o), C.byref(self._h)), "b40c_server_create")
         self._labels = {}  # ticket -> caller array kept alive until the query finishes

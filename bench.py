@@ -67,7 +67,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bound on the CPU-baseline sample")
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the batched (random 2^21) and lattice (grid2d-1000, grid3d-256) measurements")
+                    help="skip the batched (random 2^21), lattice (grid2d-1000, grid3d-256) and served measurements")
+    ap.add_argument("--extras", default="batched,lattices,served",
+                    help="which of the extra measurements to run (comma list of batched, lattices, served)")
+    ap.add_argument("--only-extras", action="store_true",
+                    help="run just the extra measurements (no single-source line); prints them as one JSON line")
     return ap.parse_args()
 
 
@@ -369,14 +373,19 @@ SERVED_SET = [("rmat16", dict(kind="rmat", scale=16, ef=16)), ("rmat18", dict(ki
 SERVED_BUDGET = 6 << 30  # device bytes the server may hold for the six graphs
 
 
-def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=(0.25, 0.5, 0.75, 0.9)):
+def served_extra(resident=None, n_requests=20000, baseline_requests=None, rates=(0.5, 0.75, 0.9),
+                 slots=(2, 4)):
     """The query server on the six resident graphs: a seeded request stream
-    (graph uniform over the six, source uniform over 4096 sampled degree > 0
-    vertices of it, depth limit unlimited w.p. 0.8 else uniform in 2..8).
-      * capacity: all requests queued at t = 0, queries/s to the last answer;
-      * one at a time: the same server with batch width 1 (plain
-        direction-optimizing search per query) on the first requests;
-      * latency: Poisson arrivals at fractions of the capacity, p50/p99 of
+    (graph uniform over the six, source uniform over the vertices of nonzero
+    degree of it, depth limit unlimited w.p. 0.8 else uniform in 2..8).
+      * capacity: all requests queued at t = 0, queries/s to the last answer,
+        for each number of in-flight slots in `slots` (each slot a stream of
+        its own with its share of every SM) and, for the first, with every
+        batch on the whole device;
+      * one at a time: one slot, batch width 1 (a plain direction-optimizing
+        search per query, whole device), on the whole stream (or its first
+        baseline_requests);
+      * latency: Poisson arrivals at fractions of the best capacity, p50/p99 of
         finish - arrival on the server clock."""
     from back40computing_b200 import CsrGraph, BuildRmatGraph, BuildGrid2dGraph, BuildGrid3dGraph, sample_sources
     from back40computing_b200.server import BfsServer, latency_summary
@@ -398,10 +407,11 @@ def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=
     gid = rng.integers(0, len(graphs), n_requests).astype(np.int32)
     src = np.empty(n_requests, np.int32)
     for i, g in enumerate(graphs):
-        pool = sample_sources(g, 4096, seed=i)
+        pool = np.flatnonzero(np.diff(g.row_offsets) > 0).astype(np.int32)  # every vertex with an edge
         sel = gid == i
         src[sel] = pool[rng.integers(0, pool.size, int(sel.sum()))]
     lim = np.where(rng.random(n_requests) < 0.8, -1, rng.integers(2, 9, n_requests)).astype(np.int32)
+    baseline_requests = baseline_requests or n_requests
 
     def run(server, count, arrivals):
         t0 = server.now_ns() + 20_000_000
@@ -409,32 +419,47 @@ def served_extra(resident=None, n_requests=20000, baseline_requests=1200, rates=
         server.drain()
         return server.results(int(tk[0]), count)
 
-    out = {"graphs": [n for n, _ in SERVED_SET], "budget_bytes": SERVED_BUDGET, "requests": n_requests}
-    with BfsServer(memory_budget_bytes=SERVED_BUDGET) as srv:
+    out = {"graphs": [n for n, _ in SERVED_SET], "budget_bytes": SERVED_BUDGET, "requests": n_requests,
+           "sources": "uniform over the vertices of nonzero degree"}
+    caps = {}
+    for k in slots:
+        for share in ((0, -1) if k == slots[0] else (0,)):
+            name = f"{k} slots" + (", whole device per batch" if share < 0 else "")
+            with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_in_flight=k, ctas_per_sm=share) as srv:
+                for g in graphs:
+                    srv.add_tuned_graph(g)
+                out["widths"] = [srv.graph_info(i)[1] for i in range(len(graphs))]
+                out["memory_used_bytes"] = srv.counters()["memory_used_bytes"]
+                run(srv, 500, np.zeros(500, np.int64))  # warm-up
+                caps[name] = latency_summary(run(srv, n_requests, np.zeros(n_requests, np.int64)))
+                caps[name].update(max_in_flight=k, ctas_per_sm=share)
+    best = max(caps, key=lambda c: caps[c]["queries_per_s"])
+    out["capacity_by_config"] = caps
+    out["capacity"] = dict(caps[best], config=best)
+    k, share = caps[best]["max_in_flight"], caps[best]["ctas_per_sm"]
+    with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_in_flight=k, ctas_per_sm=share) as srv:
         for g in graphs:
             srv.add_tuned_graph(g)
-        out["widths"] = [srv.graph_info(i)[1] for i in range(len(graphs))]
-        out["memory_used_bytes"] = srv.counters()["memory_used_bytes"]
-        run(srv, 500, np.zeros(500, np.int64))  # warm-up
-        cap = latency_summary(run(srv, n_requests, np.zeros(n_requests, np.int64)))
-        out["capacity"] = cap
+        run(srv, 500, np.zeros(500, np.int64))
         sweep = []
         for f in rates:
-            rate = f * cap["queries_per_s"]
+            rate = f * out["capacity"]["queries_per_s"]
             gaps = rng.exponential(1e9 / rate, n_requests)
             rec = run(srv, n_requests, np.cumsum(gaps).astype(np.int64))
             sm = latency_summary(rec)
             sm["offered_qps"] = rate
+            sm["load"] = f
             sweep.append(sm)
         out["latency_sweep"] = sweep
-    with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_batch=1) as one:
+    with BfsServer(memory_budget_bytes=SERVED_BUDGET, max_batch=1, max_in_flight=1, ctas_per_sm=-1) as one:
         for g in graphs:
             one.add_tuned_graph(g)
         run(one, 50, np.zeros(50, np.int64))
         base = latency_summary(run(one, baseline_requests, np.zeros(baseline_requests, np.int64)))
-        base["sample"] = f"first {baseline_requests} requests of the stream"
+        base["sample"] = (f"all {n_requests} requests" if baseline_requests == n_requests
+                          else f"first {baseline_requests} requests of the stream")
         out["one_at_a_time"] = base
-    out["speedup_queries_per_s"] = cap["queries_per_s"] / base["queries_per_s"]
+    out["speedup_queries_per_s"] = out["capacity"]["queries_per_s"] / base["queries_per_s"]
     return out
 
 
@@ -488,6 +513,21 @@ def main():
     from back40computing_b200 import CsrProblem
     from back40computing_b200 import _native as N
     from back40computing_b200.bfs import ENACTORS
+
+    if args.only_extras:
+        if rank == 0:
+            wanted = set(args.extras.split(","))
+            extras = {}
+            if "batched" in wanted:
+                extras["batched"] = batched_extra(max(args.steps, 3), args.warmup)
+            if "lattices" in wanted:
+                extras["lattices"] = lattice_extra()
+            if "served" in wanted:
+                extras["served"] = served_extra()
+            print(json.dumps(extras), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     g, fixed = build_graph(args.config)
     srcs = sources_for(g, fixed, args.sources)
@@ -610,9 +650,13 @@ def main():
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras["batched"] = batched_extra(max(args.steps, 3), args.warmup)
-        extras["lattices"] = lattice_extra()
-        extras["served"] = served_extra((args.config, g) if args.config in dict(SERVED_SET) else None)
+        wanted = set(args.extras.split(","))
+        if "batched" in wanted:
+            extras["batched"] = batched_extra(max(args.steps, 3), args.warmup)
+        if "lattices" in wanted:
+            extras["lattices"] = lattice_extra()
+        if "served" in wanted:
+            extras["served"] = served_extra((args.config, g) if args.config in dict(SERVED_SET) else None)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -283,7 +283,25 @@ int b40c_bfs_device_view_get(b40c_bfs_problem *problem, b40c_bfs_device_view *vi
 int b40c_msbfs_enact(b40c_bfs_problem *problem, const int32_t *sources, const int32_t *depth_limits, int k,
                      int max_grid_size, const b40c_bfs_policy *policy);
 
-/* Copies slot `slot`'s labels of the last batch to the host. */
+/* Adds a source to the batch in flight (no counterpart in the reference):
+ * the running search takes the request at its next level boundary and from
+ * then on searches from `source` in slot `slot` too, alongside the batch's
+ * sources; that slot's labels (and search depth) are those of a search from
+ * `source` alone with `depth_limit`.  slot must lie in [k, rows), k the
+ * batch's sources and rows the label rows the problem holds (the widest batch
+ * it has run; at most 64); at most 64 requests per batch.  Asynchronous and
+ * cheap (three small host-to-device copies on a stream of the problem's own):
+ * it may be called while the batch runs.  A request that arrives after the
+ * search ended is not taken: b40c_msbfs_joined reports how many were. */
+int b40c_msbfs_join(b40c_bfs_problem *problem, int32_t slot, int32_t source, int32_t depth_limit);
+
+/* After a batch: *taken = the number of b40c_msbfs_join requests the search
+ * took (the first *taken, in call order); search_depths (NULL or [64]) gets
+ * every slot's search depth. */
+int b40c_msbfs_joined(b40c_bfs_problem *problem, int32_t *taken, int32_t *search_depths);
+
+/* Copies slot `slot`'s labels of the last batch to the host (slots past k:
+ * the sources that joined it). */
 int b40c_msbfs_extract(b40c_bfs_problem *problem, int slot, int32_t *h_labels);
 
 /* search_depths[k]: each slot's search depth in the last batch (max label + 1,

@@ -12,8 +12,12 @@
  * would give for that query alone: labels are distances, -1 unreached or
  * beyond the depth limit, and search_depth is max label + 1.
  *
- * One background thread per server issues the GPU work on one stream and
- * retires finished batches; the calls below may come from any thread.
+ * One background thread per server issues the GPU work (one CUDA stream per
+ * in-flight slot) and retires finished batches; the calls below may come from
+ * any thread.
+ * A query that arrives while its graph's batched search is running joins
+ * that search at its next level boundary when the batch has a free slot
+ * (b40c_msbfs_join), instead of waiting for the next batch.
  * Status codes are the cudaError_t values of b40c_bfs.h.
  */
 #ifndef B40C_SERVER_H
@@ -42,10 +46,18 @@ typedef struct b40c_server_options {
      * 0 is read as this), B40C_EXPAND_CONTRACT, or -1 to use the batched
      * kernel for lone queries too. */
     int32_t single_strategy;
-    /* Batches queued on the GPU at once, over all graphs (0 = 2); at most one
-     * per graph, so queries for a busy graph gather into its next batch. */
+    /* Batches on the GPU at once, over all graphs (0 = 2); at most one per
+     * graph, so queries for a busy graph gather into its next batch.  Each
+     * in-flight batch has a CUDA stream of its own: batches of different
+     * graphs, and one batch's label read-back with another's search, overlap. */
     int32_t max_in_flight;
-    int32_t reserved[5];
+    /* CTAs per SM of each batch's persistent grid: 0 = split the SMs evenly
+     * among the max_in_flight slots (4 / max_in_flight, at least 1; the
+     * kernels are resident at up to 4), so the grids of concurrent batches
+     * are resident side by side; -1 = every batch takes the whole device
+     * (concurrent batches then mostly wait for each other). */
+    int32_t ctas_per_sm;
+    int32_t reserved[4];
 } b40c_server_options;
 
 typedef struct b40c_server_result {
@@ -57,6 +69,9 @@ typedef struct b40c_server_result {
     int64_t arrival_ns;    /* server clock: when the query became eligible */
     int64_t launch_ns;     /* when its batch was issued to the GPU */
     int64_t finish_ns;     /* when the server saw its batch (and its label copy) finish */
+    int64_t gpu_start_ns;  /* device clock (CUDA events on the batch's stream, from the server's creation):
+                              when its batch's search began on the GPU ... */
+    int64_t gpu_end_ns;    /* ... and when it ended (before the label copy) */
 } b40c_server_result;
 
 typedef struct b40c_server_counters {
@@ -64,7 +79,8 @@ typedef struct b40c_server_counters {
     int64_t batches, batched_queries, single_queries;
     int64_t memory_used_bytes, memory_budget_bytes;
     int32_t graphs;
-    int32_t reserved[3];
+    int32_t reserved;
+    int64_t joined_queries; /* of batched_queries: the ones that joined a batch in flight */
 } b40c_server_counters;
 
 /* options may be NULL (all defaults).  device < 0 = the current device. */

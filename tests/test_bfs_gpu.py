@@ -486,3 +486,59 @@ def test_subgrid_phase(threshold, kind, args, strategy, preds):
             e = ENACTORS[strategy]()
             e._problem = p
             assert e.GetStatistics()[1] == depth
+
+
+# ---- sources joining a batch in flight ------------------------------------------------
+
+@pytest.mark.parametrize("kind,args", [("grid2d", (400,)), ("rmat", (1 << 16, 1 << 20)), ("rr", (1 << 15, 8))])
+def test_sources_join_a_running_batch(kind, args):
+    """Sources added while a batch runs (b40c_msbfs_join) are taken at a level
+    boundary and searched from there on in their own slots: each joined slot's
+    labels and search depth equal the oracle's for that source alone, and the
+    batch's own slots are unchanged."""
+    import ctypes as C
+    g = _graph(kind, *args)
+    p = CsrProblem.from_graph(g)
+    srcs = sample_sources(g, 12, seed=41)
+    p.msbfs(srcs[:16] if srcs.size > 16 else srcs)  # sizes the label rows (12)
+    base, joins = srcs[:4], srcs[4:12]
+    lim = np.array([-1, 3, -1, 0, -1, 5, -1, -1], np.int32)
+    p.msbfs(base)
+    for j, s in enumerate(joins):
+        p.msbfs_join(4 + j, int(s), int(lim[j]))
+    taken, depths = p.msbfs_joined()
+    assert 0 <= taken <= joins.size
+    for slot in range(4):
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(base[slot]))
+        assert oracle.compare_labels(p.labels_of(slot), want) == -1
+        assert depths[slot] == depth
+    for j in range(taken):
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(joins[j]), int(lim[j]))
+        assert oracle.compare_labels(p.labels_of(4 + j), want) == -1, f"joined slot {4 + j}"
+        assert depths[4 + j] == depth, f"joined slot {4 + j}"
+    with pytest.raises(B40cError):
+        p.msbfs_join(2, int(joins[0]))  # a slot of the batch's own sources
+    with pytest.raises(B40cError):
+        p.msbfs_join(12, int(joins[0]))  # past the label rows
+    p.Destroy()
+
+
+def test_join_taken_while_a_long_batch_runs():
+    """On a lattice the batch takes thousands of levels: requests sent right
+    after the launch are all taken, at different levels, with exact labels."""
+    g = _graph("grid2d", 1000)
+    p = CsrProblem.from_graph(g)
+    p.msbfs(np.arange(0, 8, dtype=np.int32) * 1000)  # label rows for 8 slots
+    p.msbfs(np.array([0], np.int32))  # corner: about 2,000 levels
+    joins = [999, 500_500, 999_999, 123_456]
+    for j, s in enumerate(joins):
+        p.msbfs_join(1 + j, s, -1)
+    taken, depths = p.msbfs_joined()
+    assert taken == len(joins)
+    y, x = np.divmod(np.arange(1_000_000), 1000)
+    for j, s in enumerate(joins):
+        sy, sx = divmod(s, 1000)
+        want = (np.abs(x - sx) + np.abs(y - sy)).astype(np.int32)
+        assert np.array_equal(p.labels_of(1 + j), want), f"joined source {s}"
+        assert depths[1 + j] == int(want.max()) + 1
+    p.Destroy()

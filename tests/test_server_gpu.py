@@ -127,9 +127,18 @@ def test_budget_admission_and_accounting():
         assert (recs["status"] == 0).all() and recs["batch_size"].max() <= 8
         for r, s in zip(recs, srcs):
             assert r["search_depth"] == _oracle(gs[1], s, -1)[1]
-        # removing a graph returns its bytes to the budget
+        # removing a graph returns its bytes to the budget, and the freed bytes
+        # widen the remaining graph's batches again
         srv.remove_graph(g0)
-        assert srv.counters()["memory_used_bytes"] == b1_8
+        _, w1 = srv.graph_info(g1)
+        assert w1 > 8 and BfsServer.plan_bytes(gs[1].nodes, gs[1].edges, w1) <= budget
+        assert srv.counters()["memory_used_bytes"] == BfsServer.plan_bytes(gs[1].nodes, gs[1].edges, w1)
+        t = srv.submit_many(np.full(w1, g1, np.int32), sample_sources(gs[1], w1, seed=3))
+        srv.drain()
+        recs = srv.results(int(t[0]), w1)
+        assert (recs["status"] == 0).all() and recs["batch_size"].max() > 8
+        srv.remove_graph(g1)
+        assert srv.counters()["memory_used_bytes"] == 0
         assert srv.add_graph(gs[2]) == 2
 
 
@@ -178,3 +187,66 @@ def test_bad_queries_rejected():
         with pytest.raises(B40cError):
             srv.submit_many([g, g], [0, -1])
         assert srv.counters()["submitted"] == 0
+
+
+def test_batches_of_different_graphs_overlap_on_the_device():
+    """Each in-flight slot has its own stream and a share of every SM: batches
+    of two graphs issued together run at the same time on the GPU (their
+    device-clock intervals intersect), and their answers stay exact."""
+    gs = _graphs()[:3]
+    with BfsServer(max_in_flight=2) as srv:
+        for g in gs:
+            srv.add_graph(g)
+        rng = np.random.default_rng(4)
+        gid = np.repeat(np.arange(3, dtype=np.int32), 192)
+        src = np.concatenate([sample_sources(g, 192, seed=i) for i, g in enumerate(gs)])
+        order = rng.permutation(gid.size)
+        gid, src = gid[order], src[order]
+        t = srv.submit_many(gid, src, None, np.full(gid.size, srv.now_ns() + 50_000_000, np.int64))
+        srv.drain()
+        recs = srv.results(int(t[0]), gid.size)
+    assert (recs["status"] == 0).all()
+    assert (recs["gpu_end_ns"] > recs["gpu_start_ns"]).all()
+    spans = {(int(r["graph"]), int(r["gpu_start_ns"]), int(r["gpu_end_ns"])) for r in recs}
+    spans = sorted(spans, key=lambda x: x[1])
+    overlaps = sum(1 for i, a in enumerate(spans) for b in spans[i + 1:]
+                   if b[1] < a[2] and a[0] != b[0])
+    assert overlaps > 0, "no two batches of different graphs ran at the same time"
+    for i in range(0, gid.size, 17):
+        want, depth = _oracle(gs[gid[i]], src[i], -1)
+        assert recs["search_depth"][i] == depth
+
+
+def test_queries_join_a_running_batch_with_exact_labels():
+    """Queries that arrive while their graph's batched search runs join it at
+    a level boundary (free slots of the batch) instead of waiting for the next
+    batch; each still gets exactly the labels of its search alone."""
+    g = CsrGraph()
+    BuildGrid2dGraph(1000, g)  # about 2,000 levels: the batch runs for many milliseconds
+    y, x = np.divmod(np.arange(g.nodes), 1000)
+    with BfsServer(max_batch=8, max_in_flight=1) as srv:
+        gid = srv.add_graph(g)
+        t0 = srv.now_ns() + 20_000_000
+        first = [0, 999]
+        later = [500_500, 999_999, 1234, 777_000]
+        outs = {s: np.empty(g.nodes, np.int32) for s in first + later}
+        tickets = {}
+        for s in first:
+            tickets[s] = srv.submit(gid, s, -1, labels=outs[s], arrival_ns=t0)
+        for k, s in enumerate(later):
+            tickets[s] = srv.submit(gid, s, 3 if k == 2 else -1, labels=outs[s], arrival_ns=t0 + 2_000_000)
+        srv.drain()
+        recs = {s: srv.result(t) for s, t in tickets.items()}
+        c = srv.counters()
+    assert all(r["status"] == 0 for r in recs.values())
+    assert c["joined_queries"] >= 1, c
+    joined = [s for s in later if recs[s]["launch_ns"] > recs[first[0]]["launch_ns"] and
+              recs[s]["batch_size"] == recs[first[0]]["batch_size"]]
+    assert joined, "no late query shared the first batch"
+    for k, s in enumerate(first + later):
+        sy, sx = divmod(s, 1000)
+        want = (np.abs(x - sx) + np.abs(y - sy)).astype(np.int32)
+        if s == later[2]:
+            want = np.where(want <= 3, want, -1).astype(np.int32)
+        assert np.array_equal(outs[s], want), f"source {s}"
+        assert recs[s]["search_depth"] == int(want.max()) + 1
