@@ -49,6 +49,7 @@ class Policy(C.Structure):
         ("bottom_up_defer_frontier", C.c_int32),
         ("subgrid_frontier_edges", C.c_int32),
         ("bottom_up_long_list", C.c_int32),
+        ("history_cull", C.c_int32),
     ]
 
 

@@ -74,7 +74,30 @@ struct ExpandSmem {
     uint32_t win_word[B];              // bottom-up windows: the window's visited words, discoveries OR'ed in
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
+    uint32_t *hist;                    // history cull table (dynamic shared memory past this struct), or null
 };
+
+// History culling (the reference's HistoryCull, two_phase/contract_atomic/
+// cta.cuh:276-297, as a B200 shared-memory filter): each CTA keeps a
+// direct-mapped table of 2^p.hist_log vertex ids it has sent to the visited
+// test in this launch.  Every id in it is visited (its first test set the
+// bit, or found it set), so a gathered neighbour found in the table is
+// dropped without touching the visited mask in L2; a collision only
+// overwrites an entry (less filtering, never a wrong drop).  The table lives
+// past ExpandSmem in dynamic shared memory and is cleared when a launch starts.
+constexpr uint32_t kHistEmpty = 0xffffffffu;
+__device__ __forceinline__ unsigned hist_slot(int v, int log2) { return ((unsigned)v * 2654435761u) >> (32 - log2); }
+
+template <int B, bool PRED>
+__device__ __forceinline__ void hist_init(const BfsParams &p, ExpandSmem<B, PRED> &s, unsigned char *smem_raw)
+{
+    s.hist = nullptr;
+    if (p.hist_log > 0) {
+        uint32_t *h = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(ExpandSmem<B, PRED>) + 15) & ~size_t(15)));
+        for (int i = threadIdx.x; i < (1 << p.hist_log); i += B) h[i] = kHistEmpty;
+        s.hist = h;  // (the caller's barrier publishes both)
+    }
+}
 
 __device__ __forceinline__ unsigned long long globaltimer_ns()
 {
@@ -160,10 +183,18 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
     bool go[U];
     unsigned word[U];
     precheck = precheck && p.precheck && !(LISTS && s.ul_in >= 0);
+    uint32_t *hist = s.hist;
 #pragma unroll
     for (int t = 0; t < U; t++) {
         go[t] = valid[t];
         if (active[t] && p.warp_cull) go[t] = warp_cull(go[t], v[t]);
+        if (hist && go[t]) {
+            const unsigned h = hist_slot(v[t], p.hist_log);
+            if (hist[h] == (uint32_t)v[t])
+                go[t] = false;  // already sent to the visited test by this CTA: visited
+            else
+                hist[h] = (uint32_t)v[t];
+        }
         word[t] = 0;
         if (go[t] && precheck) word[t] = ld_mask(s.mask + (v[t] >> 5));
     }
@@ -782,15 +813,13 @@ __device__ __forceinline__ void bottom_up_queue(const BfsParams &p, const uint32
         if (cur >= 0) {
             int nb[4];
             unsigned w[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) nb[k] = (e + k < hi) ? ld_stream(p.column_indices + e + k) : -1;
+            e = ld_quad(p.column_indices, p.edges, e, hi, nb);  // one 16-byte load per step
 #pragma unroll
             for (int k = 0; k < 4; k++) w[k] = nb[k] >= 0 ? ld_mask(mask + (nb[k] >> 5)) : 0u;
             int found = -1;
 #pragma unroll
             for (int k = 3; k >= 0; k--)
                 if (nb[k] >= 0 && ((w[k] >> (nb[k] & 31)) & 1u)) found = nb[k];
-            e += 4;
             if (found >= 0) q_par[cur] = found;
             if (found >= 0 || e >= hi) cur = -1;
         }
@@ -1506,6 +1535,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
     __shared__ int s_ok;
     const int tid = threadIdx.x;
     if (tid == 0) mbar_init(&s.bar, 1);
+    hist_init<B, PRED>(p, s, smem_raw);
     unsigned bar_phase = 0, generation = 0;
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);
@@ -1759,6 +1789,7 @@ __global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
     __shared__ int s_ok;
     const int tid = threadIdx.x;
     if (tid == 0) mbar_init(&s.bar, 1);
+    hist_init<B, PRED>(p, s, smem_raw);
     unsigned bar_phase = 0, generation = 0;
     int max_level_seen = -1;
     int level = ld_cg(&p.st->cur_level);

@@ -21,6 +21,28 @@ constexpr unsigned kErrLevels = 32u;        // more levels than vertices: a capt
 constexpr unsigned kErrFrontier = 64u;      // a deferred bottom-up frontier did not match its counted size
 constexpr unsigned kSpinLimit = 1u << 22;   // polls before a wait gives up (~1-2 s with backoff)
 
+// ---- L2 residency -------------------------------------------------------------
+// Column indices are read once per search (a stream larger than L2); they are
+// loaded with an evict-first L2 policy so that what levels and searches read
+// again -- visited masks, the batched search's frontier and visited masks,
+// row offsets, hub pairs, labels -- stays in L2.  The batched search's random
+// mask gathers are marked evict-last.  B40C_L2_HINTS=0 builds without hints.
+#ifndef B40C_L2_HINTS
+#define B40C_L2_HINTS 1
+#endif
+__device__ __forceinline__ uint64_t l2_evict_first()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ uint64_t l2_evict_last()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
 // ---- loads / stores ----------------------------------------------------------
 __device__ __forceinline__ int ld_cg(const int *p)
 {
@@ -38,16 +60,73 @@ __device__ __forceinline__ unsigned ld_cg(const unsigned *p)
 __device__ __forceinline__ int ld_stream(const int *p)
 {
     int v;
+#if B40C_L2_HINTS
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(l2_evict_first()));
+#else
     asm volatile("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+#endif
     return v;
 }
 __device__ __forceinline__ int4 ld_stream4(const int4 *p)
 {
     int4 v;
+#if B40C_L2_HINTS
+    asm volatile("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+                 : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+                 : "l"(p), "l"(l2_evict_first()));
+#else
     asm volatile("ld.global.nc.L1::no_allocate.v4.s32 {%0,%1,%2,%3}, [%4];"
                  : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
                  : "l"(p));
+#endif
     return v;
+}
+// coherent (L2) 64-bit load of data read again and again (the batched search's
+// frontier and visited masks): evict-last in L2
+__device__ __forceinline__ unsigned long long ld_keep64(const unsigned long long *p)
+{
+    unsigned long long v;
+#if B40C_L2_HINTS
+    asm volatile("ld.global.cg.L2::cache_hint.u64 %0, [%1], %2;" : "=l"(v) : "l"(p), "l"(l2_evict_last()));
+#else
+    asm volatile("ld.global.cg.u64 %0, [%1];" : "=l"(v) : "l"(p));
+#endif
+    return v;
+}
+// store of data written once and not read again by the search (batch labels)
+__device__ __forceinline__ void st_stream(int *p, int v)
+{
+#if B40C_L2_HINTS
+    asm volatile("st.global.L1::no_allocate.L2::cache_hint.s32 [%0], %1, %2;" ::"l"(p), "r"(v), "l"(l2_evict_first())
+                 : "memory");
+#else
+    *p = v;
+#endif
+}
+// Column indices [e, hi) of one list, four positions per call from one
+// 16-byte load: the load covers the aligned quad holding e (aligned by
+// address, so any 4-byte aligned array works; positions outside [e, hi) come
+// back as -1); where the quad would leave the array [0, m) the positions are
+// read one by one.  Returns the next position to read.
+__device__ __forceinline__ int ld_quad(const int32_t *ci, int m, int e, int hi, int (&nb)[4])
+{
+    if (e >= hi) {
+        nb[0] = nb[1] = nb[2] = nb[3] = -1;
+        return e;
+    }
+    const int mis = (int)((reinterpret_cast<uintptr_t>(ci) >> 2) & 3u);
+    const int ea = ((e + mis) & ~3) - mis;
+    if (ea >= 0 && ea + 4 <= m) {
+        const int4 x = ld_stream4(reinterpret_cast<const int4 *>(ci + ea));
+        nb[0] = (ea >= e && ea < hi) ? x.x : -1;
+        nb[1] = (ea + 1 >= e && ea + 1 < hi) ? x.y : -1;
+        nb[2] = (ea + 2 >= e && ea + 2 < hi) ? x.z : -1;
+        nb[3] = (ea + 3 >= e && ea + 3 < hi) ? x.w : -1;
+        return ea + 4;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; k++) nb[k] = (e + k < hi) ? ld_stream(ci + e + k) : -1;
+    return e + 4;
 }
 // read-only load through L1 (row offsets)
 __device__ __forceinline__ int ld_ro(const int *p) { return __ldg(p); }

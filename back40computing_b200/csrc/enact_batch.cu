@@ -229,8 +229,8 @@ int b40c_msbfs_extract(b40c_bfs_problem *p, int slot, int32_t *h_labels)
 {
     b40c::clear_error();
     if (!p || !h_labels) return b40c::fail(B40C_ERROR_INVALID_VALUE, "null argument");
-    // slots past k hold the sources that joined the batch (b40c_msbfs_join)
-    if (slot < 0 || slot >= std::max(p->ms_k, std::min(64, (int)p->ms_labels_k)))
+    // slots past k hold the sources sent to join the batch (b40c_msbfs_join)
+    if (slot < 0 || slot >= std::min(p->ms_k + p->ms_joins, std::max(p->ms_k, std::min(64, (int)p->ms_labels_k))))
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "no source %d in the last batch", slot);
     DeviceGuard guard(p->device);
     int rc = read_state(p);

@@ -25,7 +25,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     k.vcap = (int32_t)p->vcap[0];
     k.ecap = (int32_t)(pingpong ? std::min(p->ecap[0], p->ecap[1]) : p->ecap[0]);
     const void *kern = (const void *)dev::edge_kernel<kThreads, PRED>;
-    const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
+    const size_t smem = kernel_smem<dev::ExpandSmem<kThreads, PRED>>(pol);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     if ((rc = begin_enact(p, src, depth_limit))) return rc;

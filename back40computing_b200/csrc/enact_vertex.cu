@@ -40,7 +40,7 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
                                                          : (const void *)dev::ec_kernel<kThreads, PRED, false, true, false>)
                        : direction_opt  ? (const void *)dev::ec_kernel<kThreads, PRED, false>
                                         : (const void *)dev::ec_kernel<kThreads, PRED, false, false, false>;
-    const size_t smem = sizeof(dev::ExpandSmem<kThreads, PRED>);
+    const size_t smem = kernel_smem<dev::ExpandSmem<kThreads, PRED>>(pol);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     if ((rc = begin_enact(p, src, depth_limit))) return rc;

@@ -91,7 +91,7 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
                     const int start = max(Pi, cs);
                     s.rel[j] = start - cs;
                     s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
-                    s.fm[j] = ld_cg64(fcur + ld_cg(in.v + i)) & s.active;
+                    s.fm[j] = ld_keep64(fcur + ld_cg(in.v + i)) & s.active;
                 }
             }
             const int c = __syncthreads_count(inside);
@@ -141,7 +141,7 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
         __syncthreads();  // run tables consumed: they now collect the sub-round's output
         unsigned long long nw[PER];
 #pragma unroll
-        for (int t = 0; t < PER; t++) nw[t] = (w[t] >= 0) ? (f[t] & ~ld_cg64(m.visited + w[t])) : 0ull;
+        for (int t = 0; t < PER; t++) nw[t] = (w[t] >= 0) ? (f[t] & ~ld_keep64(m.visited + w[t])) : 0ull;
         unsigned long long set[PER];
 #pragma unroll
         for (int t = 0; t < PER; t++) set[t] = nw[t] ? (nw[t] & ~atomicOr(m.visited + w[t], nw[t])) : 0ull;
@@ -155,7 +155,7 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
                 while (bits) {
                     const int src = __ffsll((long long)bits) - 1;
                     bits &= bits - 1;
-                    m.labels[(long long)src * n + w[t]] = level + 1 - s.off[src];
+                    st_stream(m.labels + (long long)src * n + w[t], level + 1 - s.off[src]);
                 }
                 first[t] = atomicOr(fnext + w[t], set[t]) == 0ull;
             }
@@ -227,7 +227,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             // vertices without edges are never reached (their labels are set at the end)
             const bool iso = inr && p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u);
             if (inr && !iso) {
-                vold = ld_cg64(m.visited + v);
+                vold = ld_keep64(m.visited + v);
                 missing = active & ~vold;
                 if (missing) {
                     r0 = ld_ro(p.row_offsets + v);
@@ -238,19 +238,25 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             if (missing && p.hub2) {
                 // the vertex's two highest-degree neighbours first (one coalesced load)
                 const int2 h = p.hub2[v];
-                if (h.x >= 0) acc |= ld_cg64(fcur + h.x) & missing;
-                if (h.y >= 0) acc |= ld_cg64(fcur + h.y) & missing;
+                if (h.x >= 0) acc |= ld_keep64(fcur + h.x) & missing;
+                if (h.y >= 0) acc |= ld_keep64(fcur + h.y) & missing;
                 if (acc == missing || r1 - r0 <= 2) missing = 0;  // nothing left to look for
             }
             const bool longlist = missing && (r1 - r0) > kPullLongList;
             if (missing && !longlist) {
-                for (int e = r0; e < r1 && acc != missing; e += U) {
-                    int nb[U];
+                for (int e = r0; e < r1 && acc != missing;) {
+                    // eight neighbours per step from two 16-byte loads
+                    int nb[U], q0[4], q1[4];
+                    e = ld_quad(p.column_indices, p.edges, e, r1, q0);
+                    e = ld_quad(p.column_indices, p.edges, e, r1, q1);
 #pragma unroll
-                    for (int k = 0; k < U; k++) nb[k] = (e + k < r1) ? ld_stream(p.column_indices + e + k) : -1;
+                    for (int k = 0; k < 4; k++) {
+                        nb[k] = q0[k];
+                        nb[4 + k] = q1[k];
+                    }
                     unsigned long long fm[U];
 #pragma unroll
-                    for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_cg64(fcur + nb[k]) : 0ull;
+                    for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_keep64(fcur + nb[k]) : 0ull;
 #pragma unroll
                     for (int k = 0; k < U; k++) acc |= fm[k] & missing;
                 }
@@ -264,7 +270,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
                 unsigned long long a = 0;
                 for (int eb = lr0; eb < lr1; eb += 32) {
                     const int ee = eb + lane;
-                    if (ee < lr1) a |= ld_cg64(fcur + ld_stream(p.column_indices + ee)) & miss;
+                    if (ee < lr1) a |= ld_keep64(fcur + ld_stream(p.column_indices + ee)) & miss;
                     for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
                     if (a == miss) break;
                 }
@@ -283,7 +289,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             while (wor) {
                 const int src = __ffsll((long long)wor) - 1;
                 wor &= wor - 1;
-                if ((acc >> src) & 1ull) m.labels[(long long)src * n + v] = level + 1 - s.off[src];
+                if ((acc >> src) & 1ull) st_stream(m.labels + (long long)src * n + v, level + 1 - s.off[src]);
             }
             const bool push = acc && r1 > r0;
             const unsigned bal = __ballot_sync(0xffffffffu, push);
@@ -479,7 +485,7 @@ __global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
             while (wor) {
                 const int src = __ffsll((long long)wor) - 1;
                 wor &= wor - 1;
-                if ((miss >> src) & 1ull) m.labels[(long long)src * n + v] = -1;
+                if ((miss >> src) & 1ull) st_stream(m.labels + (long long)src * n + v, -1);
             }
         }
     }

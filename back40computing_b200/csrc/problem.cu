@@ -145,6 +145,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.subgrid_edges = pol.subgrid_frontier_edges > 0 ? pol.subgrid_frontier_edges : 0;
     k.bu_scan = pol.bottom_up_scan;
     k.bu_long = pol.bottom_up_long_list;
+    k.hist_log = pol.history_cull > 0 ? kHistLog : 0;
     k.bu_defer = pol.bottom_up_defer_frontier > 0 ? 1 : 0;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
@@ -173,6 +174,7 @@ b40c_bfs_policy default_policy(int strategy)
     pol.bottom_up_defer_frontier = 1;
     pol.subgrid_frontier_edges = -1;
     pol.bottom_up_long_list = 256;
+    pol.history_cull = -1;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     if (strategy == B40C_DIRECTION_OPTIMIZING) {
         // measured on B200 over 16 sources: the kernel variant carrying the
@@ -208,6 +210,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->bottom_up_defer_frontier) d.bottom_up_defer_frontier = in->bottom_up_defer_frontier > 0 ? 1 : -1;
         if (in->subgrid_frontier_edges) d.subgrid_frontier_edges = in->subgrid_frontier_edges > 0 ? in->subgrid_frontier_edges : -1;
         if (in->bottom_up_long_list) d.bottom_up_long_list = in->bottom_up_long_list;
+        if (in->history_cull) d.history_cull = in->history_cull > 0 ? 1 : -1;
     }
     if (d.threads != kThreads)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: %d)", d.threads, kThreads);

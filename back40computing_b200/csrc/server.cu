@@ -49,6 +49,7 @@ struct Query {
     int64_t ticket;
     int32_t graph, source, depth_limit;
     int32_t *h_labels;
+    bool pinned;  // h_labels is page-locked: copied asynchronously behind the search
     int64_t arrival_ns;
 };
 
@@ -144,6 +145,21 @@ void finish_batch(b40c_server *s, Batch &b, int status, int64_t finish_ns)
     }
     s->joined_queries += taken;
     s->batched_queries += taken;
+    // labels bound for pageable host memory: copied now, from the rows the batch
+    // left on the device (its graph's next batch cannot start before this
+    // returns); a copy queued behind the search would have made the dispatcher
+    // wait for the whole search
+    if (status == B40C_SUCCESS) {
+        for (size_t i = 0; i < b.queries.size(); i++) {
+            const Query &q = b.queries[i];
+            if (!q.h_labels || q.pinned) continue;
+            const int32_t *src = b.single ? g.p->d_labels : g.p->d_ms_labels + i * (size_t)g.nodes;
+            if (cudaMemcpy(q.h_labels, src, sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost) != cudaSuccess) {
+                cudaGetLastError();
+                status = B40C_ERROR_INVALID_VALUE;
+            }
+        }
+    }
     float t0 = 0.f, t1 = 0.f;
     if (status == B40C_SUCCESS &&
         (cudaEventElapsedTime(&t0, s->base_ev, s->gpu_ev[2 * b.slot]) != cudaSuccess ||
@@ -201,7 +217,7 @@ int issue(b40c_server *s, Batch &b)
         CUDA_TRY(cudaEventRecord(s->gpu_ev[2 * b.slot + 1], st), "event record");
         CUDA_TRY(cudaMemcpyAsync(&l->max_level, &p->st->max_level, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
                  "depth copy");
-        if (q.h_labels)
+        if (q.h_labels && q.pinned)
             CUDA_TRY(cudaMemcpyAsync(q.h_labels, p->d_labels, sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, st),
                      "label copy");
     } else {
@@ -218,7 +234,7 @@ int issue(b40c_server *s, Batch &b)
         CUDA_TRY(cudaMemcpyAsync(&l->taken, &p->d_ms_join->taken, sizeof(int32_t), cudaMemcpyDeviceToHost, st),
                  "join count copy");
         for (int i = 0; i < k; i++)
-            if (b.queries[i].h_labels)
+            if (b.queries[i].h_labels && b.queries[i].pinned)
                 CUDA_TRY(cudaMemcpyAsync(b.queries[i].h_labels, p->d_ms_labels + (size_t)i * (size_t)g.nodes,
                                          sizeof(int32_t) * g.nodes, cudaMemcpyDeviceToHost, st),
                          "label copy");
@@ -251,7 +267,7 @@ bool join_waiting(b40c_server *s, Batch &b)
         g.ready.pop_front();
         b.queries.push_back(q);
         b.join_ns.push_back(s->now());
-        if (q.h_labels &&
+        if (q.h_labels && q.pinned &&
             cudaMemcpyAsync(q.h_labels, p->d_ms_labels + (size_t)slot * (size_t)g.nodes, sizeof(int32_t) * g.nodes,
                             cudaMemcpyDeviceToHost, st) != cudaSuccess)
             cudaGetLastError();  // the query then reports the batch's status with stale labels: not expected
@@ -421,6 +437,14 @@ int64_t enqueue(b40c_server *s, int32_t graph, int32_t source, int32_t depth_lim
     q.source = source;
     q.depth_limit = depth_limit < 0 ? -1 : depth_limit;
     q.h_labels = h_labels;
+    q.pinned = false;
+    if (h_labels) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, h_labels) == cudaSuccess)
+            q.pinned = a.type == cudaMemoryTypeHost;
+        else
+            cudaGetLastError();
+    }
     q.arrival_ns = arrival_ns < 0 ? s->now() : arrival_ns;
     b40c_server_result r{};
     r.ticket = q.ticket;

@@ -123,6 +123,10 @@ typedef struct b40c_bfs_policy {
                                       first probes found no parent) is searched by its whole warp, 32
                                       neighbours at a time; shorter lists are scanned by one lane, four at
                                       a time (>= 4; 0 = default 256) */
+    int32_t history_cull;          /* top-down levels and contractions: each CTA remembers, in a 4096-entry
+                                      shared-memory table, the neighbours it has already sent to the
+                                      visited test and drops repeats without touching the visited mask
+                                      (the reference's history culling): 1 = on, -1 = off (default) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

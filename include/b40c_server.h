@@ -116,8 +116,10 @@ int b40c_server_plan_bytes(int64_t nodes, int64_t edges, int32_t max_batch, int6
 int b40c_server_now_ns(b40c_server *server, int64_t *now_ns);
 
 /* Queues one query.  depth_limit < 0 = unlimited.  h_labels (may be NULL)
- * receives the query's labels (nodes int32 values) when it finishes; page-locked memory
- * (b40c_host_alloc) lets the copy run asynchronously.  arrival_ns < 0 =
+ * receives the query's labels (nodes int32 values) when it finishes.  Into
+ * page-locked memory (b40c_host_alloc) the copy is queued behind the search
+ * and overlaps other work; into pageable memory the server copies when the
+ * search has finished (the dispatcher is busy for that copy only).  arrival_ns < 0 =
  * now; a future arrival time makes the query eligible only then (used to
  * replay a timed request stream).  *ticket identifies the query. */
 int b40c_server_submit(b40c_server *server, int32_t graph_id, int32_t source, int32_t depth_limit,

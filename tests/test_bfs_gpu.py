@@ -542,3 +542,26 @@ def test_join_taken_while_a_long_batch_runs():
         assert np.array_equal(p.labels_of(1 + j), want), f"joined source {s}"
         assert depths[1 + j] == int(want.max()) + 1
     p.Destroy()
+
+
+@pytest.mark.parametrize("strategy", STRATS)
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("preds", [False, True])
+def test_history_cull(strategy, mode, preds):
+    """With the per-CTA history table on, repeats of neighbours already sent to
+    the visited test are dropped in shared memory: distances still equal the
+    oracle's and predecessors stay valid (R-MAT hubs repeat a lot; the
+    lattice's neighbours repeat across levels)."""
+    pol = N.Policy()
+    pol.history_cull = 1
+    for kind, args in (("rmat", (1 << 15, 1 << 19)), ("grid2d", (120,)), ("random", (20000, 60000))):
+        g = _graph(kind, *args)
+        p = CsrProblem.from_graph(g, mark_predecessors=preds)
+        for s in sample_sources(g, 2, seed=13):
+            got = search(p, int(s), strategy=strategy, mode=mode, policy=pol)
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            if preds:
+                assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+            else:
+                assert oracle.compare_labels(got, want) == -1, f"{kind} source {s}"
+        p.Destroy()

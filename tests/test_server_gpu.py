@@ -229,7 +229,11 @@ def test_queries_join_a_running_batch_with_exact_labels():
         t0 = srv.now_ns() + 20_000_000
         first = [0, 999]
         later = [500_500, 999_999, 1234, 777_000]
-        outs = {s: np.empty(g.nodes, np.int32) for s in first + later}
+        import torch
+        # pageable arrays for the first queries (copied when their batch retires),
+        # page-locked ones for the joining queries (copies queued behind the search)
+        outs = {s: np.empty(g.nodes, np.int32) for s in first}
+        outs.update({s: torch.empty(g.nodes, dtype=torch.int32, pin_memory=True).numpy() for s in later})
         tickets = {}
         for s in first:
             tickets[s] = srv.submit(gid, s, -1, labels=outs[s], arrival_ns=t0)
