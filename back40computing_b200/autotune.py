@@ -38,6 +38,7 @@ KINDS = ("direction-optimizing", "expand-contract", "batched")
 
 # knob -> values tried (0 = the library default)
 SEARCH_SPACE = {
+    "threads": [256, 512, 128],
     "ctas_per_sm": [1, 2, 3, 4],
     "chunk_edges": [512, 1024, 2048],
     "warp_gather_threshold": [32, 64, 128],
@@ -48,14 +49,17 @@ SEARCH_SPACE = {
     "bitmask_precheck": [1, -1],
     "warp_cull": [1, -1],
     "subgrid_frontier_edges": [-1, 4096, 16384, 65536],
+    "history_cull": [-1, 1],
 }
 # knobs that matter to each kind of search
 KNOBS = {
-    "direction-optimizing": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
-                             "bottom_up_alpha", "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck"],
-    "expand-contract": ["ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
-                        "warp_gather_threshold", "cta_gather_threshold", "bitmask_precheck", "warp_cull"],
-    "batched": ["ctas_per_sm", "bottom_up_alpha"],
+    "direction-optimizing": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
+                             "bottom_up_alpha", "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck",
+                             "history_cull"],
+    "expand-contract": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
+                        "warp_gather_threshold", "cta_gather_threshold", "bitmask_precheck", "warp_cull",
+                        "history_cull"],
+    "batched": ["threads", "ctas_per_sm", "bottom_up_alpha"],
 }
 
 
@@ -150,9 +154,11 @@ def _measure(problem, kind, sources, pol, reps=2) -> float:
     return float(problem.recent_search_ms(reps * len(sources)).mean())
 
 
-def tune_class(graphs, kind, sources_per_graph=4, passes=2, log=print) -> tuple[dict, float, float]:
-    """Coordinate search from the defaults: each knob in turn takes the value
-    that minimises the summed time over the class's representatives."""
+def tune_class(graphs, kind, sources_per_graph=4, passes=2, log=print, start=None,
+               knobs=None) -> tuple[dict, float, float]:
+    """Coordinate search from the defaults (or from `start`, e.g. the cached
+    policy): each knob in turn (of `knobs`, default all the kind's) takes the
+    value that minimises the summed time over the class's representatives."""
     from .bfs import CsrProblem
     from .graph import sample_sources
     probs = []
@@ -170,11 +176,13 @@ def tune_class(graphs, kind, sources_per_graph=4, passes=2, log=print) -> tuple[
             log(f"    {d}: {e}")
             return float("inf")
 
-    best = {}
+    best = dict(start or {})
     base = best_t = cost(best)
     for _ in range(passes):
         changed = False
-        for knob in KNOBS[kind]:
+        for knob in (knobs or KNOBS[kind]):
+            if knob not in KNOBS[kind]:
+                continue
             for v in SEARCH_SPACE[knob]:
                 if best.get(knob) == v:
                     continue
@@ -196,6 +204,7 @@ def main(argv=None):
     ap.add_argument("--out", default=CACHE)
     ap.add_argument("--classes", default=",".join(CLASSES))
     ap.add_argument("--kinds", default=",".join(KINDS))
+    ap.add_argument("--knobs", default="", help="tune only these knobs (comma list), from the cached policy")
     args = ap.parse_args(argv)
     import torch
     torch.cuda.init()
@@ -210,7 +219,9 @@ def main(argv=None):
     for cls in args.classes.split(","):
         for kind in args.kinds.split(","):
             print(f"[{cls} / {kind}]", flush=True)
-            best, base, t = tune_class(reps[cls], kind)
+            knobs = [k for k in args.knobs.split(",") if k] or None
+            start = out["classes"].get(cls, {}).get(kind, {}).get("policy") if knobs else None
+            best, base, t = tune_class(reps[cls], kind, start=start, knobs=knobs)
             out["classes"].setdefault(cls, {})[kind] = {
                 "policy": best, "default_ms": base, "tuned_ms": t,
                 "graphs": [name for name, _ in reps[cls]]}

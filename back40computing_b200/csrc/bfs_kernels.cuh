@@ -196,7 +196,7 @@ __device__ __forceinline__ void discover_batch(const BfsParams &p, ExpandSmem<B,
                 hist[h] = (uint32_t)v[t];
         }
         word[t] = 0;
-        if (go[t] && precheck) word[t] = ld_mask(s.mask + (v[t] >> 5));
+        if (go[t] && precheck) word[t] = p.precheck == 2 ? ld_cg(s.mask + (v[t] >> 5)) : ld_mask(s.mask + (v[t] >> 5));
     }
     bool found[U];
     if (LISTS && s.ul_in >= 0) {
@@ -1528,7 +1528,7 @@ constexpr unsigned long long kDeferMinShare = 512;
 // BU = false builds a top-down-only variant (plain expand-contract searches):
 // without the bottom-up code the kernel needs fewer registers.
 template <int B, bool PRED, bool LISTS, bool SUBGRID = false, bool BU = true>
-__global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
+__global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem<B, PRED> &s = *reinterpret_cast<ExpandSmem<B, PRED> *>(smem_raw);
@@ -1782,7 +1782,7 @@ __global__ void __launch_bounds__(B, 4) ec_kernel(BfsParams p)
 // With `hybrid`, a persistent launch returns when the edge frontier exceeds
 // gridDim * saturation items (SATURATION_QUIT, enactor_hybrid.cuh:571).
 template <int B, bool PRED>
-__global__ void __launch_bounds__(B, 4) edge_kernel(BfsParams p)
+__global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem<B, PRED> &s = *reinterpret_cast<ExpandSmem<B, PRED> *>(smem_raw);

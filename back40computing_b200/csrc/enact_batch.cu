@@ -115,8 +115,13 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     m.k = k;
     m.rows = p->ms_labels_k;
     m.pull_ok = p->symmetric == 1 ? 1 : 0;
-    const void *kern = (const void *)dev::msbfs_kernel<kThreads>;
-    const size_t smem = sizeof(dev::MsSmem<kThreads>);
+    const int block = pol.threads;
+    const void *kern = block == 128   ? (const void *)dev::msbfs_kernel<128>
+                       : block == 512 ? (const void *)dev::msbfs_kernel<512>
+                                      : (const void *)dev::msbfs_kernel<256>;
+    const size_t smem = block == 128   ? sizeof(dev::MsSmem<128>)
+                        : block == 512 ? sizeof(dev::MsSmem<512>)
+                                       : sizeof(dev::MsSmem<256>);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     CUDA_TRY(cudaEventRecord(p->ev0, p->stream), "event record");
@@ -135,7 +140,7 @@ int enact_batch(b40c_bfs_problem *p, const int32_t *sources, const int32_t *limi
     p->ms_joins = 0;
     if ((rc = mark_search_start(p))) return rc;
     void *args[] = {&bp, &m};
-    CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream),
+    CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(block), args, smem, p->stream),
              "cooperative launch of the batched kernel");
     p->ms_k = k;
     p->needs_init = true;  // the single-source labels/mask are untouched but the queues were reused

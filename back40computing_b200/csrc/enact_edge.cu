@@ -9,7 +9,7 @@ namespace rt {
 
 namespace {
 
-template <bool PRED>
+template <int B, bool PRED>
 int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                  int32_t depth_limit)
 {
@@ -24,8 +24,8 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     k.edge_pingpong = pingpong ? 1 : 0;
     k.vcap = (int32_t)p->vcap[0];
     k.ecap = (int32_t)(pingpong ? std::min(p->ecap[0], p->ecap[1]) : p->ecap[0]);
-    const void *kern = (const void *)dev::edge_kernel<kThreads, PRED>;
-    const size_t smem = kernel_smem<dev::ExpandSmem<kThreads, PRED>>(pol);
+    const void *kern = (const void *)dev::edge_kernel<B, PRED>;
+    const size_t smem = kernel_smem<dev::ExpandSmem<B, PRED>>(pol);
     int grid = 0;
     if ((rc = persistent_grid(p, kern, pol, max_grid, smem, &grid))) return rc;
     if ((rc = begin_enact(p, src, depth_limit))) return rc;
@@ -39,7 +39,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     if (mode == B40C_ENACT_GRAPH) {
         if ((rc = mark_search_start(p))) return rc;
         KernelNode init{init_kernel_ptr<PRED>(false, true), dim3(init_grid(p, true)), dim3(kThreads), 0, k};
-        KernelNode body[2] = {{kern, dim3(grid), dim3(kThreads), smem, kc}, {kern, dim3(grid), dim3(kThreads), smem, kx}};
+        KernelNode body[2] = {{kern, dim3(grid), dim3(B), smem, kc}, {kern, dim3(grid), dim3(B), smem, kx}};
         if ((rc = run_graph(p, strategy, init, body, 2))) return rc;
         return finish_timing(p);
     }
@@ -50,8 +50,8 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     // one level as two launches (contract, expand); returns with the state read back
     auto two_phase_level = [&]() -> int {
         int r;
-        if ((r = launch_plain(p, kern, grid, smem, kc, "contract launch"))) return r;
-        if ((r = launch_plain(p, kern, grid, smem, kx, "expand launch"))) return r;
+        if ((r = launch_plain(p, kern, grid, B, smem, kc, "contract launch"))) return r;
+        if ((r = launch_plain(p, kern, grid, B, smem, kx, "expand launch"))) return r;
         return read_state(p);
     };
 
@@ -66,7 +66,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         while (true) {
             CUDA_TRY(cudaMemsetAsync(&p->st->barrier, 0, sizeof(unsigned long long), p->stream), "barrier reset");
             CUDA_TRY(cudaMemsetAsync(&p->st->saturated, 0, sizeof(int32_t), p->stream), "flag reset");
-            if ((rc = launch_cooperative(p, kern, grid, smem, kf, "cooperative launch of the contract-expand kernel")))
+            if ((rc = launch_cooperative(p, kern, grid, B, smem, kf, "cooperative launch of the contract-expand kernel")))
                 return rc;
             if ((rc = read_state(p))) return rc;
             if (p->h_st->error || p->h_st->done || !p->h_st->saturated) break;
@@ -89,7 +89,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         kf.phase_mask = 3;
         kf.max_levels = INT32_MAX;
         kf.skip_arrival_cta = injected_skip_cta();
-        if ((rc = launch_cooperative(p, kern, grid, smem, kf, "cooperative launch of the contract-expand kernel")))
+        if ((rc = launch_cooperative(p, kern, grid, B, smem, kf, "cooperative launch of the contract-expand kernel")))
             return rc;
     } else if (mode == B40C_ENACT_ITERATIVE) {
         if ((rc = read_state(p))) return rc;
@@ -106,8 +106,15 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
 int enact_edge(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int max_grid, const b40c_bfs_policy &pol,
                int32_t depth_limit)
 {
-    return p->mark_pred ? enact_edge_t<true>(p, strategy, mode, src, max_grid, pol, depth_limit)
-                        : enact_edge_t<false>(p, strategy, mode, src, max_grid, pol, depth_limit);
+#define B40C_EDGE(B)                                                                      \
+    (p->mark_pred ? enact_edge_t<B, true>(p, strategy, mode, src, max_grid, pol, depth_limit) \
+                  : enact_edge_t<B, false>(p, strategy, mode, src, max_grid, pol, depth_limit))
+    switch (pol.threads) {
+    case 128: return B40C_EDGE(128);
+    case 512: return B40C_EDGE(512);
+    default: return B40C_EDGE(256);
+    }
+#undef B40C_EDGE
 }
 
 }  // namespace rt

@@ -60,20 +60,24 @@ inline int mark_search_start(b40c_bfs_problem *p)
     return B40C_SUCCESS;
 }
 
-inline int launch_cooperative(b40c_bfs_problem *p, const void *kern, int grid, size_t smem, BfsParams &k,
+inline int launch_cooperative(b40c_bfs_problem *p, const void *kern, int grid, int block, size_t smem, BfsParams &k,
                               const char *what)
 {
     void *args[] = {&k};
-    CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream), what);
+    CUDA_TRY(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(block), args, smem, p->stream), what);
     return B40C_SUCCESS;
 }
 
-inline int launch_plain(b40c_bfs_problem *p, const void *kern, int grid, size_t smem, BfsParams &k, const char *what)
+inline int launch_plain(b40c_bfs_problem *p, const void *kern, int grid, int block, size_t smem, BfsParams &k,
+                        const char *what)
 {
     void *args[] = {&k};
-    CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(kThreads), args, smem, p->stream), what);
+    CUDA_TRY(cudaLaunchKernel(kern, dim3(grid), dim3(block), args, smem, p->stream), what);
     return B40C_SUCCESS;
 }
+
+// Kernel variants are built for these CTA sizes (policy.threads).
+constexpr int kCtaSizes[3] = {128, 256, 512};
 
 // Test-only fault injection: B40C_TEST_SKIP_ARRIVAL_CTA=<cta> makes that CTA
 // of a persistent launch leave at its first whole-grid end-of-level barrier

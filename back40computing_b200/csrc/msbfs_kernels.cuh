@@ -382,7 +382,7 @@ __device__ __forceinline__ void take_joins(const BfsParams &p, const MsParams &m
 
 // Whole batched search in one persistent cooperative grid.
 template <int B>
-__global__ void __launch_bounds__(B, 4) msbfs_kernel(BfsParams p, MsParams m)
+__global__ void __launch_bounds__(B, 1024 / B) msbfs_kernel(BfsParams p, MsParams m)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     MsSmem<B> &s = *reinterpret_cast<MsSmem<B> *>(smem_raw);

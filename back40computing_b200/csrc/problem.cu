@@ -129,7 +129,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.warp_thresh = pol.warp_gather_threshold;
     k.cta_thresh = pol.cta_gather_threshold;
     k.warp_cull = pol.warp_cull;
-    k.precheck = pol.bitmask_precheck;
+    k.precheck = pol.bitmask_precheck > 0 ? pol.bitmask_precheck : 0;  // -1 (off) must not read as true
     k.saturation = pol.saturation_quit;
     k.persistent = 0;
     k.skip_arrival_cta = -1;
@@ -199,7 +199,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->cta_gather_threshold) d.cta_gather_threshold = in->cta_gather_threshold;
         if (in->saturation_quit) d.saturation_quit = in->saturation_quit;
         if (in->warp_cull) d.warp_cull = in->warp_cull > 0 ? 1 : 0;
-        if (in->bitmask_precheck) d.bitmask_precheck = in->bitmask_precheck > 0 ? 1 : 0;
+        if (in->bitmask_precheck) d.bitmask_precheck = in->bitmask_precheck > 0 ? std::min(in->bitmask_precheck, 2) : -1;
         if (in->queue_allocation) d.queue_allocation = in->queue_allocation;
         if (in->bottom_up_alpha) d.bottom_up_alpha = in->bottom_up_alpha;
         if (in->bottom_up_beta) d.bottom_up_beta = in->bottom_up_beta;
@@ -212,8 +212,9 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->bottom_up_long_list) d.bottom_up_long_list = in->bottom_up_long_list;
         if (in->history_cull) d.history_cull = in->history_cull > 0 ? 1 : -1;
     }
-    if (d.threads != kThreads)
-        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: %d)", d.threads, kThreads);
+    if (d.threads != 128 && d.threads != 256 && d.threads != 512)
+        return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: 128, 256, 512)",
+                          d.threads);
     if (d.chunk_edges < 256 || d.chunk_edges > dev::kChunkMax || (d.chunk_edges & 31))
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.chunk_edges must be a multiple of 32 in [256, %d]",
                           dev::kChunkMax);

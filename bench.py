@@ -72,6 +72,9 @@ def parse():
                     help="which of the extra measurements to run (comma list of batched, lattices, served)")
     ap.add_argument("--only-extras", action="store_true",
                     help="run just the extra measurements (no single-source line); prints them as one JSON line")
+    ap.add_argument("--ablate", action="store_true",
+                    help="policy ablations (the reference's gather / cull microbenchmarks, test/bfs/microbench/): "
+                         "each knob's variants interleaved on the same searches; prints one JSON line and exits")
     return ap.parse_args()
 
 
@@ -248,6 +251,65 @@ def level_report(problem, enact, srcs):
         out.append({"source": int(s), "search_us": round(search_us, 2), "levels": levels})
     problem.set_instrument(False)
     return out
+
+
+# Policy ablations: (strategy, knob, values).  Each variant changes one knob of
+# the tuned policy; the first value of every row is the reference point.
+ABLATIONS = [
+    (4, "bottom_up_hub_probes", [1, -1]),
+    (4, "bottom_up_defer_frontier", [1, -1]),
+    (4, "bottom_up_long_list", [256, 64]),
+    (4, "bitmask_precheck", [-1, 1]),
+    (4, "history_cull", [-1, 1]),
+    (4, "ctas_per_sm", [4, 3, 2]),
+    (4, "small_frontier_edges", [1024, 256, 4096]),
+    (0, "queue_allocation", [2, 1]),
+    (0, "chunk_edges", [2048, 1024, 512]),
+    (0, "warp_gather_threshold", [32, 128]),
+    (0, "cta_gather_threshold", [512, 256, 2048]),
+    (0, "bitmask_precheck", [1, -1]),
+    (0, "warp_cull", [-1, 1]),
+    (0, "history_cull", [-1, 1]),
+    (0, "ctas_per_sm", [4, 3, 2]),
+]
+
+
+def ablate(cfg_name, sources=16, rounds=3):
+    """Device time per search of one-knob variants of the tuned policy, the
+    variants of a row interleaved round by round on the same sources."""
+    from back40computing_b200 import CsrProblem, autotune
+    from back40computing_b200 import _native as N
+    from back40computing_b200.bfs import ENACTORS
+    g, fixed = build_graph(cfg_name)
+    srcs = sources_for(g, fixed, sources)
+    p = CsrProblem.from_graph(g)
+    rows = []
+    for strategy, knob, values in ABLATIONS:
+        kind = {0: "expand-contract", 4: "direction-optimizing"}[strategy]
+        tuned = autotune.policy_for(g, kind)
+        enactors = []
+        for v in values:
+            pol = N.Policy()
+            if tuned is not None:
+                for f, _ in N.Policy._fields_:
+                    setattr(pol, f, getattr(tuned, f))
+            setattr(pol, knob, v)
+            enactors.append(ENACTORS[strategy](policy=pol))
+        N.check(p.Reset(enactors[0].GetFrontierType(), 1.3), "Reset")
+        times = [[] for _ in values]
+        for e in enactors:  # warm-up
+            N.check(e._enact(p, int(srcs[0]), 0, 0))
+        for _ in range(rounds):
+            for i, e in enumerate(enactors):
+                for s in srcs:
+                    N.check(e._enact(p, int(s), 0, 0))
+                times[i].extend(p.recent_search_ms(len(srcs)).tolist())
+        rows.append({"strategy": STRATEGY_NAMES[strategy], "knob": knob,
+                     "us_per_search": {str(v): round(float(np.mean(t)) * 1e3, 1) for v, t in zip(values, times)},
+                     "median_us": {str(v): round(float(np.median(t)) * 1e3, 1) for v, t in zip(values, times)}})
+        print(json.dumps(rows[-1]), file=sys.stderr, flush=True)
+    p.Destroy()
+    return {"workload": CONFIGS[cfg_name]["workload"], "sources": len(srcs), "rounds": rounds, "ablations": rows}
 
 
 def max_over_ranks(x, dist=None, device="cuda"):
@@ -513,6 +575,13 @@ def main():
     from back40computing_b200 import CsrProblem
     from back40computing_b200 import _native as N
     from back40computing_b200.bfs import ENACTORS
+
+    if args.ablate:
+        if rank == 0:
+            print(json.dumps(ablate(args.config, min(args.sources, 16), max(args.steps, 2))), flush=True)
+        if world > 1:
+            dist.destroy_process_group()
+        return
 
     if args.only_extras:
         if rank == 0:

@@ -87,8 +87,9 @@ typedef struct b40c_bfs_policy {
     int32_t saturation_quit;       /* hybrid: queue items per CTA above which the search leaves the fused kernel */
     int32_t warp_cull;             /* 1: drop duplicate neighbours within a warp before the bitmask test,
                                       -1: do not (default) */
-    int32_t bitmask_precheck;      /* 1: read the visited word before the atomic test-and-set (default),
-                                      -1: go straight to the atomic (default of direction-optimizing) */
+    int32_t bitmask_precheck;      /* 1: read the visited word (through L1) before the atomic test-and-set
+                                      (default), 2: read it from L2 (never stale), -1: go straight to the
+                                      atomic (default of direction-optimizing) */
     int32_t queue_allocation;      /* frontier-slot allocation per tile of output: 1 = decoupled look-back
                                       over tile ids, 2 = one packed 64-bit atomicAdd; 0 = default */
     int32_t bottom_up_alpha;       /* direction-optimizing: go bottom-up when frontier edges exceed
