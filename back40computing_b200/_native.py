@@ -50,6 +50,7 @@ class Policy(C.Structure):
         ("subgrid_frontier_edges", C.c_int32),
         ("bottom_up_long_list", C.c_int32),
         ("history_cull", C.c_int32),
+        ("bottom_up_prefetch", C.c_int32),
     ]
 
 

@@ -46,16 +46,17 @@ SEARCH_SPACE = {
     "small_frontier_edges": [256, 1024, 2048, 4096, 16384],
     "bottom_up_alpha": [6, 14, 24, 48],
     "bottom_up_beta": [12, 24, 48],
-    "bitmask_precheck": [1, -1],
+    "bitmask_precheck": [1, -1, 2],
     "warp_cull": [1, -1],
     "subgrid_frontier_edges": [-1, 4096, 16384, 65536],
     "history_cull": [-1, 1],
+    "bottom_up_prefetch": [1, -1],
 }
 # knobs that matter to each kind of search
 KNOBS = {
     "direction-optimizing": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
                              "bottom_up_alpha", "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck",
-                             "history_cull"],
+                             "history_cull", "bottom_up_prefetch"],
     "expand-contract": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
                         "warp_gather_threshold", "cta_gather_threshold", "bitmask_precheck", "warp_cull",
                         "history_cull"],

@@ -75,7 +75,25 @@ struct ExpandSmem {
     unsigned long long scan_warp[B / 32];
     unsigned long long prefix;
     uint32_t *hist;                    // history cull table (dynamic shared memory past this struct), or null
+    struct BuPrefetch *pf;             // bottom-up chunk prefetch buffer (dynamic shared memory), or null
+    unsigned pf_phase;                 // parity of its mbarrier's next completion
 };
+
+// The first bottom-up level of a run walks its CTA's vertex ids in chunks of
+// kChunkMax.  With p.bu_prefetch, the next chunk's visited words, row offsets
+// and hub pairs are staged into shared memory by bulk copies (cp.async.bulk,
+// one mbarrier) while the current chunk's lists are scanned, so a chunk starts
+// from shared memory instead of two dependent round trips to L2/HBM.  Entries
+// a 16-byte copy cannot cover (the ragged end of the vertex range) are read
+// from global memory.
+struct alignas(16) BuPrefetch {
+    int32_t rows[kChunkMax + 4];  // row_offsets[cs .. cs + nr)
+    int2 hub[kChunkMax];          // hub2[cs .. cs + nh)
+    uint32_t words[kChunkMax / 32];
+    uint64_t bar;
+    int32_t nr, nh, nw;           // entries staged (the rest: global loads)
+};
+constexpr size_t kBuPrefetchBytes = (sizeof(BuPrefetch) + 15) & ~size_t(15);
 
 // History culling (the reference's HistoryCull, two_phase/contract_atomic/
 // cta.cuh:276-297, as a B200 shared-memory filter): each CTA keeps a
@@ -88,14 +106,24 @@ struct ExpandSmem {
 constexpr uint32_t kHistEmpty = 0xffffffffu;
 __device__ __forceinline__ unsigned hist_slot(int v, int log2) { return ((unsigned)v * 2654435761u) >> (32 - log2); }
 
+// Dynamic shared memory past ExpandSmem: the history table (when on), then
+// the bottom-up prefetch buffer (when on); the caller's barrier publishes both.
 template <int B, bool PRED>
 __device__ __forceinline__ void hist_init(const BfsParams &p, ExpandSmem<B, PRED> &s, unsigned char *smem_raw)
 {
+    size_t off = (sizeof(ExpandSmem<B, PRED>) + 15) & ~size_t(15);
     s.hist = nullptr;
+    s.pf = nullptr;
+    s.pf_phase = 0;
     if (p.hist_log > 0) {
-        uint32_t *h = reinterpret_cast<uint32_t *>(smem_raw + ((sizeof(ExpandSmem<B, PRED>) + 15) & ~size_t(15)));
+        uint32_t *h = reinterpret_cast<uint32_t *>(smem_raw + off);
         for (int i = threadIdx.x; i < (1 << p.hist_log); i += B) h[i] = kHistEmpty;
-        s.hist = h;  // (the caller's barrier publishes both)
+        s.hist = h;
+        off += sizeof(uint32_t) << p.hist_log;
+    }
+    if (p.bu_prefetch) {
+        s.pf = reinterpret_cast<BuPrefetch *>(smem_raw + off);
+        if (threadIdx.x == 0) mbar_init(&s.pf->bar, 1);
     }
 }
 
@@ -414,8 +442,10 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
     if (rs >= re) return;
     int i_cur = ld_cg(in.cf + rs / kChunkGrain);  // entry owning position rs
     if (FUSED_CULL) stamp(p, pass, 0);
-    for (int cs = rs; cs < re; cs += kChunkMax) {
-        const int ce = min(cs + kChunkMax, re);
+    // sub-round length: policy.chunk_edges (a solo level kept in shared memory is one full sub-round)
+    const int chunk = defer_emit ? kChunkMax : min(max(p.chunk_edges, 256), kChunkMax);
+    for (int cs = rs; cs < re; cs += chunk) {
+        const int ce = min(cs + chunk, re);
         const int len = ce - cs;
         const bool first = FUSED_CULL && cs == rs;
         // ---- load the runs of entries i_cur.. that start before ce ----------------
@@ -650,8 +680,9 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
     constexpr int PER = kChunkMax / B;
     int rs, re;
     cta_range(q, blockIdx.x, gridDim.x, rs, re);
-    for (int cs = rs; cs < re; cs += kChunkMax) {
-        const int ce = min(cs + kChunkMax, re);
+    const int chunk = min(max(p.chunk_edges, 256), kChunkMax);
+    for (int cs = rs; cs < re; cs += chunk) {
+        const int ce = min(cs + chunk, re);
         if (tid == 0) s.out_count = 0;
         int v[PER], u[PER];
         bool valid[PER], active[PER];
@@ -888,6 +919,29 @@ __device__ __forceinline__ void write_unvisited(const BfsParams &p, Smem &s, int
         if (base + j < p.nodes) list[base + j] = s.stage[j];
 }
 
+// Thread 0: stages chunk [cs, cs + kChunkMax) of [.., re) into the prefetch
+// buffer (the buffer's previous contents must be consumed, and a CTA barrier
+// passed, before the call).  Every source is 16-byte aligned (cudaMalloc'd
+// arrays, cs a multiple of 32); sizes are rounded down to whole 16 bytes.
+__device__ __forceinline__ void bu_prefetch_issue(const BfsParams &p, BuPrefetch &f, const uint32_t *mask, int cs,
+                                                  int re)
+{
+    const int nv = min(kChunkMax, re - cs);
+    const int nr = (nv + 1) & ~3;                                  // of the nv + 1 row offsets
+    const int nh = p.hub2 ? (nv & ~1) : 0;                         // hub pairs (8 bytes each)
+    const int nw = (((nv + 31) >> 5) & ~3);                        // visited words
+    f.nr = nr;
+    f.nh = nh;
+    f.nw = nw;
+    const unsigned bytes = 4u * nr + 8u * nh + 4u * nw;
+    if (bytes == 0) return;  // the consumer sees nothing staged and waits for nothing
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(&f.bar, bytes);
+    if (nr) bulk_g2s(f.rows, p.row_offsets + cs, 4u * nr, &f.bar);
+    if (nh) bulk_g2s(f.hub, p.hub2 + cs, 8u * nh, &f.bar);
+    if (nw) bulk_g2s(f.words, mask + (cs >> 5), 4u * nw, &f.bar);
+}
+
 //
 // With `defer` (CTA-uniform) the discoveries are only counted: each thread
 // sums (1 << 32 | degree) over its discoveries and the CTA adds its total to
@@ -905,6 +959,8 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     unsigned long long found_acc = 0;  // defer: this thread's (count << 32 | degree) of discoveries
+    BuPrefetch *pf = s.pf;             // CTA-uniform
+    if (pf && tid == 0 && rs < re) bu_prefetch_issue(p, *pf, mask, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
         const bool first = cs == rs;
         if (tid == 0) {
@@ -913,23 +969,62 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
         }
         __syncthreads();  // the counters are reset before any warp appends
         if (first) stamp(p, pass, 0);
+        bool staged = false;
+        const unsigned ph = s.pf_phase;  // (thread 0 flips it below, after every thread has read it)
+        if (pf) {
+            // this chunk's words, rows and hub pairs, staged during the last chunk
+            staged = true;
+            if (pf->nr + pf->nh + pf->nw > 0) {
+                unsigned spins = 0;
+                while (!mbar_try_wait(&pf->bar, ph)) {
+                    if (++spins > p.spin_limit) {
+                        staged = false;
+                        break;
+                    }
+                }
+            }
+            if (!__syncthreads_and(staged)) {
+                // the copy did not land in time: report it, one more bounded wait for
+                // the copy in flight, and leave the level (every caller reads the error word)
+                if (tid == 0) {
+                    atomicOr(&p.st->error, kErrBulk);
+                    unsigned spins = 0;
+                    while (!mbar_try_wait(&pf->bar, ph) && ++spins <= p.spin_limit) __nanosleep(256);
+                }
+                __syncthreads();
+                return;
+            }
+        }
+        const int pnr = pf ? pf->nr : 0, pnh = pf ? pf->nh : 0, pnw = pf ? pf->nw : 0;
         // ---- own visited words (the snapshot is read coherently: ld.cg) ----------
         unsigned word[PER];
 #pragma unroll
         for (int t = 0; t < PER; t++) {
             const int vb = cs + t * B + (tid & ~31);
-            word[t] = vb < re ? ld_cg(mask + (vb >> 5)) : 0xffffffffu;
+            const int wi = (vb - cs) >> 5;
+            word[t] = vb < re ? (wi < pnw ? pf->words[wi] : ld_cg(mask + (vb >> 5))) : 0xffffffffu;
         }
         int r0[PER], r1[PER];
         bool todo[PER];
+        int2 hubv[PER];
 #pragma unroll
         for (int t = 0; t < PER; t++) {
-            const int v = cs + t * B + tid;
+            const int v = cs + t * B + tid, j = v - cs;
             todo[t] = v < re && !((word[t] >> lane) & 1u);
             r0[t] = r1[t] = 0;
+            hubv[t] = make_int2(-1, -1);
             if (todo[t]) {
-                r0[t] = ld_ro(p.row_offsets + v);
-                r1[t] = ld_ro(p.row_offsets + v + 1);
+                r0[t] = j < pnr ? pf->rows[j] : ld_ro(p.row_offsets + v);
+                r1[t] = j + 1 < pnr ? pf->rows[j + 1] : ld_ro(p.row_offsets + v + 1);
+                if (pf && p.hub2) hubv[t] = j < pnh ? pf->hub[j] : p.hub2[v];
+            }
+        }
+        if (pf) {
+            // the buffer is consumed: stage the next chunk while this one is scanned
+            __syncthreads();
+            if (tid == 0) {
+                if (pnr + pnh + pnw > 0) s.pf_phase = ph ^ 1u;
+                if (cs + kChunkMax < re) bu_prefetch_issue(p, *pf, mask, cs + kChunkMax, re);
             }
         }
         stamp_synced(p, pass, 1, first);
@@ -942,9 +1037,11 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
             for (int t = 0; t < PER; t++) {
                 todo[t] = todo[t] && r1[t] > r0[t];
                 if (p.hub2) {
-                    // the vertex's two highest-degree neighbours (one coalesced 8-byte load)
-                    int2 h = make_int2(-1, -1);
-                    if (todo[t]) h = p.hub2[cs + t * B + tid];
+                    // the vertex's two highest-degree neighbours (one coalesced 8-byte load,
+                    // or staged with the chunk)
+                    int2 h = hubv[t];
+                    if (!pf && todo[t]) h = p.hub2[cs + t * B + tid];
+                    if (!todo[t]) h = make_int2(-1, -1);
                     nb[t][0] = h.x;
                     nb[t][1] = h.y;
                 } else {

@@ -159,6 +159,7 @@ struct BfsParams {
     int32_t bu_scan;          // bottom-up continuation: 1 per lane, 2 per CTA (edge-parallel worklist)
     int32_t bu_long;          // bottom-up: lists longer than this are searched by the whole warp
     int32_t hist_log;         // history cull table of 2^hist_log entries per CTA (0: off)
+    int32_t bu_prefetch;      // 1: the first bottom-up level stages each next chunk with bulk copies
     int32_t bu_defer;         // persistent bottom-up levels count their discoveries; the frontier is built
                               // from the mask buffers only when a top-down level follows
     const uint32_t *iso;      // bit v: v has no edges in or out; a search starts with these bits visited (null: none)

@@ -6,6 +6,16 @@
 namespace b40c {
 namespace rt {
 
+// Dynamic shared memory of the vertex/edge kernels: their state, plus the
+// history cull table and the bottom-up prefetch buffer when the policy turns
+// them on.
+template <typename Smem>
+inline size_t kernel_smem(const b40c_bfs_policy &pol)
+{
+    return ((sizeof(Smem) + 15) & ~size_t(15)) + (pol.history_cull > 0 ? sizeof(uint32_t) << kHistLog : 0) +
+           (pol.bottom_up_prefetch > 0 ? dev::kBuPrefetchBytes : 0);
+}
+
 // Grid of the set-up kernel: the full label/mask initialisation is a
 // grid-stride fill, the source-only set-up a single CTA.
 inline int init_grid(b40c_bfs_problem *p, bool full)

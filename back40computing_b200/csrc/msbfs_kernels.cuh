@@ -75,8 +75,9 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
     cta_range(E, blockIdx.x, gridDim.x, rs, re);
     if (rs >= re) return;
     int i_cur = ld_cg(in.cf + rs / kChunkGrain);
-    for (int cs = rs; cs < re; cs += kChunkMax) {
-        const int ce = min(cs + kChunkMax, re);
+    const int chunk = min(max(p.chunk_edges, 256), kChunkMax);
+    for (int cs = rs; cs < re; cs += chunk) {
+        const int ce = min(cs + chunk, re);
         const int len = ce - cs;
         if (tid == 0) s.out_count = 0;
         int k = 0;

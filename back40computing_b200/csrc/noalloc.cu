@@ -166,6 +166,7 @@ extern "C" int b40c_bfs_search_noalloc(const int32_t *d_row_offsets, const int32
     k.bu_scan = 1;
     k.bu_long = 256;
     k.hist_log = 0;
+    k.bu_prefetch = 0;
     k.mask_alt = nullptr;  // never bottom-up
     k.hub2 = nullptr;
     k.levels = nullptr;

@@ -146,6 +146,8 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.bu_scan = pol.bottom_up_scan;
     k.bu_long = pol.bottom_up_long_list;
     k.hist_log = pol.history_cull > 0 ? kHistLog : 0;
+    // the staged copies need 16-byte aligned device arrays (not a host-mapped CSR)
+    k.bu_prefetch = pol.bottom_up_prefetch > 0 && k.bulk_ok && (reinterpret_cast<uintptr_t>(p->d_ro) & 15) == 0 ? 1 : 0;
     k.bu_defer = pol.bottom_up_defer_frontier > 0 ? 1 : 0;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
@@ -211,6 +213,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->subgrid_frontier_edges) d.subgrid_frontier_edges = in->subgrid_frontier_edges > 0 ? in->subgrid_frontier_edges : -1;
         if (in->bottom_up_long_list) d.bottom_up_long_list = in->bottom_up_long_list;
         if (in->history_cull) d.history_cull = in->history_cull > 0 ? 1 : -1;
+        if (in->bottom_up_prefetch) d.bottom_up_prefetch = in->bottom_up_prefetch > 0 ? 1 : -1;
     }
     if (d.threads != 128 && d.threads != 256 && d.threads != 512)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: 128, 256, 512)",
@@ -230,6 +233,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     if (d.bottom_up_scan != 1)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_scan must be 1 (per-lane list scans)");
     if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
+    if (d.bottom_up_prefetch == 0) d.bottom_up_prefetch = d.threads >= 512 ? 1 : -1;
     if (d.bottom_up_long_list < 4)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_long_list must be >= 4");
     *out = d;

@@ -116,14 +116,6 @@ namespace rt {
 constexpr int kThreads = 256;
 constexpr int kHistLog = 12;  // history cull table: 4096 vertex ids (16 KB) per CTA
 
-// Dynamic shared memory of the vertex/edge kernels: their state, plus the
-// history cull table when the policy turns it on.
-template <typename Smem>
-inline size_t kernel_smem(const b40c_bfs_policy &pol)
-{
-    return ((sizeof(Smem) + 15) & ~size_t(15)) + (pol.history_cull > 0 ? sizeof(uint32_t) << kHistLog : 0);
-}
-
 struct DeviceGuard {
     int prev = -1;
     explicit DeviceGuard(int dev)

@@ -81,7 +81,8 @@ enum {
 typedef struct b40c_bfs_policy {
     int32_t threads;               /* CTA size (256: the size the kernels are built for) */
     int32_t ctas_per_sm;           /* resident CTAs per SM for persistent grids (0 = occupancy limit) */
-    int32_t chunk_edges;           /* edges per CTA work chunk in the edge-balanced expansion (<= 4096) */
+    int32_t chunk_edges;           /* edges (or edge-frontier items) per sub-round of a CTA's share of a level:
+                                      a multiple of 32 in [256, 2048] (default 2048) */
     int32_t warp_gather_threshold; /* run length at or above which a warp gathers cooperatively (>= 32) */
     int32_t cta_gather_threshold;  /* run length at or above which the CTA gathers with bulk staging */
     int32_t saturation_quit;       /* hybrid: queue items per CTA above which the search leaves the fused kernel */
@@ -128,6 +129,10 @@ typedef struct b40c_bfs_policy {
                                       shared-memory table, the neighbours it has already sent to the
                                       visited test and drops repeats without touching the visited mask
                                       (the reference's history culling): 1 = on, -1 = off (default) */
+    int32_t bottom_up_prefetch;    /* the first bottom-up level of a run stages each next chunk's visited words,
+                                      row offsets and hub pairs into shared memory with bulk copies while it
+                                      scans the current one (25 KB of shared memory per CTA): 1 = on, -1 = off;
+                                      default: on for 512-thread CTAs (no occupancy cost), else off */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

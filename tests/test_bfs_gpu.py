@@ -565,3 +565,35 @@ def test_history_cull(strategy, mode, preds):
             else:
                 assert oracle.compare_labels(got, want) == -1, f"{kind} source {s}"
         p.Destroy()
+
+
+@pytest.mark.parametrize("threads", [128, 256, 512])
+@pytest.mark.parametrize("prefetch", [1, -1])
+@pytest.mark.parametrize("preds", [False, True])
+def test_cta_sizes_and_bottom_up_prefetch(threads, prefetch, preds):
+    """Every strategy built for 128-, 256- and 512-thread CTAs, and the first
+    bottom-up level with and without its chunks staged by bulk copies, gives
+    the oracle's distances and valid predecessors (graphs whose vertex count
+    is not a multiple of the chunk, so the ragged last chunk is covered)."""
+    pol = N.Policy()
+    pol.threads = threads
+    pol.bottom_up_prefetch = prefetch
+    pol.bottom_up_alpha = 4
+    for kind, args in (("rmat", (1 << 15, 1 << 19)), ("rr", (20011, 10)), ("grid3d", (23,))):
+        g = _graph(kind, *args)
+        p = CsrProblem.from_graph(g, mark_predecessors=preds)
+        for strategy in (DIRECTION_OPTIMIZING, EXPAND_CONTRACT, CONTRACT_EXPAND):
+            for s in sample_sources(g, 2, seed=19):
+                got = search(p, int(s), strategy=strategy, policy=pol)
+                want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+                if preds:
+                    assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+                else:
+                    assert oracle.compare_labels(got, want) == -1, f"{kind} {strategy} source {s}"
+        if not preds:
+            srcs = sample_sources(g, 20, seed=3)
+            p.msbfs(srcs, policy=pol)
+            for slot in (0, 19):
+                want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
+                assert oracle.compare_labels(p.labels_of(slot), want) == -1
+        p.Destroy()
