@@ -214,9 +214,10 @@ def main(argv=None):
     out.setdefault("classes", {})
     out["device"] = torch.cuda.get_device_name(0)
     out["generated"] = time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime())
-    out["how"] = ("coordinate search over SEARCH_SPACE from the library defaults; cost = mean device time per "
-                  "search (per batch for 'batched') summed over the class's representatives; quick="
-                  f"{args.quick}")
+    out["how"] = ("coordinate search over SEARCH_SPACE "
+                  + (f"of the knobs {args.knobs} from the cached policy" if args.knobs else "from the library defaults")
+                  + "; cost = mean device time per search (per batch for 'batched') summed over the class's "
+                  f"representatives; quick={args.quick}")
     for cls in args.classes.split(","):
         for kind in args.kinds.split(","):
             print(f"[{cls} / {kind}]", flush=True)

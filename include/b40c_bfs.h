@@ -168,8 +168,11 @@ int b40c_bfs_default_policy(int strategy, b40c_bfs_policy *policy);
 /* ---- problem (bfs::CsrProblem, csr_problem.cuh:72-756) ---------------------- */
 
 /* CsrProblem::FromHostProblem (csr_problem.cuh:328-540): copies the CSR to the
- * device (or, with stream_from_host, maps the caller's pinned host arrays
- * zero-copy: they must stay valid until destroy).  device < 0 selects the
+ * device (or, with stream_from_host, maps the caller's host arrays zero-copy,
+ * pinning them in place when they are not page-locked yet: they must stay
+ * valid until destroy; the kernels then read them over the bus with plain
+ * loads).  Both arrays must be 4-byte aligned (B40C_ERROR_INVALID_VALUE
+ * otherwise); no stronger alignment is needed.  device < 0 selects the
  * calling thread's current CUDA device.  num_gpus other than 1 is
  * rejected by the C++ layer (single-GPU library). */
 int b40c_bfs_problem_create(const int32_t *h_row_offsets, const int32_t *h_column_indices,
@@ -332,9 +335,13 @@ int b40c_msbfs_device_labels(b40c_bfs_problem *problem, void **d_labels, int32_t
  * in a fixed scratch array built into the library (about 6.3 MB held on every
  * device that loads it, until the process exits).  Limits: at most 262,144
  * vertices and 4,194,304 edges; larger graphs are rejected with
- * B40C_ERROR_INVALID_VALUE (use b40c_bfs_problem_create).  The first call on
- * a device sets that device up (looks up the scratch's device address and
- * the kernel's launch shape), so make it before any stream capture.  Every
+ * B40C_ERROR_INVALID_VALUE (use b40c_bfs_problem_create).  The three arrays
+ * must be 4-byte aligned (else B40C_ERROR_INVALID_VALUE); the column array
+ * need not be 16-byte aligned (bulk copies of it are aligned by address).
+ * The first call on a device sets that device up (looks up the scratch's
+ * device address and the kernel's launch shape), so make it before any
+ * stream capture, and do not call it after a cudaDeviceReset in the same
+ * process (the set-up belongs to the context that was reset).  Every
  * call shares the one scratch array: calls whose work overlaps on the GPU
  * (different streams or threads at once) race and must be serialised by the
  * caller.  Runs on cuda_stream (NULL: the legacy default stream) on the
