@@ -51,6 +51,7 @@ class Policy(C.Structure):
         ("bottom_up_long_list", C.c_int32),
         ("history_cull", C.c_int32),
         ("bottom_up_prefetch", C.c_int32),
+        ("warp_contract", C.c_int32),
     ]
 
 

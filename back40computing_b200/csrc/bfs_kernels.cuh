@@ -702,6 +702,172 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
     }
 }
 
+// One warp's output (bv = vertex, bc = row start, bd = degree, `count`
+// entries in the warp's own slice of the shared tables) appended to the
+// vertex frontier: a warp scan of (count, degree) pairs, one packed 64-bit
+// atomicAdd on the pass counter for the slots and the degree prefix, then the
+// entries, their degree prefixes P and their kChunkGrain boundaries in cf
+// (runs over more than kCfSerialChunks chunks written by the whole warp).
+// bc is overwritten with each entry's flush-relative degree prefix.  All 32
+// lanes call it with the same count.
+__device__ __forceinline__ void warp_emit(const BfsParams &p, const int32_t *bv, int32_t *bc, const int32_t *bd,
+                                          int count, const VertexFrontier &vout, unsigned long long *qe_out)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    const int per = (count + 31) >> 5;
+    const int jb = min(lane * per, count), je = min(jb + per, count);
+    unsigned my_deg = 0;
+    for (int j = jb; j < je; j++) my_deg += (unsigned)bd[j];
+    const unsigned long long x = pack((unsigned)(je - jb), my_deg);
+    unsigned long long incl = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    const unsigned long long tot = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long prefix = 0;
+    if (lane == 0) prefix = atomicAdd(qe_out, tot);
+    prefix = __shfl_sync(0xffffffffu, prefix, 0);
+    const unsigned long long excl = incl - x;
+    const unsigned g0 = (unsigned)(prefix >> 32), d0 = (unsigned)(prefix & 0xffffffffu);
+    unsigned g = g0 + (unsigned)(excl >> 32);
+    unsigned d = d0 + (unsigned)(excl & 0xffffffffu);
+    bool long_run = false;
+    for (int j = jb; j < je; j++) {
+        const unsigned deg = (unsigned)bd[j];
+        if ((int)g < p.vcap) {
+            vout.v[g] = bv[j];
+            vout.col[g] = bc[j];
+            vout.P[g] = (int)d;
+            const unsigned c0 = (d + kChunkGrain - 1) / kChunkGrain, c1 = (d + deg + kChunkGrain - 1) / kChunkGrain;
+            if (c1 - c0 > kCfSerialChunks) {
+                long_run = true;
+            } else {
+                for (unsigned c = c0; c < c1; c++) {
+                    if (c >= (unsigned)p.cf_cap) {  // a level's edges exceed the graph's: never past the end
+                        atomicOr(&p.st->error, kErrOverflow);
+                        break;
+                    }
+                    vout.cf[c] = (int)g;
+                }
+            }
+        } else {
+            atomicOr(&p.st->error, kErrOverflow);
+        }
+        bc[j] = (int)(d - d0);
+        g++;
+        d += deg;
+    }
+    unsigned lanes = __ballot_sync(0xffffffffu, long_run);
+    if (!lanes) return;
+    __syncwarp();  // bc holds the flush-relative prefixes
+    // entries spanning many chunks (high-degree vertices): the whole warp
+    // writes each one's run of cf, 32 chunks per step
+    while (lanes) {
+        const int L = __ffs(lanes) - 1;
+        lanes &= lanes - 1;
+        const int lb = min(L * per, count), le = min(lb + per, count);
+        for (int j = lb; j < le; j++) {
+            const unsigned ed = d0 + (unsigned)bc[j], deg = (unsigned)bd[j];
+            const unsigned c0 = (ed + kChunkGrain - 1) / kChunkGrain, c1 = (ed + deg + kChunkGrain - 1) / kChunkGrain;
+            if (c1 - c0 <= kCfSerialChunks || (int)(g0 + j) >= p.vcap) continue;
+            if (lane == 0 && c1 > (unsigned)p.cf_cap) atomicOr(&p.st->error, kErrOverflow);
+            const unsigned c_end = min(c1, (unsigned)p.cf_cap);
+            for (unsigned c = c0 + lane; c < c_end; c += 32) vout.cf[c] = (int)(g0 + j);
+        }
+    }
+}
+
+// Warp-autonomous contraction of the CTA's share of an edge frontier
+// (policy.warp_contract): warp w of the CTA takes slices w, w + NW, ... of
+// 32 * PER items and runs the visited test on each (pre-check loads, atomic
+// test-and-set, the CSR rows of the winners) with no CTA barrier; winners
+// with edges collect in the warp's slice of the shared tables and go to the
+// vertex frontier in flushes of their own (warp_emit).  A warp therefore never
+// waits for the slowest load of another warp, and the frontier slots cost one
+// atomic per flush (a flush when the next slice could overrun the warp's
+// 32 * PER entries, and one at the end).  Same labels and frontier contents as
+// contract_range (the reference's contraction, contract_expand_atomic/
+// cta.cuh:213-304); the entries' order differs.
+template <int B, bool PRED>
+__device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSmem<B, PRED> &s,
+                                                    const EdgeFrontier &in, int level, const VertexFrontier &vout,
+                                                    unsigned long long *qe_out)
+{
+    constexpr int PER = kChunkMax / B;
+    constexpr int NW = B / 32;
+    constexpr int S = 32 * PER;  // items per slice == entries of a warp's output
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *bv = s.out + warp * S;
+    int32_t *bc = s.colstart + warp * S;
+    int32_t *bd = s.rel + warp * S;
+    int rs, re;
+    cta_range(s.q, blockIdx.x, gridDim.x, rs, re);
+    const int pre = p.precheck;
+    int count = 0;  // warp-uniform
+    bool any = false;
+    for (int base = rs + warp * S; base < re; base += NW * S) {
+        int v[PER], u[PER];
+        bool go[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int i = base + t * 32 + lane;
+            go[t] = i < re;
+            v[t] = go[t] ? ld_cg(in.v + i) : -1;
+            u[t] = (PRED && go[t]) ? ld_cg(in.pred + i) : -1;
+        }
+        unsigned word[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            word[t] = 0;
+            if (go[t] && pre) word[t] = pre == 2 ? ld_cg(s.mask + (v[t] >> 5)) : ld_mask(s.mask + (v[t] >> 5));
+        }
+        bool found[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const unsigned bit = 1u << (v[t] & 31);
+            found[t] = go[t] && !(word[t] & bit) && !(atomicOr(s.mask + (v[t] >> 5), bit) & bit);
+        }
+        int r0[PER], deg[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            r0[t] = deg[t] = 0;
+            if (found[t]) {
+                p.labels[v[t]] = PRED ? u[t] : level;
+                r0[t] = ld_ro(p.row_offsets + v[t]);
+                deg[t] = ld_ro(p.row_offsets + v[t] + 1);
+                any = true;
+            }
+        }
+        int n_new = 0;
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            deg[t] -= r0[t];  // 0 for the lanes that found nothing
+            n_new += __popc(__ballot_sync(0xffffffffu, deg[t] > 0));
+        }
+        if (count + n_new > S) {
+            warp_emit(p, bv, bc, bd, count, vout, qe_out);
+            __syncwarp();  // the flush has read the slice before it is refilled
+            count = 0;
+        }
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const unsigned bal = __ballot_sync(0xffffffffu, deg[t] > 0);
+            if (deg[t] > 0) {
+                const int slot = count + __popc(bal & lanemask_lt());
+                bv[slot] = v[t];
+                bc[slot] = r0[t];
+                bd[slot] = deg[t];
+            }
+            count += __popc(bal);
+        }
+    }
+    if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
+    if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
+}
+
 // ------------------------------------------------------------------------------------
 // Bottom-up step (direction-optimizing levels, undirected graphs only)
 // ------------------------------------------------------------------------------------
@@ -1905,7 +2071,10 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
                 break;
             }
             if (tid == 0 && blockIdx.x == 0 && pass > 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
-            contract_range<B, PRED>(p, s, p.ef[in_idx], level, pass, &p.st->qe[(pass + 1) % 3]);
+            if (p.warp_contract)
+                contract_range_warp<B, PRED>(p, s, p.ef[in_idx], level, p.vf[0], &p.st->qe[(pass + 1) % 3]);
+            else
+                contract_range<B, PRED>(p, s, p.ef[in_idx], level, pass, &p.st->qe[(pass + 1) % 3]);
             __syncthreads();
             if (s.flag) max_level_seen = max(max_level_seen, level);
             if (p.persistent) {

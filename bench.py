@@ -271,6 +271,8 @@ ABLATIONS = [
     (0, "warp_cull", [-1, 1]),
     (0, "history_cull", [-1, 1]),
     (0, "ctas_per_sm", [4, 3, 2]),
+    (1, "warp_contract", [1, -1]),
+    (3, "warp_contract", [1, -1]),
 ]
 
 
@@ -285,7 +287,7 @@ def ablate(cfg_name, sources=16, rounds=3):
     p = CsrProblem.from_graph(g)
     rows = []
     for strategy, knob, values in ABLATIONS:
-        kind = {0: "expand-contract", 4: "direction-optimizing"}[strategy]
+        kind = "direction-optimizing" if strategy == 4 else "expand-contract"
         tuned = autotune.policy_for(g, kind)
         enactors = []
         for v in values:

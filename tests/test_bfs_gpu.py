@@ -597,3 +597,36 @@ def test_cta_sizes_and_bottom_up_prefetch(threads, prefetch, preds):
                 want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(srcs[slot]))
                 assert oracle.compare_labels(p.labels_of(slot), want) == -1
         p.Destroy()
+
+
+@pytest.mark.parametrize("warp_contract", [1, -1])
+@pytest.mark.parametrize("strategy", [CONTRACT_EXPAND, TWO_PHASE, HYBRID])
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("preds", [False, True])
+def test_contract_by_warps_and_by_ctas(warp_contract, strategy, mode, preds):
+    """The contraction of the edge-frontier strategies, warp by warp (each warp
+    flushing its own winners to the vertex frontier; the default) or in
+    CTA-wide sub-rounds: the oracle's distances, valid predecessors, and the
+    reference's total_queued (the edges of the reached vertices).  The R-MAT
+    graph has hubs whose lists span many 256-edge chunks (their chunk-index
+    runs are written by the whole warp); the directed graph has vertices
+    without out-edges (labelled, never enqueued)."""
+    pol = N.Policy()
+    pol.warp_contract = warp_contract
+    for kind, args, kw in (("rmat", (1 << 16, 1 << 20), {}), ("rr", (30011, 5), {"sym": False}),
+                           ("grid2d", (150,), {})):
+        g = _graph(kind, *args, **kw)
+        assert kind != "rmat" or np.diff(g.row_offsets).max() > 8 * 256
+        p = CsrProblem.from_graph(g, mark_predecessors=preds)
+        e = ENACTORS[strategy](policy=pol)
+        e._problem = p
+        for s in sample_sources(g, 2, seed=23):
+            got = search(p, int(s), strategy=strategy, mode=mode, policy=pol)
+            want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            if preds:
+                assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+            else:
+                assert oracle.compare_labels(got, want) == -1, f"{kind} source {s}"
+                nv, ev = oracle.visited_stats(g.row_offsets, got)
+                assert e.GetStatistics()[0] == ev, f"{kind} source {s}: total_queued"
+        p.Destroy()
