@@ -55,7 +55,7 @@ struct ExpandSmem {
     int32_t colstart[kChunkMax + 2];
     int32_t rel[kChunkMax + 2];
     int32_t vert[PRED ? kChunkMax + 2 : 1];
-    uint16_t own[kChunkMax];  // position -> run j owning it
+    alignas(16) uint16_t own[kChunkMax];  // position -> run j owning it
     int32_t out[kChunkMax];   // discovered vertices of the sub-round
     alignas(16) int32_t stage[kChunkMax + 16];  // bulk-staged run (sub-round inside one list)
     uint64_t bar;             // mbarrier of the bulk copy
@@ -780,17 +780,95 @@ __device__ __forceinline__ void warp_emit(const BfsParams &p, const int32_t *bv,
     }
 }
 
+// Warp-autonomous passes are taken by levels with at least a full sub-round
+// of work per CTA: in smaller ones (the first levels from a hub, which
+// discover most of what they touch) a warp would flush its output after
+// nearly every slice, and the CTA-wide sub-rounds measured 3x faster there.
+__device__ __forceinline__ bool warp_sized(int items) { return items >= (int)gridDim.x * kChunkMax; }
+
+// Warp-autonomous passes deal their slices over every warp of the grid,
+// warp-major (slice k goes to warp k / gridDim of CTA k % gridDim, then
+// every gridDim * NW slices on), so a small level spreads over all SMs and a
+// large one is balanced to a slice.  First slice of warp `warp` of this CTA.
+__device__ __forceinline__ int warp_slice0(int warp) { return warp * (int)gridDim.x + (int)blockIdx.x; }
+
+// Visited test of one warp's batch of PER neighbours per lane (pre-check
+// loads, atomic test-and-set, the CSR rows of the winners; each winner is
+// labelled), then the winners with edges appended to the warp's output
+// (bv / bc / bd, `count` entries of at most `cap`, flushed to the vertex
+// frontier first when the batch could overrun it).  With LEAVES the winners
+// without edges are added to total_queued (vertex-frontier strategies queue
+// every discovered vertex, expand_contract_atomic/cta.cuh:432-466).  Returns
+// whether this lane labelled a vertex.  All 32 lanes call it.
+template <int PER, bool PRED, bool LEAVES>
+__device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask, const int (&v)[PER],
+                                             const int (&u)[PER], const bool (&go)[PER], int label_value,
+                                             int32_t *bv, int32_t *bc, int32_t *bd, int &count, int cap,
+                                             const VertexFrontier &vout, unsigned long long *qe_out)
+{
+    const int lane = threadIdx.x & 31;
+    const int pre = p.precheck;
+    unsigned word[PER];
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        word[t] = 0;
+        if (go[t] && pre) word[t] = pre == 2 ? ld_cg(mask + (v[t] >> 5)) : ld_mask(mask + (v[t] >> 5));
+    }
+    bool found[PER];
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const unsigned bit = 1u << (v[t] & 31);
+        found[t] = go[t] && !(word[t] & bit) && !(atomicOr(mask + (v[t] >> 5), bit) & bit);
+    }
+    bool any = false;
+    int r0[PER], deg[PER];
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        r0[t] = deg[t] = 0;
+        if (found[t]) {
+            p.labels[v[t]] = PRED ? u[t] : label_value;
+            r0[t] = ld_ro(p.row_offsets + v[t]);
+            deg[t] = ld_ro(p.row_offsets + v[t] + 1);
+            any = true;
+        }
+    }
+    int n_new = 0;
+    unsigned leaves = 0;
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        deg[t] -= r0[t];  // 0 for the lanes that found nothing
+        n_new += __popc(__ballot_sync(0xffffffffu, deg[t] > 0));
+        if (LEAVES) leaves += __popc(__ballot_sync(0xffffffffu, found[t] && deg[t] == 0));
+    }
+    if (LEAVES && leaves && lane == 0) atomicAdd(&p.st->total_queued, (unsigned long long)leaves);
+    if (count + n_new > cap) {
+        warp_emit(p, bv, bc, bd, count, vout, qe_out);
+        __syncwarp();  // the flush has read the output before it is refilled
+        count = 0;
+    }
+#pragma unroll
+    for (int t = 0; t < PER; t++) {
+        const unsigned bal = __ballot_sync(0xffffffffu, deg[t] > 0);
+        if (deg[t] > 0) {
+            const int slot = count + __popc(bal & lanemask_lt());
+            bv[slot] = v[t];
+            bc[slot] = r0[t];
+            bd[slot] = deg[t];
+        }
+        count += __popc(bal);
+    }
+    return any;
+}
+
 // Warp-autonomous contraction of the CTA's share of an edge frontier
-// (policy.warp_contract): warp w of the CTA takes slices w, w + NW, ... of
-// 32 * PER items and runs the visited test on each (pre-check loads, atomic
-// test-and-set, the CSR rows of the winners) with no CTA barrier; winners
-// with edges collect in the warp's slice of the shared tables and go to the
-// vertex frontier in flushes of their own (warp_emit).  A warp therefore never
+// (policy.warp_contract): each warp takes its slices of 32 * PER items
+// (warp_slice0) and runs the visited test on each with no CTA barrier;
+// winners with edges collect in the warp's slice of the shared tables and go
+// to the vertex frontier in flushes of their own (warp_emit).  A warp never
 // waits for the slowest load of another warp, and the frontier slots cost one
-// atomic per flush (a flush when the next slice could overrun the warp's
-// 32 * PER entries, and one at the end).  Same labels and frontier contents as
-// contract_range (the reference's contraction, contract_expand_atomic/
-// cta.cuh:213-304); the entries' order differs.
+// atomic per flush.  Same labels and frontier contents as contract_range (the
+// reference's contraction, contract_expand_atomic/cta.cuh:213-304); the
+// entries' order differs.
 template <int B, bool PRED>
 __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSmem<B, PRED> &s,
                                                     const EdgeFrontier &in, int level, const VertexFrontier &vout,
@@ -803,12 +881,12 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
     int32_t *bv = s.out + warp * S;
     int32_t *bc = s.colstart + warp * S;
     int32_t *bd = s.rel + warp * S;
-    int rs, re;
-    cta_range(s.q, blockIdx.x, gridDim.x, rs, re);
-    const int pre = p.precheck;
+    const int re = s.q;
     int count = 0;  // warp-uniform
     bool any = false;
-    for (int base = rs + warp * S; base < re; base += NW * S) {
+    const long long stride = (long long)gridDim.x * NW * S;
+    for (long long b64 = (long long)warp_slice0(warp) * S; b64 < re; b64 += stride) {
+        const int base = (int)b64;
         int v[PER], u[PER];
         bool go[PER];
 #pragma unroll
@@ -818,54 +896,140 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
             v[t] = go[t] ? ld_cg(in.v + i) : -1;
             u[t] = (PRED && go[t]) ? ld_cg(in.pred + i) : -1;
         }
-        unsigned word[PER];
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            word[t] = 0;
-            if (go[t] && pre) word[t] = pre == 2 ? ld_cg(s.mask + (v[t] >> 5)) : ld_mask(s.mask + (v[t] >> 5));
-        }
-        bool found[PER];
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            const unsigned bit = 1u << (v[t] & 31);
-            found[t] = go[t] && !(word[t] & bit) && !(atomicOr(s.mask + (v[t] >> 5), bit) & bit);
-        }
-        int r0[PER], deg[PER];
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            r0[t] = deg[t] = 0;
-            if (found[t]) {
-                p.labels[v[t]] = PRED ? u[t] : level;
-                r0[t] = ld_ro(p.row_offsets + v[t]);
-                deg[t] = ld_ro(p.row_offsets + v[t] + 1);
-                any = true;
-            }
-        }
-        int n_new = 0;
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            deg[t] -= r0[t];  // 0 for the lanes that found nothing
-            n_new += __popc(__ballot_sync(0xffffffffu, deg[t] > 0));
-        }
-        if (count + n_new > S) {
-            warp_emit(p, bv, bc, bd, count, vout, qe_out);
-            __syncwarp();  // the flush has read the slice before it is refilled
-            count = 0;
-        }
-#pragma unroll
-        for (int t = 0; t < PER; t++) {
-            const unsigned bal = __ballot_sync(0xffffffffu, deg[t] > 0);
-            if (deg[t] > 0) {
-                const int slot = count + __popc(bal & lanemask_lt());
-                bv[slot] = v[t];
-                bc[slot] = r0[t];
-                bd[slot] = deg[t];
-            }
-            count += __popc(bal);
-        }
+        any |= warp_discover<PER, PRED, false>(p, s.mask, v, u, go, level, bv, bc, bd, count, S, vout, qe_out);
     }
     if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
     if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
+}
+
+// Warp-autonomous expand-contract level (policy.warp_contract, top-down-only
+// kernels with CTAs of at most 256 threads): each warp takes its
+// kChunkGrain-position slices (warp_slice0) of the frontier's flattened edge
+// space.  A slice starts at a chunk boundary, so
+// the chunk index gives the entry owning its first position; the warp loads
+// the entries overlapping the slice (32 per round trip), marks where each one
+// starts in its own position -> entry map and fills the map by a warp
+// max-scan; then every lane gathers kWarpSlice / 32 positions (a warp reads
+// 32 consecutive positions of a run, one coalesced segment) and runs the
+// visited test (warp_discover) with no CTA barrier.  Same labels and
+// frontier contents as expand_range (the reference's expand-contract,
+// expand_contract_atomic/cta.cuh:82-789); the entries' order differs.
+constexpr int kWarpSlice = kChunkGrain;  // positions per warp slice
+// With CULL = false (the expand pass of the edge-frontier strategies) the
+// gathered neighbours (and their predecessors) are written to the edge
+// frontier `eout` at their flattened positions instead: the reference's
+// two-phase expansion (two_phase/expand_atomic/cta.cuh:215-423).
+template <int B, bool PRED, bool CULL = true>
+__device__ __forceinline__ void expand_range_warp(const BfsParams &p, const VertexFrontier &in,
+                                                  ExpandSmem<B, PRED> &s, int level, const VertexFrontier &vout,
+                                                  unsigned long long *qe_out, const EdgeFrontier *eout = nullptr)
+{
+    static_assert(B <= 256, "a warp's output holds a whole slice's discoveries only up to 256-thread CTAs");
+    constexpr int NW = B / 32;
+    constexpr int PW = kWarpSlice / 32;    // positions per lane per slice
+    constexpr int CAP = kChunkMax / NW;    // a warp's output entries (>= kWarpSlice)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *bv = s.out + warp * CAP;
+    int32_t *bc = s.colstart + warp * CAP;
+    int32_t *bd = s.rel + warp * CAP;
+    uint16_t *own = s.own + warp * kWarpSlice;   // slice position -> table entry
+    int32_t *tcol = s.stage + warp * kWarpSlice;  // table entry -> column index of slice position 0
+    int32_t *tver = PRED ? s.vert + warp * kWarpSlice : nullptr;
+    const int q = s.q, re = s.E;
+    int count = 0;  // warp-uniform
+    bool any = false;
+    const long long stride = (long long)gridDim.x * NW * kWarpSlice;
+    for (long long x64 = (long long)warp_slice0(warp) * kWarpSlice; x64 < re; x64 += stride) {
+        const int x0 = (int)x64;
+        const int len = min(kWarpSlice, re - x0);
+        // ---- the entries overlapping [x0, x0 + len), 32 per round trip; each
+        // marks its first slice position in the map (cleared first) -------------
+        reinterpret_cast<uint4 *>(own)[lane] = make_uint4(0u, 0u, 0u, 0u);
+        __syncwarp();
+        const int i0 = ld_cg(in.cf + x0 / kChunkGrain);  // owns position x0 (a chunk start)
+        int n = 0;
+        for (int i = i0;; i += 32) {
+            const int j = i + lane;
+            int Pj = INT_MAX;
+            int cj = 0, vj = -1;
+            if (j < q) {
+                Pj = ld_cg(in.P + j);
+                cj = ld_cg(in.col + j);
+                if (PRED) vj = ld_cg(in.v + j);
+            }
+            const bool inside = Pj < x0 + len;  // the inside lanes form a prefix (P increases)
+            const unsigned in_mask = __ballot_sync(0xffffffffu, inside);
+            const int k = n + lane;
+            if (inside && k < kWarpSlice) {
+                const int start = max(Pj, x0) - x0;
+                own[start] = (uint16_t)k;
+                tcol[k] = cj + (max(Pj, x0) - Pj) - start;  // + slice position = column index
+                if (PRED) tver[k] = vj;
+            }
+            n += __popc(in_mask);
+            if (in_mask != 0xffffffffu || i + 32 >= q) break;
+        }
+        __syncwarp();
+        // ---- position r belongs to the largest mark at or before r (entries start
+        // in increasing order): lane L scans positions 8L .. 8L + 7, then the lanes'
+        // maxima are combined by a warp max-scan ------------------------------------
+        {
+            static_assert(PW == 8, "a lane's share of the map is one 16-byte word");
+            uint4 w = reinterpret_cast<uint4 *>(own)[lane];
+            unsigned e[8] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16,
+                             w.z & 0xffffu, w.z >> 16, w.w & 0xffffu, w.w >> 16};
+#pragma unroll
+            for (int t = 1; t < 8; t++) e[t] = max(e[t], e[t - 1]);
+            unsigned incl = e[7];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl = max(incl, y);
+            }
+            unsigned before = __shfl_up_sync(0xffffffffu, incl, 1);
+            if (lane == 0) before = 0;
+#pragma unroll
+            for (int t = 0; t < 8; t++) e[t] = max(e[t], before);
+            w.x = e[0] | (e[1] << 16);
+            w.y = e[2] | (e[3] << 16);
+            w.z = e[4] | (e[5] << 16);
+            w.w = e[6] | (e[7] << 16);
+            reinterpret_cast<uint4 *>(own)[lane] = w;
+        }
+        __syncwarp();
+        // ---- gather and test ------------------------------------------------------
+        int v[PW], u[PW];
+        bool go[PW];
+#pragma unroll
+        for (int t = 0; t < PW; t++) {
+            const int r = t * 32 + lane;
+            go[t] = r < len;
+            v[t] = -1;
+            u[t] = -1;
+            if (go[t]) {
+                const int k = own[r];
+                v[t] = ld_stream(p.column_indices + tcol[k] + r);
+                if (PRED) u[t] = tver[k];
+            }
+        }
+        if constexpr (CULL) {
+            any |= warp_discover<PW, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP, vout,
+                                                 qe_out);
+        } else {
+#pragma unroll
+            for (int t = 0; t < PW; t++) {
+                if (go[t]) {
+                    eout->v[x0 + t * 32 + lane] = v[t];
+                    if (PRED) eout->pred[x0 + t * 32 + lane] = u[t];
+                }
+            }
+        }
+        __syncwarp();  // the slice's tables are free for the next slice
+    }
+    if constexpr (CULL) {
+        if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
+        if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
+    }
 }
 
 // ------------------------------------------------------------------------------------
@@ -1793,6 +1957,12 @@ constexpr unsigned long long kDeferMinShare = 512;
 template <int B, bool PRED, bool LISTS, bool SUBGRID = false, bool BU = true>
 __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
 {
+    // top-down levels with at least a full sub-round per CTA run warp by warp
+    // (expand_range_warp) in the top-down-only variants with CTAs of at most
+    // 256 threads, when the policy asks for it
+    const auto warp_levels = [](const BfsParams &q, int E) {
+        return !BU && !LISTS && B <= 256 && q.warp_contract != 0 && warp_sized(E);
+    };
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem<B, PRED> &s = *reinterpret_cast<ExpandSmem<B, PRED> *>(smem_raw);
     __shared__ int s_ok;
@@ -1996,6 +2166,12 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
         else if (bu)
             // later bottom-up levels: the unvisited vertices of each window, compacted
             bottom_up_windows<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], defer);
+        else if (warp_levels(p, s.E))
+        {
+            if constexpr (!BU && !LISTS && B <= 256)
+                expand_range_warp<B, PRED>(p, p.vf[level & 1], s, level, p.vf[(level + 1) & 1],
+                                           &p.st->qe[(pass + 1) % 3]);
+        }
         else
         {
             // direction-optimizing: once this level's output passes E* edges, where
@@ -2071,7 +2247,7 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
                 break;
             }
             if (tid == 0 && blockIdx.x == 0 && pass > 0) atomicAdd(&p.st->total_queued, (unsigned long long)s.q);
-            if (p.warp_contract)
+            if (p.warp_contract && warp_sized(s.q))
                 contract_range_warp<B, PRED>(p, s, p.ef[in_idx], level, p.vf[0], &p.st->qe[(pass + 1) % 3]);
             else
                 contract_range<B, PRED>(p, s, p.ef[in_idx], level, pass, &p.st->qe[(pass + 1) % 3]);
@@ -2097,9 +2273,15 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
                 break;
             }
             if (tid == 0 && blockIdx.x == 0) p.st->qe[(pass + 1) % 3] = pack((unsigned)(q == 0 ? 0 : E), 0u);
-            if (q > 0)
-                expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr, bar_phase,
-                                             blockIdx.x, gridDim.x);
+            if (q > 0) {
+                if (B <= 256 && p.warp_contract && warp_sized(E)) {
+                    if constexpr (B <= 256)
+                        expand_range_warp<B, PRED, false>(p, p.vf[0], s, level, p.vf[1], nullptr, &p.ef[out_idx]);
+                } else {
+                    expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr,
+                                                 bar_phase, blockIdx.x, gridDim.x);
+                }
+            }
             __syncthreads();
             completed_level = true;
             if (p.persistent) {

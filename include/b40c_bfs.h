@@ -134,11 +134,12 @@ typedef struct b40c_bfs_policy {
                                       scans the current one (25 KB of shared memory per CTA): 1 = on, -1 = off;
                                       default: on for 512-thread CTAs (no occupancy cost), else off */
     int32_t warp_contract;         /* contract passes of the edge-frontier strategies (contract-expand,
-                                      two-phase, hybrid): 1 = each warp works through its own slices of
-                                      the CTA's share of the edge frontier, with no CTA barriers, and sends
-                                      its winners to the vertex frontier in flushes of its own (one packed
-                                      atomic each; default), -1 = CTA-wide sub-rounds (queue_allocation
-                                      applies) */
+                                      two-phase, hybrid), and with CTAs of up to 256 threads their expand
+                                      passes and the top-down levels of expand-contract searches: 1 = each
+                                      warp works through its own slices of the level, dealt over every
+                                      warp of the grid, with no CTA barriers, and sends its winners to the
+                                      vertex frontier in flushes of its own (one packed atomic each;
+                                      default), -1 = CTA-wide sub-rounds (queue_allocation applies) */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

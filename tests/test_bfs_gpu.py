@@ -600,17 +600,22 @@ def test_cta_sizes_and_bottom_up_prefetch(threads, prefetch, preds):
 
 
 @pytest.mark.parametrize("warp_contract", [1, -1])
-@pytest.mark.parametrize("strategy", [CONTRACT_EXPAND, TWO_PHASE, HYBRID])
+@pytest.mark.parametrize("strategy", [EXPAND_CONTRACT, CONTRACT_EXPAND, TWO_PHASE, HYBRID])
 @pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("preds", [False, True])
-def test_contract_by_warps_and_by_ctas(warp_contract, strategy, mode, preds):
-    """The contraction of the edge-frontier strategies, warp by warp (each warp
-    flushing its own winners to the vertex frontier; the default) or in
-    CTA-wide sub-rounds: the oracle's distances, valid predecessors, and the
-    reference's total_queued (the edges of the reached vertices).  The R-MAT
-    graph has hubs whose lists span many 256-edge chunks (their chunk-index
-    runs are written by the whole warp); the directed graph has vertices
-    without out-edges (labelled, never enqueued)."""
+@pytest.mark.parametrize("grid", [0, 16])
+def test_levels_by_warps_and_by_ctas(warp_contract, strategy, mode, preds, grid):
+    """Top-down levels of expand-contract and the contract and expand passes
+    of the edge-frontier strategies, warp by warp (each warp flushing its own
+    winners to the vertex frontier; the default for levels with a full
+    sub-round per CTA) or in CTA-wide sub-rounds: the oracle's distances,
+    valid predecessors, and the reference's total_queued (expand-contract:
+    the reached vertices but the source; the others: the edges of the reached
+    vertices).  A 16-CTA grid puts the larger levels of these graphs on the
+    warp path.  The R-MAT graph has hubs whose lists span many 256-edge
+    chunks (their chunk-index runs are written by the whole warp); the
+    directed graph has vertices without out-edges (labelled, never
+    enqueued)."""
     pol = N.Policy()
     pol.warp_contract = warp_contract
     for kind, args, kw in (("rmat", (1 << 16, 1 << 20), {}), ("rr", (30011, 5), {"sym": False}),
@@ -621,12 +626,13 @@ def test_contract_by_warps_and_by_ctas(warp_contract, strategy, mode, preds):
         e = ENACTORS[strategy](policy=pol)
         e._problem = p
         for s in sample_sources(g, 2, seed=23):
-            got = search(p, int(s), strategy=strategy, mode=mode, policy=pol)
+            got = search(p, int(s), strategy=strategy, mode=mode, policy=pol, max_grid_size=grid)
             want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
             if preds:
                 assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
             else:
                 assert oracle.compare_labels(got, want) == -1, f"{kind} source {s}"
                 nv, ev = oracle.visited_stats(g.row_offsets, got)
-                assert e.GetStatistics()[0] == ev, f"{kind} source {s}: total_queued"
+                queued = nv - 1 if strategy == EXPAND_CONTRACT else ev
+                assert e.GetStatistics()[0] == queued, f"{kind} source {s}: total_queued"
         p.Destroy()
