@@ -52,6 +52,7 @@ class Policy(C.Structure):
         ("history_cull", C.c_int32),
         ("bottom_up_prefetch", C.c_int32),
         ("warp_contract", C.c_int32),
+        ("warp_bottom_up", C.c_int32),
     ]
 
 

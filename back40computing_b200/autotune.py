@@ -51,15 +51,17 @@ SEARCH_SPACE = {
     "subgrid_frontier_edges": [-1, 4096, 16384, 65536],
     "history_cull": [-1, 1],
     "bottom_up_prefetch": [1, -1],
+    "warp_contract": [1, -1],
+    "warp_bottom_up": [1, -1],
 }
 # knobs that matter to each kind of search
 KNOBS = {
     "direction-optimizing": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
                              "bottom_up_alpha", "bottom_up_beta", "warp_gather_threshold", "bitmask_precheck",
-                             "history_cull", "bottom_up_prefetch"],
+                             "history_cull", "bottom_up_prefetch", "warp_bottom_up"],
     "expand-contract": ["threads", "ctas_per_sm", "chunk_edges", "small_frontier_edges", "subgrid_frontier_edges",
                         "warp_gather_threshold", "cta_gather_threshold", "bitmask_precheck", "warp_cull",
-                        "history_cull"],
+                        "history_cull", "warp_contract"],
     "batched": ["threads", "ctas_per_sm", "bottom_up_alpha"],
 }
 

@@ -1457,6 +1457,107 @@ __device__ __forceinline__ void bottom_up_range(const BfsParams &p, ExpandSmem<B
     }
 }
 
+// The first bottom-up level of a run, when it only counts its discoveries
+// (fused searches, not list mode), warp by warp (policy.warp_bottom_up): each
+// warp takes blocks of 32 * PER vertex ids dealt over every warp of the grid
+// (warp_slice0) and handles them with no CTA barrier -- the blocks' visited
+// words, rows and hub pairs in one round trip (rows and pairs of visited
+// vertices too: at a first bottom-up level nearly every vertex is
+// unvisited), the hub probes, the per-warp queue of lists still to scan
+// (bottom_up_queue), then the block's words of the other mask buffer, the
+// labels and the count of discoveries and their edges.  The CTA adds its
+// count to the pass counter once, at the end.  Same labels and visited words
+// as bottom_up_range.  (Later bottom-up levels, where most vertices are
+// visited, keep the compacted windows: warp by warp they measured slower.)
+template <int B, bool PRED>
+__device__ __forceinline__ void bottom_up_range_warp(const BfsParams &p, ExpandSmem<B, PRED> &s, int level,
+                                                     unsigned long long *qe_out)
+{
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    constexpr int PER = kChunkMax / B;
+    constexpr int NW = B / 32;
+    constexpr int K = kBottomUpProbe;
+    static_assert(K == 2, "the hub pair supplies two probes");
+    constexpr int S = 32 * PER;  // vertices per warp block
+    const uint32_t *mask = s.mask;
+    uint32_t *mask_out = (s.mask == p.mask) ? p.mask_alt : p.mask;
+    const int n = p.nodes;
+    unsigned long long found_acc = 0;  // (count << 32 | degree) of this lane's discoveries
+    bool any = false;
+    const long long stride = (long long)gridDim.x * NW * S;
+    for (long long c64 = (long long)warp_slice0(warp) * S; c64 < n; c64 += stride) {
+        const int cs = (int)c64;
+        unsigned word[PER];
+        int r0[PER], r1[PER];
+        int2 hubv[PER];
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * 32, v = vb + lane;
+            word[t] = vb < n ? ld_cg(mask + (vb >> 5)) : 0xffffffffu;
+            r0[t] = r1[t] = 0;
+            hubv[t] = make_int2(-1, -1);
+            if (v < n) {
+                r0[t] = ld_ro(p.row_offsets + v);
+                r1[t] = ld_ro(p.row_offsets + v + 1);
+                if (p.hub2) hubv[t] = p.hub2[v];
+            }
+        }
+        bool todo[PER];
+        int parent[PER];
+        {
+            int nb[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                const int v = cs + t * 32 + lane;
+                todo[t] = v < n && !((word[t] >> lane) & 1u) && r1[t] > r0[t];
+                if (p.hub2) {
+                    nb[t][0] = todo[t] ? hubv[t].x : -1;
+                    nb[t][1] = todo[t] ? hubv[t].y : -1;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < K; k++)
+                        nb[t][k] = (todo[t] && r0[t] + k < r1[t]) ? ld_stream(p.column_indices + r0[t] + k) : -1;
+                }
+            }
+            unsigned w[PER][K];
+#pragma unroll
+            for (int t = 0; t < PER; t++)
+#pragma unroll
+                for (int k = 0; k < K; k++) w[t][k] = nb[t][k] >= 0 ? ld_mask(mask + (nb[t][k] >> 5)) : 0u;
+#pragma unroll
+            for (int t = 0; t < PER; t++) {
+                parent[t] = -1;
+#pragma unroll
+                for (int k = K - 1; k >= 0; k--)
+                    if (nb[t][k] >= 0 && ((w[t][k] >> (nb[t][k] & 31)) & 1u)) parent[t] = nb[t][k];
+            }
+        }
+        // (s.colstart / s.rel / s.out: each warp's own part is its queue)
+        if (p.hub2)
+            bottom_up_queue<PER, 0, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
+        else
+            bottom_up_queue<PER, K, K>(p, mask, todo, r0, r1, parent, s.colstart, s.rel, s.out);
+#pragma unroll
+        for (int t = 0; t < PER; t++) {
+            const int vb = cs + t * 32;
+            if (vb >= n) continue;  // warp-uniform
+            const int v = vb + lane;
+            const bool found = parent[t] >= 0;
+            const unsigned fb = __ballot_sync(0xffffffffu, found);
+            if (lane == 0) mask_out[vb >> 5] = word[t] | fb;  // this warp owns the whole word
+            if (found) {
+                p.labels[v] = PRED ? parent[t] : level + 1;
+                found_acc += pack(1u, (unsigned)(r1[t] - r0[t]));
+                any = true;
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
+    unsigned long long tot;
+    cta_exclusive_scan<B>(found_acc, s.scan_warp, &tot);
+    if (tid == 0 && tot != 0) atomicAdd(qe_out, tot);
+}
+
 // Writes the vertex ids of the set bits of `bits` (the word of vertices
 // v0..v0+31) whose positions, counted from `pos` in bit order, fall in
 // [lo, lo + n), to list[position - lo].
@@ -2158,6 +2259,9 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
             record_direction(p, s.visited_edges, pass, bu, s.mask, s.ul_in, s.ul_n, defer);
         if (LISTS && bu && s.ul_in >= 0)
             bottom_up_list<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3]);
+        else if (bu && !LISTS && s.prev_bu == 0 && defer && p.warp_bu)
+            // the first bottom-up level of a run, counting only: warp by warp
+            bottom_up_range_warp<B, PRED>(p, s, level, &p.st->qe[(pass + 1) % 3]);
         else if (bu && (LISTS || s.prev_bu == 0))
             // the first bottom-up level of a run: most vertices are unvisited, so the
             // chunks of vertex ids are walked directly

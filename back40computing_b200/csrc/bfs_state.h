@@ -161,6 +161,7 @@ struct BfsParams {
     int32_t hist_log;         // history cull table of 2^hist_log entries per CTA (0: off)
     int32_t bu_prefetch;      // 1: the first bottom-up level stages each next chunk with bulk copies
     int32_t warp_contract;    // 1: contract passes run warp by warp (no CTA barriers), 0: CTA sub-rounds
+    int32_t warp_bu;          // 1: first bottom-up levels of counting runs go warp by warp
     int32_t bu_defer;         // persistent bottom-up levels count their discoveries; the frontier is built
                               // from the mask buffers only when a top-down level follows
     const uint32_t *iso;      // bit v: v has no edges in or out; a search starts with these bits visited (null: none)

@@ -150,6 +150,7 @@ BfsParams make_params(b40c_bfs_problem *p, const b40c_bfs_policy &pol)
     k.bu_prefetch = pol.bottom_up_prefetch > 0 && k.bulk_ok && (reinterpret_cast<uintptr_t>(p->d_ro) & 15) == 0 ? 1 : 0;
     k.bu_defer = pol.bottom_up_defer_frontier > 0 ? 1 : 0;
     k.warp_contract = pol.warp_contract > 0 ? 1 : 0;
+    k.warp_bu = pol.warp_bottom_up > 0 ? 1 : 0;
     k.levels = p->instrument ? p->d_levels : nullptr;
     k.duty = p->instrument ? p->d_duty : nullptr;
     k.arrive = p->instrument ? p->d_arrive : nullptr;
@@ -180,6 +181,7 @@ b40c_bfs_policy default_policy(int strategy)
     pol.history_cull = -1;
     pol.queue_allocation = 2;  // measured faster than look-back on RMAT-22 (1.75 vs 2.29 ms)
     pol.warp_contract = 1;
+    pol.warp_bottom_up = 1;
     if (strategy == B40C_DIRECTION_OPTIMIZING) {
         // measured on B200 over 16 sources: the kernel variant carrying the
         // unvisited lists is slower overall (R-MAT 22 241 vs 222 us, random
@@ -217,6 +219,7 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
         if (in->history_cull) d.history_cull = in->history_cull > 0 ? 1 : -1;
         if (in->bottom_up_prefetch) d.bottom_up_prefetch = in->bottom_up_prefetch > 0 ? 1 : -1;
         if (in->warp_contract) d.warp_contract = in->warp_contract > 0 ? 1 : -1;
+        if (in->warp_bottom_up) d.warp_bottom_up = in->warp_bottom_up > 0 ? 1 : -1;
     }
     if (d.threads != 128 && d.threads != 256 && d.threads != 512)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.threads %d not built (available: 128, 256, 512)",

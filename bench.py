@@ -256,6 +256,7 @@ def level_report(problem, enact, srcs):
 # Policy ablations: (strategy, knob, values).  Each variant changes one knob of
 # the tuned policy; the first value of every row is the reference point.
 ABLATIONS = [
+    (4, "warp_bottom_up", [1, -1]),
     (4, "bottom_up_hub_probes", [1, -1]),
     (4, "bottom_up_defer_frontier", [1, -1]),
     (4, "bottom_up_long_list", [256, 64]),
@@ -263,6 +264,7 @@ ABLATIONS = [
     (4, "history_cull", [-1, 1]),
     (4, "ctas_per_sm", [4, 3, 2]),
     (4, "small_frontier_edges", [1024, 256, 4096]),
+    (0, "warp_contract", [1, -1]),
     (0, "queue_allocation", [2, 1]),
     (0, "chunk_edges", [2048, 1024, 512]),
     (0, "warp_gather_threshold", [32, 128]),

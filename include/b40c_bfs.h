@@ -140,6 +140,11 @@ typedef struct b40c_bfs_policy {
                                       warp of the grid, with no CTA barriers, and sends its winners to the
                                       vertex frontier in flushes of its own (one packed atomic each;
                                       default), -1 = CTA-wide sub-rounds (queue_allocation applies) */
+    int32_t warp_bottom_up;        /* direction-optimizing fused searches, the first bottom-up level of a
+                                      run when it only counts its discoveries: 1 = each warp takes blocks
+                                      of vertex ids dealt over every warp of the grid, with no CTA
+                                      barriers (default; bottom_up_prefetch does not apply), -1 = CTA-wide
+                                      chunks */
 } b40c_bfs_policy;
 
 typedef struct b40c_bfs_problem b40c_bfs_problem; /* opaque */

@@ -570,14 +570,17 @@ def test_history_cull(strategy, mode, preds):
 @pytest.mark.parametrize("threads", [128, 256, 512])
 @pytest.mark.parametrize("prefetch", [1, -1])
 @pytest.mark.parametrize("preds", [False, True])
-def test_cta_sizes_and_bottom_up_prefetch(threads, prefetch, preds):
-    """Every strategy built for 128-, 256- and 512-thread CTAs, and the first
-    bottom-up level with and without its chunks staged by bulk copies, gives
-    the oracle's distances and valid predecessors (graphs whose vertex count
-    is not a multiple of the chunk, so the ragged last chunk is covered)."""
+@pytest.mark.parametrize("warp_bu", [1, -1])
+def test_cta_sizes_and_bottom_up_prefetch(threads, prefetch, preds, warp_bu):
+    """Every strategy built for 128-, 256- and 512-thread CTAs, and counting
+    bottom-up levels warp by warp or in CTA-wide chunks (the first level of a
+    run with and without its chunks staged by bulk copies), gives the
+    oracle's distances and valid predecessors (graphs whose vertex count is
+    not a multiple of the chunk, so the ragged last chunk is covered)."""
     pol = N.Policy()
     pol.threads = threads
     pol.bottom_up_prefetch = prefetch
+    pol.warp_bottom_up = warp_bu
     pol.bottom_up_alpha = 4
     for kind, args in (("rmat", (1 << 15, 1 << 19)), ("rr", (20011, 10)), ("grid3d", (23,))):
         g = _graph(kind, *args)
@@ -635,4 +638,30 @@ def test_levels_by_warps_and_by_ctas(warp_contract, strategy, mode, preds, grid)
                 nv, ev = oracle.visited_stats(g.row_offsets, got)
                 queued = nv - 1 if strategy == EXPAND_CONTRACT else ev
                 assert e.GetStatistics()[0] == queued, f"{kind} source {s}: total_queued"
+        p.Destroy()
+
+
+@pytest.mark.parametrize("threads", [256, 512])
+@pytest.mark.parametrize("preds", [False, True])
+@pytest.mark.parametrize("grid", [0, 7])
+def test_bottom_up_level_by_warps(threads, preds, grid):
+    """The first bottom-up level of a run warp by warp (blocks of vertex ids
+    dealt over every warp of the grid, no CTA barriers): the oracle's
+    distances and valid predecessors on power-law, uniform and lattice
+    graphs, with a low switching threshold so that several bottom-up runs
+    occur, on the whole device and on a 7-CTA grid (many blocks per warp)."""
+    pol = N.Policy()
+    pol.threads = threads
+    pol.warp_bottom_up = 1
+    pol.bottom_up_alpha = 4
+    for kind, args in (("rmat", (1 << 16, 1 << 20)), ("rr", (40009, 8)), ("grid2d", (181,))):
+        g = _graph(kind, *args)
+        p = CsrProblem.from_graph(g, mark_predecessors=preds)
+        for s in sample_sources(g, 3, seed=29):
+            got = search(p, int(s), strategy=DIRECTION_OPTIMIZING, policy=pol, max_grid_size=grid)
+            want, _ = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+            if preds:
+                assert oracle.check_predecessors(g.row_offsets, g.column_indices, want, got) == (-1, 0)
+            else:
+                assert oracle.compare_labels(got, want) == -1, f"{kind} source {s}"
         p.Destroy()
