@@ -77,6 +77,8 @@ struct ExpandSmem {
     uint32_t *hist;                    // history cull table (dynamic shared memory past this struct), or null
     struct BuPrefetch *pf;             // bottom-up chunk prefetch buffer (dynamic shared memory), or null
     unsigned pf_phase;                 // parity of its mbarrier's next completion
+    uint16_t *wmap;                    // warp-autonomous levels: each warp's position -> entry map, or null
+    int32_t *wcol;                     // and its entry -> column index table (kWarpSlice entries per warp)
 };
 
 // The first bottom-up level of a run walks its CTA's vertex ids in chunks of
@@ -106,8 +108,16 @@ constexpr size_t kBuPrefetchBytes = (sizeof(BuPrefetch) + 15) & ~size_t(15);
 constexpr uint32_t kHistEmpty = 0xffffffffu;
 __device__ __forceinline__ unsigned hist_slot(int v, int log2) { return ((unsigned)v * 2654435761u) >> (32 - log2); }
 
+// Positions per slice of a warp-autonomous level (one cf chunk), and the
+// shared memory of a warp's tables for it (position -> entry map, entry ->
+// column index).
+constexpr int kWarpSlice = kChunkGrain;
+constexpr size_t kWarpTableBytes = kWarpSlice * (sizeof(uint16_t) + sizeof(int32_t));
+
 // Dynamic shared memory past ExpandSmem: the history table (when on), then
-// the bottom-up prefetch buffer (when on); the caller's barrier publishes both.
+// the bottom-up prefetch buffer (when on), then (CTAs of more than 256
+// threads) the warp-autonomous levels' tables; the caller's barrier
+// publishes them.
 template <int B, bool PRED>
 __device__ __forceinline__ void hist_init(const BfsParams &p, ExpandSmem<B, PRED> &s, unsigned char *smem_raw)
 {
@@ -124,6 +134,20 @@ __device__ __forceinline__ void hist_init(const BfsParams &p, ExpandSmem<B, PRED
     if (p.bu_prefetch) {
         s.pf = reinterpret_cast<BuPrefetch *>(smem_raw + off);
         if (threadIdx.x == 0) mbar_init(&s.pf->bar, 1);
+        off += kBuPrefetchBytes;
+    }
+    // the warp-autonomous levels' tables: in the sub-round arrays they leave
+    // unused for CTAs of up to 256 threads, past the rest for larger CTAs
+    // (kWarpTableBytes per warp; the host sizes the launch the same way)
+    if (B <= 256) {
+        s.wmap = s.own;
+        s.wcol = s.stage;
+    } else if (p.warp_contract) {
+        s.wmap = reinterpret_cast<uint16_t *>(smem_raw + off);
+        s.wcol = reinterpret_cast<int32_t *>(smem_raw + off + (B / 32) * kWarpSlice * sizeof(uint16_t));
+    } else {
+        s.wmap = nullptr;
+        s.wcol = nullptr;
     }
 }
 
@@ -708,10 +732,12 @@ __device__ __forceinline__ void contract_range(const BfsParams &p, ExpandSmem<B,
 // atomicAdd on the pass counter for the slots and the degree prefix, then the
 // entries, their degree prefixes P and their kChunkGrain boundaries in cf
 // (runs over more than kCfSerialChunks chunks written by the whole warp).
-// bc is overwritten with each entry's flush-relative degree prefix.  All 32
-// lanes call it with the same count.
+// bc is overwritten with each entry's flush-relative degree prefix.  A flush
+// whose output ends past `skip_above` edges of the pass total only counts
+// (see emit_frontier).  All 32 lanes call it with the same count.
 __device__ __forceinline__ void warp_emit(const BfsParams &p, const int32_t *bv, int32_t *bc, const int32_t *bd,
-                                          int count, const VertexFrontier &vout, unsigned long long *qe_out)
+                                          int count, const VertexFrontier &vout, unsigned long long *qe_out,
+                                          unsigned long long skip_above = ~0ull)
 {
     const int lane = threadIdx.x & 31;
     __syncwarp();
@@ -732,6 +758,13 @@ __device__ __forceinline__ void warp_emit(const BfsParams &p, const int32_t *bv,
     prefix = __shfl_sync(0xffffffffu, prefix, 0);
     const unsigned long long excl = incl - x;
     const unsigned g0 = (unsigned)(prefix >> 32), d0 = (unsigned)(prefix & 0xffffffffu);
+    if ((unsigned long long)d0 + (tot & 0xffffffffull) > skip_above) {
+        // counted above; the entries themselves are never read (the next level
+        // is certain to run bottom-up, as in emit_frontier)
+        if (lane == 0 && (unsigned long long)g0 + (tot >> 32) > (unsigned long long)p.vcap)
+            atomicOr(&p.st->error, kErrOverflow);
+        return;
+    }
     unsigned g = g0 + (unsigned)(excl >> 32);
     unsigned d = d0 + (unsigned)(excl & 0xffffffffu);
     bool long_run = false;
@@ -804,7 +837,8 @@ template <int PER, bool PRED, bool LEAVES>
 __device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask, const int (&v)[PER],
                                              const int (&u)[PER], const bool (&go)[PER], int label_value,
                                              int32_t *bv, int32_t *bc, int32_t *bd, int &count, int cap,
-                                             const VertexFrontier &vout, unsigned long long *qe_out)
+                                             const VertexFrontier &vout, unsigned long long *qe_out,
+                                             unsigned long long skip_above = ~0ull)
 {
     const int lane = threadIdx.x & 31;
     const int pre = p.precheck;
@@ -842,7 +876,7 @@ __device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask
     }
     if (LEAVES && leaves && lane == 0) atomicAdd(&p.st->total_queued, (unsigned long long)leaves);
     if (count + n_new > cap) {
-        warp_emit(p, bv, bc, bd, count, vout, qe_out);
+        warp_emit(p, bv, bc, bd, count, vout, qe_out, skip_above);
         __syncwarp();  // the flush has read the output before it is refilled
         count = 0;
     }
@@ -902,38 +936,44 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
     if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
 }
 
-// Warp-autonomous expand-contract level (policy.warp_contract, top-down-only
-// kernels with CTAs of at most 256 threads): each warp takes its
-// kChunkGrain-position slices (warp_slice0) of the frontier's flattened edge
-// space.  A slice starts at a chunk boundary, so
-// the chunk index gives the entry owning its first position; the warp loads
-// the entries overlapping the slice (32 per round trip), marks where each one
-// starts in its own position -> entry map and fills the map by a warp
-// max-scan; then every lane gathers kWarpSlice / 32 positions (a warp reads
-// 32 consecutive positions of a run, one coalesced segment) and runs the
-// visited test (warp_discover) with no CTA barrier.  Same labels and
-// frontier contents as expand_range (the reference's expand-contract,
-// expand_contract_atomic/cta.cuh:82-789); the entries' order differs.
-constexpr int kWarpSlice = kChunkGrain;  // positions per warp slice
+// Warp-autonomous top-down level (policy.warp_contract; levels with a full
+// sub-round per CTA): each warp takes its kWarpSlice-position slices
+// (warp_slice0) of the frontier's flattened edge space.  A slice starts at a
+// chunk boundary, so the chunk index gives the entry owning its first
+// position; the warp loads the entries overlapping the slice (32 per round
+// trip), marks where each one starts in its own position -> entry map and
+// fills the map by a warp max-scan; then every lane gathers kWarpSlice / 32
+// positions (a warp reads 32 consecutive positions of a run, one coalesced
+// segment) and runs the visited test (warp_discover) with no CTA barrier --
+// in halves when the warp's output holds fewer entries than a slice (CTAs
+// of more than 256 threads).  Same labels and frontier contents as
+// expand_range (the reference's expand-contract, expand_contract_atomic/
+// cta.cuh:82-789); the entries' order differs.  `skip_above` as in
+// emit_frontier (direction-optimizing searches).
 // With CULL = false (the expand pass of the edge-frontier strategies) the
 // gathered neighbours (and their predecessors) are written to the edge
 // frontier `eout` at their flattened positions instead: the reference's
 // two-phase expansion (two_phase/expand_atomic/cta.cuh:215-423).
+// Predecessor searches with CTAs of more than 256 threads keep the CTA-wide
+// sub-rounds (the entries' vertices would need a third table).
 template <int B, bool PRED, bool CULL = true>
 __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const VertexFrontier &in,
                                                   ExpandSmem<B, PRED> &s, int level, const VertexFrontier &vout,
-                                                  unsigned long long *qe_out, const EdgeFrontier *eout = nullptr)
+                                                  unsigned long long *qe_out, const EdgeFrontier *eout = nullptr,
+                                                  unsigned long long skip_above = ~0ull)
 {
-    static_assert(B <= 256, "a warp's output holds a whole slice's discoveries only up to 256-thread CTAs");
+    static_assert(B <= 256 || !PRED, "predecessor tables exist for CTAs of up to 256 threads only");
     constexpr int NW = B / 32;
     constexpr int PW = kWarpSlice / 32;    // positions per lane per slice
-    constexpr int CAP = kChunkMax / NW;    // a warp's output entries (>= kWarpSlice)
+    constexpr int CAP = kChunkMax / NW;    // a warp's output entries
+    constexpr int PB = CAP / 32 < PW ? CAP / 32 : PW;  // positions per lane per visited-test batch
+    static_assert(PW % PB == 0 && PB * 32 <= CAP, "a batch's winners fit the warp's output");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int32_t *bv = s.out + warp * CAP;
     int32_t *bc = s.colstart + warp * CAP;
     int32_t *bd = s.rel + warp * CAP;
-    uint16_t *own = s.own + warp * kWarpSlice;   // slice position -> table entry
-    int32_t *tcol = s.stage + warp * kWarpSlice;  // table entry -> column index of slice position 0
+    uint16_t *own = s.wmap + warp * kWarpSlice;  // slice position -> table entry
+    int32_t *tcol = s.wcol + warp * kWarpSlice;  // table entry -> column index of slice position 0
     int32_t *tver = PRED ? s.vert + warp * kWarpSlice : nullptr;
     const int q = s.q, re = s.E;
     int count = 0;  // warp-uniform
@@ -997,37 +1037,41 @@ __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const Vert
             reinterpret_cast<uint4 *>(own)[lane] = w;
         }
         __syncwarp();
-        // ---- gather and test ------------------------------------------------------
-        int v[PW], u[PW];
-        bool go[PW];
+        // ---- gather and test (or copy), PB positions per lane at a time -------------
 #pragma unroll
-        for (int t = 0; t < PW; t++) {
-            const int r = t * 32 + lane;
-            go[t] = r < len;
-            v[t] = -1;
-            u[t] = -1;
-            if (go[t]) {
-                const int k = own[r];
-                v[t] = ld_stream(p.column_indices + tcol[k] + r);
-                if (PRED) u[t] = tver[k];
-            }
-        }
-        if constexpr (CULL) {
-            any |= warp_discover<PW, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP, vout,
-                                                 qe_out);
-        } else {
+        for (int h = 0; h < PW / PB; h++) {
+            int v[PB], u[PB];
+            bool go[PB];
 #pragma unroll
-            for (int t = 0; t < PW; t++) {
+            for (int t = 0; t < PB; t++) {
+                const int r = (h * PB + t) * 32 + lane;
+                go[t] = r < len;
+                v[t] = -1;
+                u[t] = -1;
                 if (go[t]) {
-                    eout->v[x0 + t * 32 + lane] = v[t];
-                    if (PRED) eout->pred[x0 + t * 32 + lane] = u[t];
+                    const int k = own[r];
+                    v[t] = ld_stream(p.column_indices + tcol[k] + r);
+                    if (PRED) u[t] = tver[k];
+                }
+            }
+            if constexpr (CULL) {
+                any |= warp_discover<PB, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP, vout,
+                                                     qe_out, skip_above);
+            } else {
+#pragma unroll
+                for (int t = 0; t < PB; t++) {
+                    if (go[t]) {
+                        const int r = (h * PB + t) * 32 + lane;
+                        eout->v[x0 + r] = v[t];
+                        if (PRED) eout->pred[x0 + r] = u[t];
+                    }
                 }
             }
         }
         __syncwarp();  // the slice's tables are free for the next slice
     }
     if constexpr (CULL) {
-        if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
+        if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out, skip_above);
         if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
     }
 }
@@ -2059,10 +2103,10 @@ template <int B, bool PRED, bool LISTS, bool SUBGRID = false, bool BU = true>
 __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
 {
     // top-down levels with at least a full sub-round per CTA run warp by warp
-    // (expand_range_warp) in the top-down-only variants with CTAs of at most
-    // 256 threads, when the policy asks for it
+    // (expand_range_warp) when the policy asks for it (not in list mode, nor
+    // predecessor searches with CTAs of more than 256 threads)
     const auto warp_levels = [](const BfsParams &q, int E) {
-        return !BU && !LISTS && B <= 256 && q.warp_contract != 0 && warp_sized(E);
+        return !LISTS && (B <= 256 || !PRED) && q.warp_contract != 0 && warp_sized(E);
     };
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ExpandSmem<B, PRED> &s = *reinterpret_cast<ExpandSmem<B, PRED> *>(smem_raw);
@@ -2270,9 +2314,9 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
         else if (bu)
             // later bottom-up levels: the unvisited vertices of each window, compacted
             bottom_up_windows<B, PRED>(p, s, level, pass, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], defer);
-        else if (warp_levels(p, s.E))
+        else if (!BU && warp_levels(p, s.E))
         {
-            if constexpr (!BU && !LISTS && B <= 256)
+            if constexpr (!BU && !LISTS && (B <= 256 || !PRED))
                 expand_range_warp<B, PRED>(p, p.vf[level & 1], s, level, p.vf[(level + 1) & 1],
                                            &p.st->qe[(pass + 1) % 3]);
         }
@@ -2285,15 +2329,21 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
             // E* is at least the solo-phase threshold: a next level that small runs
             // top-down on CTA 0 before any switch test.
             unsigned long long skip_above = ~0ull;
-            if (p.direction_opt && !LISTS) {
+            if (BU && p.direction_opt && !LISTS) {
                 const unsigned long long un =
                     (unsigned long long)p.edges - min((unsigned long long)p.edges, s.visited_edges);
                 skip_above = max(un / (unsigned long long)(p.bu_alpha + 1),
                                  (unsigned long long)max(p.small_edges, 0));
             }
-            expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1], p.ef[0],
-                                               &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x, gridDim.x, false,
-                                               skip_above);
+            if (BU && warp_levels(p, s.E)) {
+                if constexpr (BU && !LISTS && (B <= 256 || !PRED))
+                    expand_range_warp<B, PRED>(p, p.vf[level & 1], s, level, p.vf[(level + 1) & 1],
+                                               &p.st->qe[(pass + 1) % 3], nullptr, skip_above);
+            } else {
+                expand_range<B, PRED, true, LISTS>(p, p.vf[level & 1], s, level, pass, p.vf[(level + 1) & 1],
+                                                   p.ef[0], &p.st->qe[(pass + 1) % 3], bar_phase, blockIdx.x,
+                                                   gridDim.x, false, skip_above);
+            }
         }
         __syncthreads();
         worked = true;
@@ -2378,8 +2428,8 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
             }
             if (tid == 0 && blockIdx.x == 0) p.st->qe[(pass + 1) % 3] = pack((unsigned)(q == 0 ? 0 : E), 0u);
             if (q > 0) {
-                if (B <= 256 && p.warp_contract && warp_sized(E)) {
-                    if constexpr (B <= 256)
+                if ((B <= 256 || !PRED) && p.warp_contract && warp_sized(E)) {
+                    if constexpr (B <= 256 || !PRED)
                         expand_range_warp<B, PRED, false>(p, p.vf[0], s, level, p.vf[1], nullptr, &p.ef[out_idx]);
                 } else {
                     expand_range<B, PRED, false>(p, p.vf[0], s, level, pass, p.vf[1], p.ef[out_idx], nullptr,

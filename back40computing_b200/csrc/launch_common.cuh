@@ -8,12 +8,15 @@ namespace rt {
 
 // Dynamic shared memory of the vertex/edge kernels: their state, plus the
 // history cull table and the bottom-up prefetch buffer when the policy turns
-// them on.
+// them on, plus the warp-autonomous levels' tables for CTAs of more than 256
+// threads (smaller CTAs keep them in their sub-round arrays); the same order
+// as hist_init.
 template <typename Smem>
 inline size_t kernel_smem(const b40c_bfs_policy &pol)
 {
     return ((sizeof(Smem) + 15) & ~size_t(15)) + (pol.history_cull > 0 ? sizeof(uint32_t) << kHistLog : 0) +
-           (pol.bottom_up_prefetch > 0 ? dev::kBuPrefetchBytes : 0);
+           (pol.bottom_up_prefetch > 0 ? dev::kBuPrefetchBytes : 0) +
+           (pol.warp_contract > 0 && pol.threads > 256 ? (size_t)(pol.threads / 32) * dev::kWarpTableBytes : 0);
 }
 
 // Grid of the set-up kernel: the full label/mask initialisation is a
