@@ -239,7 +239,9 @@ int resolve_policy(int strategy, const b40c_bfs_policy *in, b40c_bfs_policy *out
     if (d.bottom_up_scan != 1)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_scan must be 1 (per-lane list scans)");
     if (d.ctas_per_sm < 0) return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.ctas_per_sm must be >= 0");
-    if (d.bottom_up_prefetch == 0) d.bottom_up_prefetch = d.threads >= 512 ? 1 : -1;
+    // the prefetch buffer serves the CTA-wide first bottom-up level only (the
+    // warp-autonomous one reads straight from global memory)
+    if (d.bottom_up_prefetch == 0) d.bottom_up_prefetch = d.threads >= 512 && d.warp_bottom_up < 0 ? 1 : -1;
     if (d.bottom_up_long_list < 4)
         return b40c::fail(B40C_ERROR_INVALID_VALUE, "policy.bottom_up_long_list must be >= 4");
     *out = d;

@@ -132,7 +132,8 @@ typedef struct b40c_bfs_policy {
     int32_t bottom_up_prefetch;    /* the first bottom-up level of a run stages each next chunk's visited words,
                                       row offsets and hub pairs into shared memory with bulk copies while it
                                       scans the current one (25 KB of shared memory per CTA): 1 = on, -1 = off;
-                                      default: on for 512-thread CTAs (no occupancy cost), else off */
+                                      default: on for 512-thread CTAs whose first bottom-up levels run in
+                                      CTA-wide chunks (warp_bottom_up = -1), else off */
     int32_t warp_contract;         /* contract passes of the edge-frontier strategies (contract-expand,
                                       two-phase, hybrid), and with CTAs of up to 256 threads their expand
                                       passes and the top-down levels of expand-contract searches: 1 = each
