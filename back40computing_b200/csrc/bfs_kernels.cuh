@@ -479,16 +479,20 @@ __device__ __forceinline__ void expand_range(const BfsParams &p, const VertexFro
         }
         int k;
         {
+            // (an entry's degree prefix, row start and vertex are loaded together:
+            // one round trip, not two)
             const int i = i_cur + tid;
             bool inside = false;
             if (i < q) {
                 const int Pi = ld_cg(in.P + i);
+                const int ci = ld_cg(in.col + i);
+                const int vi = PRED ? ld_cg(in.v + i) : 0;
                 if (Pi < ce) {
                     inside = true;
                     const int start = max(Pi, cs);
                     s.rel[tid] = start - cs;
-                    s.colstart[tid] = ld_cg(in.col + i) + (start - Pi);
-                    if (PRED) s.vert[tid] = ld_cg(in.v + i);
+                    s.colstart[tid] = ci + (start - Pi);
+                    if (PRED) s.vert[tid] = vi;
                 }
             }
             k = __syncthreads_count(inside);
@@ -936,17 +940,101 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
     if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
 }
 
+// One warp's tables for the slice [x0, x0 + len) of a vertex frontier's
+// flattened edge space (x0 a chunk start): the entries overlapping the slice,
+// loaded 32 per round trip starting from the chunk index's owner of x0, each
+// marking its first slice position in `own` (cleared first), which a warp
+// max-scan then fills: position r belongs to the largest mark at or before r
+// (the entries start in increasing order).  tcol[k] + r is the column index
+// of slice position r in entry k's list; tver[k] is entry k's vertex.  All
+// 32 lanes call it, after every lane has finished reading the tables.
+template <bool PRED>
+__device__ __forceinline__ void warp_slice_map(const VertexFrontier &in, int q, int x0, int len, uint16_t *own,
+                                               int32_t *tcol, int32_t *tver)
+{
+    const int lane = threadIdx.x & 31;
+    reinterpret_cast<uint4 *>(own)[lane] = make_uint4(0u, 0u, 0u, 0u);
+    __syncwarp();
+    const int i0 = ld_cg(in.cf + x0 / kChunkGrain);  // owns position x0 (a chunk start)
+    int n = 0;
+    for (int i = i0;; i += 32) {
+        const int j = i + lane;
+        int Pj = INT_MAX;
+        int cj = 0, vj = -1;
+        if (j < q) {
+            Pj = ld_cg(in.P + j);
+            cj = ld_cg(in.col + j);
+            if (PRED) vj = ld_cg(in.v + j);
+        }
+        const bool inside = Pj < x0 + len;  // the inside lanes form a prefix (P increases)
+        const unsigned in_mask = __ballot_sync(0xffffffffu, inside);
+        const int k = n + lane;
+        if (inside && k < kWarpSlice) {
+            const int start = max(Pj, x0) - x0;
+            own[start] = (uint16_t)k;
+            tcol[k] = cj + (max(Pj, x0) - Pj) - start;  // + slice position = column index
+            if (PRED) tver[k] = vj;
+        }
+        n += __popc(in_mask);
+        if (in_mask != 0xffffffffu || i + 32 >= q) break;
+    }
+    __syncwarp();
+    static_assert(kWarpSlice == 256, "a lane's share of the map is one 16-byte word");
+    uint4 w = reinterpret_cast<uint4 *>(own)[lane];
+    unsigned e[8] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16, w.z & 0xffffu, w.z >> 16, w.w & 0xffffu, w.w >> 16};
+#pragma unroll
+    for (int t = 1; t < 8; t++) e[t] = max(e[t], e[t - 1]);
+    unsigned incl = e[7];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl = max(incl, y);
+    }
+    unsigned before = __shfl_up_sync(0xffffffffu, incl, 1);
+    if (lane == 0) before = 0;
+#pragma unroll
+    for (int t = 0; t < 8; t++) e[t] = max(e[t], before);
+    w.x = e[0] | (e[1] << 16);
+    w.y = e[2] | (e[3] << 16);
+    w.z = e[4] | (e[5] << 16);
+    w.w = e[6] | (e[7] << 16);
+    reinterpret_cast<uint4 *>(own)[lane] = w;
+    __syncwarp();
+}
+
+// Lane positions (h * PB + t) * 32 + lane, t < PB, of a slice of `len`
+// positions: the gathered neighbour (a coalesced read along a run) and its
+// predecessor, from the warp's tables.
+template <int PB, bool PRED>
+__device__ __forceinline__ void warp_slice_gather(const BfsParams &p, int h, int len, const uint16_t *own,
+                                                  const int32_t *tcol, const int32_t *tver, int (&v)[PB],
+                                                  int (&u)[PB], bool (&go)[PB])
+{
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int t = 0; t < PB; t++) {
+        const int r = (h * PB + t) * 32 + lane;
+        go[t] = r < len;
+        v[t] = -1;
+        u[t] = -1;
+        if (go[t]) {
+            const int k = own[r];
+            v[t] = ld_stream(p.column_indices + tcol[k] + r);
+            if (PRED) u[t] = tver[k];
+        }
+    }
+}
+
 // Warp-autonomous top-down level (policy.warp_contract; levels with a full
 // sub-round per CTA): each warp takes its kWarpSlice-position slices
-// (warp_slice0) of the frontier's flattened edge space.  A slice starts at a
-// chunk boundary, so the chunk index gives the entry owning its first
-// position; the warp loads the entries overlapping the slice (32 per round
-// trip), marks where each one starts in its own position -> entry map and
-// fills the map by a warp max-scan; then every lane gathers kWarpSlice / 32
-// positions (a warp reads 32 consecutive positions of a run, one coalesced
-// segment) and runs the visited test (warp_discover) with no CTA barrier --
-// in halves when the warp's output holds fewer entries than a slice (CTAs
-// of more than 256 threads).  Same labels and frontier contents as
+// (warp_slice0) of the frontier's flattened edge space, builds its tables
+// for a slice (warp_slice_map), gathers kWarpSlice / 32 positions per lane
+// (a warp reads 32 consecutive positions of a run, one coalesced segment)
+// and runs the visited test (warp_discover) with no CTA barrier.  With CTAs
+// of more than 256 threads a warp's output holds half a slice: each slice is
+// tested in two halves.  (Building the next slice's tables and issuing its
+// loads before testing the current slice measured slower: 908 -> 968 us per
+// R-MAT 22 search; the second slice's registers spill.)  Same labels and frontier contents as
 // expand_range (the reference's expand-contract, expand_contract_atomic/
 // cta.cuh:82-789); the entries' order differs.  `skip_above` as in
 // emit_frontier (direction-optimizing searches).
@@ -982,81 +1070,15 @@ __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const Vert
     for (long long x64 = (long long)warp_slice0(warp) * kWarpSlice; x64 < re; x64 += stride) {
         const int x0 = (int)x64;
         const int len = min(kWarpSlice, re - x0);
-        // ---- the entries overlapping [x0, x0 + len), 32 per round trip; each
-        // marks its first slice position in the map (cleared first) -------------
-        reinterpret_cast<uint4 *>(own)[lane] = make_uint4(0u, 0u, 0u, 0u);
-        __syncwarp();
-        const int i0 = ld_cg(in.cf + x0 / kChunkGrain);  // owns position x0 (a chunk start)
-        int n = 0;
-        for (int i = i0;; i += 32) {
-            const int j = i + lane;
-            int Pj = INT_MAX;
-            int cj = 0, vj = -1;
-            if (j < q) {
-                Pj = ld_cg(in.P + j);
-                cj = ld_cg(in.col + j);
-                if (PRED) vj = ld_cg(in.v + j);
-            }
-            const bool inside = Pj < x0 + len;  // the inside lanes form a prefix (P increases)
-            const unsigned in_mask = __ballot_sync(0xffffffffu, inside);
-            const int k = n + lane;
-            if (inside && k < kWarpSlice) {
-                const int start = max(Pj, x0) - x0;
-                own[start] = (uint16_t)k;
-                tcol[k] = cj + (max(Pj, x0) - Pj) - start;  // + slice position = column index
-                if (PRED) tver[k] = vj;
-            }
-            n += __popc(in_mask);
-            if (in_mask != 0xffffffffu || i + 32 >= q) break;
-        }
-        __syncwarp();
-        // ---- position r belongs to the largest mark at or before r (entries start
-        // in increasing order): lane L scans positions 8L .. 8L + 7, then the lanes'
-        // maxima are combined by a warp max-scan ------------------------------------
-        {
-            static_assert(PW == 8, "a lane's share of the map is one 16-byte word");
-            uint4 w = reinterpret_cast<uint4 *>(own)[lane];
-            unsigned e[8] = {w.x & 0xffffu, w.x >> 16, w.y & 0xffffu, w.y >> 16,
-                             w.z & 0xffffu, w.z >> 16, w.w & 0xffffu, w.w >> 16};
-#pragma unroll
-            for (int t = 1; t < 8; t++) e[t] = max(e[t], e[t - 1]);
-            unsigned incl = e[7];
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const unsigned y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl = max(incl, y);
-            }
-            unsigned before = __shfl_up_sync(0xffffffffu, incl, 1);
-            if (lane == 0) before = 0;
-#pragma unroll
-            for (int t = 0; t < 8; t++) e[t] = max(e[t], before);
-            w.x = e[0] | (e[1] << 16);
-            w.y = e[2] | (e[3] << 16);
-            w.z = e[4] | (e[5] << 16);
-            w.w = e[6] | (e[7] << 16);
-            reinterpret_cast<uint4 *>(own)[lane] = w;
-        }
-        __syncwarp();
-        // ---- gather and test (or copy), PB positions per lane at a time -------------
+        warp_slice_map<PRED>(in, q, x0, len, own, tcol, tver);
 #pragma unroll
         for (int h = 0; h < PW / PB; h++) {
             int v[PB], u[PB];
             bool go[PB];
-#pragma unroll
-            for (int t = 0; t < PB; t++) {
-                const int r = (h * PB + t) * 32 + lane;
-                go[t] = r < len;
-                v[t] = -1;
-                u[t] = -1;
-                if (go[t]) {
-                    const int k = own[r];
-                    v[t] = ld_stream(p.column_indices + tcol[k] + r);
-                    if (PRED) u[t] = tver[k];
-                }
-            }
+            warp_slice_gather<PB, PRED>(p, h, len, own, tcol, tver, v, u, go);
             if constexpr (CULL) {
-                any |= warp_discover<PB, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP, vout,
-                                                     qe_out, skip_above);
+                any |= warp_discover<PB, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP,
+                                                     vout, qe_out, skip_above);
             } else {
 #pragma unroll
                 for (int t = 0; t < PB; t++) {

@@ -85,14 +85,17 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
             const int i = base + tid;
             bool inside = false;
             if (i < q) {
+                // (degree prefix, row start and vertex in one round trip)
                 const int Pi = ld_cg(in.P + i);
+                const int ci = ld_cg(in.col + i);
+                const int vi = ld_cg(in.v + i);
                 if (Pi < ce && i - i_cur <= kChunkMax) {
                     inside = true;
                     const int j = i - i_cur;
                     const int start = max(Pi, cs);
                     s.rel[j] = start - cs;
-                    s.colstart[j] = ld_cg(in.col + i) + (start - Pi);
-                    s.fm[j] = ld_keep64(fcur + ld_cg(in.v + i)) & s.active;
+                    s.colstart[j] = ci + (start - Pi);
+                    s.fm[j] = ld_keep64(fcur + vi) & s.active;
                 }
             }
             const int c = __syncthreads_count(inside);
