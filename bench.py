@@ -75,7 +75,29 @@ def parse():
     ap.add_argument("--ablate", action="store_true",
                     help="policy ablations (the reference's gather / cull microbenchmarks, test/bfs/microbench/): "
                          "each knob's variants interleaved on the same searches; prints one JSON line and exits")
+    ap.add_argument("--policy", action="append", default=[], metavar="KNOB=VALUE",
+                    help="override one field of the single-source search's policy (b40c_bfs_policy), e.g. "
+                         "warp_contract=-1; repeatable; recorded in the line's config")
     return ap.parse_args()
+
+
+def policy_overrides(base, items):
+    """The policy `base` (or the library defaults, None) with KNOB=VALUE overrides;
+    None when there are none and no base."""
+    from back40computing_b200 import _native as N
+    if not items:
+        return base
+    pol = N.Policy()
+    if base is not None:
+        for f, _ in N.Policy._fields_:
+            setattr(pol, f, getattr(base, f))
+    names = {f for f, _ in N.Policy._fields_}
+    for item in items:
+        knob, _, value = item.partition("=")
+        if knob not in names or not value.lstrip("-").isdigit():
+            raise SystemExit(f"--policy {item!r}: expected KNOB=INT with KNOB one of {sorted(names)}")
+        setattr(pol, knob, int(value))
+    return pol
 
 
 def build_graph(cfg_name):
@@ -333,6 +355,14 @@ def replica_gteps(edges_per_replica, world, seconds):
     return float(edges_per_replica) * world / seconds / 1e9
 
 
+def workload_config(args, g, sources):
+    """The line's `config`: the workload alone, the same for both arms (how a
+    search runs goes under the line's `search` key)."""
+    return {"workload": CONFIGS[args.config]["workload"], "graph": args.config, "vertices": int(g.nodes),
+            "edges": int(g.edges), "sources": int(sources),
+            "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6)}
+
+
 def run_reference(args, rank):
     """--impl reference: the reference's CPU BFS on the host cores (independent
     searches in parallel threads; ctypes releases the GIL during each call)."""
@@ -368,8 +398,8 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int32",
         "data": "synthetic (seeded generator, no dataset)",
-        "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
-                   "sample_per_step": f"{len(per_step)} searches in parallel threads"},
+        "config": workload_config(args, g, len(srcs)),
+        "search": {"sample_per_step": f"{len(per_step)} searches in parallel threads"},
         "cpu_baseline": {"value": value, "unit": "GTEPS", "cores": threads, "kind": kind,
                          "sample": f"{len(per_step)} independent searches per step on {threads} threads"},
         "e2e": {"value": value, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -613,7 +643,7 @@ def main():
     from back40computing_b200 import autotune
     graph_class = autotune.classify(g)
     kind = {0: "expand-contract", 4: "direction-optimizing"}.get(args.strategy)
-    policy = autotune.policy_for(graph_class, kind) if kind else None
+    policy = policy_overrides(autotune.policy_for(graph_class, kind) if kind else None, args.policy)
     enactor = ENACTORS[args.strategy](policy=policy)
     N.check(problem.Reset(enactor.GetFrontierType(), 1.3), "Reset")
 
@@ -740,12 +770,11 @@ def main():
             "metric": METRIC, "value": value, "unit": "GTEPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int32", "data": "synthetic (seeded generator, no dataset)",
-            "config": {"workload": CONFIGS[args.config]["workload"], "graph": args.config,
-                       "vertices": g.nodes, "edges": g.edges, "searches_per_step": len(srcs),
-                       "strategy": STRATEGY_NAMES[args.strategy],
-                       "policy": f"autotuned for class {graph_class}" if policy is not None else "library defaults",
+            "config": workload_config(args, g, len(srcs)),
+            "search": {"searches_per_step": len(srcs), "strategy": STRATEGY_NAMES[args.strategy],
+                       "policy": (f"autotuned for class {graph_class}" if policy is not None else "library defaults")
+                       + ("".join(f", {x}" for x in args.policy)),
                        "mode": ["fused persistent", "per-level launches", "cuda graph"][args.mode],
-                       "l2": "inputs larger than L2 (CSR %.0f MB)" % ((g.edges + g.nodes) * 4 / 1e6),
                        "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
