@@ -237,8 +237,15 @@ def test_queries_join_a_running_batch_with_exact_labels():
         tickets = {}
         for s in first:
             tickets[s] = srv.submit(gid, s, -1, labels=outs[s], arrival_ns=t0)
+        # the late queries arrive once the first batch is on the device (a batch
+        # of this graph runs for many milliseconds)
+        import time
+        deadline = time.monotonic() + 30
+        while srv.counters()["batches"] < 1 and time.monotonic() < deadline:
+            time.sleep(0.0002)
+        assert srv.counters()["batches"] == 1
         for k, s in enumerate(later):
-            tickets[s] = srv.submit(gid, s, 3 if k == 2 else -1, labels=outs[s], arrival_ns=t0 + 2_000_000)
+            tickets[s] = srv.submit(gid, s, 3 if k == 2 else -1, labels=outs[s], arrival_ns=srv.now_ns())
         srv.drain()
         recs = {s: srv.result(t) for s, t in tickets.items()}
         c = srv.counters()
