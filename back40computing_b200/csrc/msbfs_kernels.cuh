@@ -203,6 +203,103 @@ __device__ __forceinline__ void ms_expand_range(const BfsParams &p, const MsPara
 // thread writes V[v] and F[next][v].
 constexpr int kPullLongList = 256;
 
+// One warp's block of 32 consecutive vertices [vb, vb + 32) of a pull level,
+// below `re`: every lane takes one vertex, eight neighbours per step, stopping
+// once every missing source is found; lists longer than kPullLongList are
+// searched by the whole warp afterwards.  Only v's own lane writes V[v] and
+// F[next][v]; the labels are stored source by source, one coalesced store per
+// warp.  Returns whether the lane's vertex joins the next frontier (it was
+// reached and has edges), with its row start and degree.
+template <int B>
+__device__ __forceinline__ bool ms_pull_block(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
+                                              int vb, int re, unsigned long long &found, int &r0_out,
+                                              int &deg_out)
+{
+    const int lane = threadIdx.x & 31;
+    constexpr int U = 8;
+    const unsigned long long *fcur = m.fmask[level & 1];
+    unsigned long long *fnext = m.fmask[(level + 1) & 1];
+    const unsigned long long active = s.active;
+    const long long n = p.nodes;
+    const int v = vb + lane;
+    const bool inr = v < re;
+    unsigned long long vold = 0, missing = 0;
+    int r0 = 0, r1 = 0;
+    // vertices without edges are never reached (their labels are set at the end)
+    const bool iso = inr && p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u);
+    if (inr && !iso) {
+        vold = ld_keep64(m.visited + v);
+        missing = active & ~vold;
+        if (missing) {
+            r0 = ld_ro(p.row_offsets + v);
+            r1 = ld_ro(p.row_offsets + v + 1);
+        }
+    }
+    unsigned long long acc = 0;
+    if (missing && p.hub2) {
+        // the vertex's two highest-degree neighbours first (one coalesced load)
+        const int2 h = p.hub2[v];
+        if (h.x >= 0) acc |= ld_keep64(fcur + h.x) & missing;
+        if (h.y >= 0) acc |= ld_keep64(fcur + h.y) & missing;
+        if (acc == missing || r1 - r0 <= 2) missing = 0;  // nothing left to look for
+    }
+    const bool longlist = missing && (r1 - r0) > kPullLongList;
+    if (missing && !longlist) {
+        for (int e = r0; e < r1 && acc != missing;) {
+            // eight neighbours per step from two 16-byte loads
+            int nb[U], q0[4], q1[4];
+            e = ld_quad(p.column_indices, p.edges, e, r1, q0);
+            e = ld_quad(p.column_indices, p.edges, e, r1, q1);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                nb[k] = q0[k];
+                nb[4 + k] = q1[k];
+            }
+            unsigned long long fm[U];
+#pragma unroll
+            for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_keep64(fcur + nb[k]) : 0ull;
+#pragma unroll
+            for (int k = 0; k < U; k++) acc |= fm[k] & missing;
+        }
+    }
+    unsigned lmask = __ballot_sync(0xffffffffu, longlist);
+    while (lmask) {
+        const int owner = __ffs(lmask) - 1;
+        lmask &= lmask - 1;
+        const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
+        const unsigned long long miss = __shfl_sync(0xffffffffu, missing, owner);
+        unsigned long long a = 0;
+        for (int eb = lr0; eb < lr1; eb += 32) {
+            const int ee = eb + lane;
+            if (ee < lr1) a |= ld_keep64(fcur + ld_stream(p.column_indices + ee)) & miss;
+            for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
+            if (a == miss) break;
+        }
+        if (lane == owner) acc = a;
+    }
+    found |= acc;
+    if (acc) {
+        m.visited[v] = vold | acc;
+        fnext[v] = acc;
+        s.flag = 1;
+    }
+    // labels, source by source: one coalesced store per warp
+    const unsigned long long wor_lo = __reduce_or_sync(0xffffffffu, (unsigned)(acc & 0xffffffffull));
+    const unsigned long long wor_hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc >> 32));
+    unsigned long long wor = wor_lo | (wor_hi << 32);
+    while (wor) {
+        const int src = __ffsll((long long)wor) - 1;
+        wor &= wor - 1;
+        if ((acc >> src) & 1ull) st_stream(m.labels + (long long)src * n + v, level + 1 - s.off[src]);
+    }
+    r0_out = r0;
+    deg_out = r1 - r0;
+    return acc && r1 > r0;
+}
+
+// Pull level (symmetric graphs) in CTA-wide chunks: each warp takes PER
+// blocks of the CTA's chunk; the chunk's discoveries go to the next frontier
+// through one emit per chunk.
 template <int B>
 __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
                                               const VertexFrontier &vout, unsigned long long *qe_out,
@@ -210,11 +307,6 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
 {
     const int tid = threadIdx.x, lane = tid & 31;
     constexpr int PER = kChunkMax / B;
-    constexpr int U = 8;
-    const unsigned long long *fcur = m.fmask[level & 1];
-    unsigned long long *fnext = m.fmask[(level + 1) & 1];
-    const unsigned long long active = s.active;
-    const long long n = p.nodes;
     int rs, re;
     cta_range(p.nodes, blockIdx.x, gridDim.x, rs, re);
     for (int cs = rs; cs < re; cs += kChunkMax) {
@@ -225,77 +317,8 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
             const int vb = cs + t * B + (tid & ~31);
             if (vb >= re) break;  // warp-uniform
             const int v = vb + lane;
-            const bool inr = v < re;
-            unsigned long long vold = 0, missing = 0;
-            int r0 = 0, r1 = 0;
-            // vertices without edges are never reached (their labels are set at the end)
-            const bool iso = inr && p.iso && ((p.iso[v >> 5] >> (v & 31)) & 1u);
-            if (inr && !iso) {
-                vold = ld_keep64(m.visited + v);
-                missing = active & ~vold;
-                if (missing) {
-                    r0 = ld_ro(p.row_offsets + v);
-                    r1 = ld_ro(p.row_offsets + v + 1);
-                }
-            }
-            unsigned long long acc = 0;
-            if (missing && p.hub2) {
-                // the vertex's two highest-degree neighbours first (one coalesced load)
-                const int2 h = p.hub2[v];
-                if (h.x >= 0) acc |= ld_keep64(fcur + h.x) & missing;
-                if (h.y >= 0) acc |= ld_keep64(fcur + h.y) & missing;
-                if (acc == missing || r1 - r0 <= 2) missing = 0;  // nothing left to look for
-            }
-            const bool longlist = missing && (r1 - r0) > kPullLongList;
-            if (missing && !longlist) {
-                for (int e = r0; e < r1 && acc != missing;) {
-                    // eight neighbours per step from two 16-byte loads
-                    int nb[U], q0[4], q1[4];
-                    e = ld_quad(p.column_indices, p.edges, e, r1, q0);
-                    e = ld_quad(p.column_indices, p.edges, e, r1, q1);
-#pragma unroll
-                    for (int k = 0; k < 4; k++) {
-                        nb[k] = q0[k];
-                        nb[4 + k] = q1[k];
-                    }
-                    unsigned long long fm[U];
-#pragma unroll
-                    for (int k = 0; k < U; k++) fm[k] = nb[k] >= 0 ? ld_keep64(fcur + nb[k]) : 0ull;
-#pragma unroll
-                    for (int k = 0; k < U; k++) acc |= fm[k] & missing;
-                }
-            }
-            unsigned lmask = __ballot_sync(0xffffffffu, longlist);
-            while (lmask) {
-                const int owner = __ffs(lmask) - 1;
-                lmask &= lmask - 1;
-                const int lr0 = __shfl_sync(0xffffffffu, r0, owner), lr1 = __shfl_sync(0xffffffffu, r1, owner);
-                const unsigned long long miss = __shfl_sync(0xffffffffu, missing, owner);
-                unsigned long long a = 0;
-                for (int eb = lr0; eb < lr1; eb += 32) {
-                    const int ee = eb + lane;
-                    if (ee < lr1) a |= ld_keep64(fcur + ld_stream(p.column_indices + ee)) & miss;
-                    for (int off = 16; off > 0; off >>= 1) a |= __shfl_xor_sync(0xffffffffu, a, off);
-                    if (a == miss) break;
-                }
-                if (lane == owner) acc = a;
-            }
-            found |= acc;
-            if (acc) {
-                m.visited[v] = vold | acc;
-                fnext[v] = acc;
-                s.flag = 1;
-            }
-            // labels, source by source: one coalesced store per warp
-            const unsigned long long wor_lo = __reduce_or_sync(0xffffffffu, (unsigned)(acc & 0xffffffffull));
-            const unsigned long long wor_hi = __reduce_or_sync(0xffffffffu, (unsigned)(acc >> 32));
-            unsigned long long wor = wor_lo | (wor_hi << 32);
-            while (wor) {
-                const int src = __ffsll((long long)wor) - 1;
-                wor &= wor - 1;
-                if ((acc >> src) & 1ull) st_stream(m.labels + (long long)src * n + v, level + 1 - s.off[src]);
-            }
-            const bool push = acc && r1 > r0;
+            int r0, deg;
+            const bool push = ms_pull_block<B>(p, m, s, level, vb, re, found, r0, deg);
             const unsigned bal = __ballot_sync(0xffffffffu, push);
             if (bal) {
                 const int leader = __ffs(bal) - 1;
@@ -306,7 +329,7 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
                     const int slot = base + __popc(bal & lanemask_lt());
                     s.out[slot] = v;
                     s.colstart[slot] = r0;
-                    s.rel[slot] = r1 - r0;
+                    s.rel[slot] = deg;
                 }
             }
         }
@@ -314,6 +337,46 @@ __device__ __forceinline__ void ms_pull_range(const BfsParams &p, const MsParams
         emit_frontier<B>(p, s, level, vout, qe_out);
         __syncthreads();
     }
+}
+
+// Pull level warp by warp (policy.warp_contract): blocks of 32 vertices dealt
+// warp-major over every warp of the grid (warp_slice0), no CTA barrier; each
+// warp's discoveries collect in its slice of the shared tables and go to the
+// next frontier in flushes of their own (warp_emit).  A warp whose block holds
+// a long scan no longer holds up the rest of its CTA.
+template <int B>
+__device__ __forceinline__ void ms_pull_range_warp(const BfsParams &p, const MsParams &m, MsSmem<B> &s, int level,
+                                                   const VertexFrontier &vout, unsigned long long *qe_out,
+                                                   unsigned long long &found)
+{
+    constexpr int NW = B / 32;
+    constexpr int CAP = kChunkMax / NW;  // >= 32: a block's discoveries always fit after a flush
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *bv = s.out + warp * CAP;
+    int32_t *bc = s.colstart + warp * CAP;
+    int32_t *bd = s.rel + warp * CAP;
+    int count = 0;  // warp-uniform
+    const int n = p.nodes;
+    const long long stride = (long long)gridDim.x * NW * 32;
+    for (long long b64 = (long long)warp_slice0(warp) * 32; b64 < n; b64 += stride) {
+        const int vb = (int)b64;
+        int r0, deg;
+        const bool push = ms_pull_block<B>(p, m, s, level, vb, n, found, r0, deg);
+        const unsigned bal = __ballot_sync(0xffffffffu, push);
+        if (count + __popc(bal) > CAP) {
+            warp_emit(p, bv, bc, bd, count, vout, qe_out);
+            __syncwarp();  // the flush has read the output before it is refilled
+            count = 0;
+        }
+        if (push) {
+            const int slot = count + __popc(bal & lanemask_lt());
+            bv[slot] = vb + lane;
+            bc[slot] = r0;
+            bd[slot] = deg;
+        }
+        count += __popc(bal);
+    }
+    if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
 }
 
 // Block 0, between the grid barriers that end level `level` (no CTA touches the
@@ -440,7 +503,9 @@ __global__ void __launch_bounds__(B, 1024 / B) msbfs_kernel(BfsParams p, MsParam
         const bool pull = m.pull_ok && (long long)s.E * p.bu_alpha > (long long)p.edges;
         if (tid == 0 && blockIdx.x == 0 && pull && p.levels && pass < kMaxLevelRecords) p.levels[pass].bottom_up = 1;
         unsigned long long found = 0;
-        if (pull)
+        if (pull && p.warp_contract)
+            ms_pull_range_warp<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], found);
+        else if (pull)
             ms_pull_range<B>(p, m, s, level, p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3], found);
         else
             ms_expand_range<B>(p, m, s, level, p.vf[level & 1], p.vf[(level + 1) & 1], &p.st->qe[(pass + 1) % 3],

@@ -136,7 +136,8 @@ typedef struct b40c_bfs_policy {
                                       CTA-wide chunks (warp_bottom_up = -1), else off */
     int32_t warp_contract;         /* contract passes of the edge-frontier strategies (contract-expand,
                                       two-phase, hybrid), and with CTAs of up to 256 threads their expand
-                                      passes and the top-down levels of expand-contract searches: 1 = each
+                                      passes, the top-down levels of expand-contract and direction-
+                                      optimizing searches, and the pull levels of batched searches: 1 = each
                                       warp works through its own slices of the level, dealt over every
                                       warp of the grid, with no CTA barriers, and sends its winners to the
                                       vertex frontier in flushes of its own (one packed atomic each;
