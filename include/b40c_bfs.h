@@ -134,14 +134,16 @@ typedef struct b40c_bfs_policy {
                                       scans the current one (25 KB of shared memory per CTA): 1 = on, -1 = off;
                                       default: on for 512-thread CTAs whose first bottom-up levels run in
                                       CTA-wide chunks (warp_bottom_up = -1), else off */
-    int32_t warp_contract;         /* contract passes of the edge-frontier strategies (contract-expand,
-                                      two-phase, hybrid), and with CTAs of up to 256 threads their expand
-                                      passes, the top-down levels of expand-contract and direction-
-                                      optimizing searches, and the pull levels of batched searches: 1 = each
-                                      warp works through its own slices of the level, dealt over every
-                                      warp of the grid, with no CTA barriers, and sends its winners to the
-                                      vertex frontier in flushes of its own (one packed atomic each;
-                                      default), -1 = CTA-wide sub-rounds (queue_allocation applies) */
+    int32_t warp_contract;         /* levels with at least a full 2048-edge sub-round per CTA, warp by warp:
+                                      the contract and expand passes of the edge-frontier strategies
+                                      (contract-expand, two-phase, hybrid), the top-down levels of
+                                      expand-contract and direction-optimizing searches (predecessor
+                                      searches: CTAs of up to 256 threads), and the pull levels of
+                                      batched searches.  1 = each warp works through its own slices of
+                                      the level, dealt over every warp of the grid, with no CTA barriers,
+                                      and sends its winners to the vertex frontier in flushes of its own
+                                      (one packed atomic each; default), -1 = CTA-wide sub-rounds
+                                      (queue_allocation applies) */
     int32_t warp_bottom_up;        /* direction-optimizing fused searches, the first bottom-up level of a
                                       run when it only counts its discoveries: 1 = each warp takes blocks
                                       of vertex ids dealt over every warp of the grid, with no CTA
