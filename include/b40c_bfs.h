@@ -79,7 +79,9 @@ enum {
  * template parameters, e.g. enactor_contract_expand.cuh:339-373).  A zero
  * field means "use the tuned default". */
 typedef struct b40c_bfs_policy {
-    int32_t threads;               /* CTA size (256: the size the kernels are built for) */
+    int32_t threads;               /* CTA size: 128, 256 or 512 (default 256; b40c_bfs_enact with no policy
+                                      at all runs 512 for the distance searches of expand-contract,
+                                      contract-expand and two-phase) */
     int32_t ctas_per_sm;           /* resident CTAs per SM for persistent grids (0 = occupancy limit) */
     int32_t chunk_edges;           /* edges (or edge-frontier items) per sub-round of a CTA's share of a level:
                                       a multiple of 32 in [256, 2048] (default 2048) */
