@@ -837,10 +837,10 @@ __device__ __forceinline__ int warp_slice0(int warp) { return warp * (int)gridDi
 // without edges are added to total_queued (vertex-frontier strategies queue
 // every discovered vertex, expand_contract_atomic/cta.cuh:432-466).  Returns
 // whether this lane labelled a vertex.  All 32 lanes call it.
-template <int PER, bool PRED, bool LEAVES>
+template <int PER, bool PRED, bool LEAVES, int CAP>
 __device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask, const int (&v)[PER],
                                              const int (&u)[PER], const bool (&go)[PER], int label_value,
-                                             int32_t *bv, int32_t *bc, int32_t *bd, int &count, int cap,
+                                             int32_t *bv, int32_t *bc, int32_t *bd, int &count,
                                              const VertexFrontier &vout, unsigned long long *qe_out,
                                              unsigned long long skip_above = ~0ull)
 {
@@ -870,30 +870,39 @@ __device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask
             any = true;
         }
     }
-    int n_new = 0;
     unsigned leaves = 0;
 #pragma unroll
     for (int t = 0; t < PER; t++) {
         deg[t] -= r0[t];  // 0 for the lanes that found nothing
-        n_new += __popc(__ballot_sync(0xffffffffu, deg[t] > 0));
         if (LEAVES) leaves += __popc(__ballot_sync(0xffffffffu, found[t] && deg[t] == 0));
     }
     if (LEAVES && leaves && lane == 0) atomicAdd(&p.st->total_queued, (unsigned long long)leaves);
-    if (count + n_new > cap) {
-        warp_emit(p, bv, bc, bd, count, vout, qe_out, skip_above);
-        __syncwarp();  // the flush has read the output before it is refilled
-        count = 0;
-    }
+    // append, flushing first when the winners could overrun the output; a batch
+    // larger than the output (CTAs of more than 256 threads test 256 neighbours
+    // into 128 entries) is appended in halves
+    constexpr int HALF = PER * 32 > CAP ? PER / 2 : PER;
+    static_assert(HALF * 32 <= CAP && PER % HALF == 0, "a half batch's winners fit the warp's output");
 #pragma unroll
-    for (int t = 0; t < PER; t++) {
-        const unsigned bal = __ballot_sync(0xffffffffu, deg[t] > 0);
-        if (deg[t] > 0) {
-            const int slot = count + __popc(bal & lanemask_lt());
-            bv[slot] = v[t];
-            bc[slot] = r0[t];
-            bd[slot] = deg[t];
+    for (int h0 = 0; h0 < PER; h0 += HALF) {
+        int n_new = 0;
+#pragma unroll
+        for (int t = h0; t < h0 + HALF; t++) n_new += __popc(__ballot_sync(0xffffffffu, deg[t] > 0));
+        if (count + n_new > CAP) {
+            warp_emit(p, bv, bc, bd, count, vout, qe_out, skip_above);
+            __syncwarp();  // the flush has read the output before it is refilled
+            count = 0;
         }
-        count += __popc(bal);
+#pragma unroll
+        for (int t = h0; t < h0 + HALF; t++) {
+            const unsigned bal = __ballot_sync(0xffffffffu, deg[t] > 0);
+            if (deg[t] > 0) {
+                const int slot = count + __popc(bal & lanemask_lt());
+                bv[slot] = v[t];
+                bc[slot] = r0[t];
+                bd[slot] = deg[t];
+            }
+            count += __popc(bal);
+        }
     }
     return any;
 }
@@ -934,7 +943,7 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
             v[t] = go[t] ? ld_cg(in.v + i) : -1;
             u[t] = (PRED && go[t]) ? ld_cg(in.pred + i) : -1;
         }
-        any |= warp_discover<PER, PRED, false>(p, s.mask, v, u, go, level, bv, bc, bd, count, S, vout, qe_out);
+        any |= warp_discover<PER, PRED, false, S>(p, s.mask, v, u, go, level, bv, bc, bd, count, vout, qe_out);
     }
     if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
     if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
@@ -1030,21 +1039,20 @@ __device__ __forceinline__ void warp_slice_gather(const BfsParams &p, int h, int
 // (warp_slice0) of the frontier's flattened edge space, builds its tables
 // for a slice (warp_slice_map), gathers kWarpSlice / 32 positions per lane
 // (a warp reads 32 consecutive positions of a run, one coalesced segment)
-// and runs the visited test (warp_discover) with no CTA barrier.  With CTAs
-// of more than 256 threads a warp's output holds half a slice: each slice is
-// tested in two halves.  (Building the next slice's tables and issuing its
-// loads before testing the current slice measured slower: 908 -> 968 us per
-// R-MAT 22 search; the second slice's registers spill.)  Same labels and frontier contents as
-// expand_range (the reference's expand-contract, expand_contract_atomic/
-// cta.cuh:82-789); the entries' order differs.  `skip_above` as in
-// emit_frontier (direction-optimizing searches).
+// and runs the visited test (warp_discover) with no CTA barrier (batch sizes
+// below).  (Building the next slice's tables and issuing its loads before
+// testing the current slice measured slower: 908 -> 968 us per R-MAT 22
+// search; the second slice's registers spill.)  Same labels and frontier
+// contents as expand_range (the reference's expand-contract,
+// expand_contract_atomic/cta.cuh:82-789); the entries' order differs.
+// `skip_above` as in emit_frontier (direction-optimizing searches).
 // With CULL = false (the expand pass of the edge-frontier strategies) the
 // gathered neighbours (and their predecessors) are written to the edge
 // frontier `eout` at their flattened positions instead: the reference's
 // two-phase expansion (two_phase/expand_atomic/cta.cuh:215-423).
 // Predecessor searches with CTAs of more than 256 threads keep the CTA-wide
 // sub-rounds (the entries' vertices would need a third table).
-template <int B, bool PRED, bool CULL = true>
+template <int B, bool PRED, bool CULL = true, bool WHOLE = false>
 __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const VertexFrontier &in,
                                                   ExpandSmem<B, PRED> &s, int level, const VertexFrontier &vout,
                                                   unsigned long long *qe_out, const EdgeFrontier *eout = nullptr,
@@ -1054,8 +1062,14 @@ __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const Vert
     constexpr int NW = B / 32;
     constexpr int PW = kWarpSlice / 32;    // positions per lane per slice
     constexpr int CAP = kChunkMax / NW;    // a warp's output entries
-    constexpr int PB = CAP / 32 < PW ? CAP / 32 : PW;  // positions per lane per visited-test batch
-    static_assert(PW % PB == 0 && PB * 32 <= CAP, "a batch's winners fit the warp's output");
+    // positions per lane per batch: with CTAs of more than 256 threads a warp's
+    // output holds half a slice, so the slice goes in two halves, except with
+    // WHOLE (top-down-only searches), which test the whole slice at once and
+    // append its winners in halves: expand-contract 888 -> 852 us per R-MAT 22
+    // search, while direction-optimizing searches and the edge strategies'
+    // copy pass measured 1-4% slower that way
+    constexpr int PB = (CULL && WHOLE) || CAP / 32 >= PW ? PW : CAP / 32;
+    static_assert(PW % PB == 0, "a slice splits into whole batches");
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     int32_t *bv = s.out + warp * CAP;
     int32_t *bc = s.colstart + warp * CAP;
@@ -1077,7 +1091,7 @@ __device__ __forceinline__ void expand_range_warp(const BfsParams &p, const Vert
             bool go[PB];
             warp_slice_gather<PB, PRED>(p, h, len, own, tcol, tver, v, u, go);
             if constexpr (CULL) {
-                any |= warp_discover<PB, PRED, true>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count, CAP,
+                any |= warp_discover<PB, PRED, true, CAP>(p, s.mask, v, u, go, level + 1, bv, bc, bd, count,
                                                      vout, qe_out, skip_above);
             } else {
 #pragma unroll
@@ -2339,8 +2353,8 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
         else if (!BU && warp_levels(p, s.E))
         {
             if constexpr (!BU && !LISTS && (B <= 256 || !PRED))
-                expand_range_warp<B, PRED>(p, p.vf[level & 1], s, level, p.vf[(level + 1) & 1],
-                                           &p.st->qe[(pass + 1) % 3]);
+                expand_range_warp<B, PRED, true, true>(p, p.vf[level & 1], s, level, p.vf[(level + 1) & 1],
+                                                       &p.st->qe[(pass + 1) % 3]);
         }
         else
         {
