@@ -908,7 +908,7 @@ __device__ __forceinline__ bool warp_discover(const BfsParams &p, uint32_t *mask
 }
 
 // Warp-autonomous contraction of the CTA's share of an edge frontier
-// (policy.warp_contract): each warp takes its slices of 32 * PER items
+// (policy.warp_contract): each warp takes its slices of 256 items
 // (warp_slice0) and runs the visited test on each with no CTA barrier;
 // winners with edges collect in the warp's slice of the shared tables and go
 // to the vertex frontier in flushes of their own (warp_emit).  A warp never
@@ -921,13 +921,16 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
                                                     const EdgeFrontier &in, int level, const VertexFrontier &vout,
                                                     unsigned long long *qe_out)
 {
-    constexpr int PER = kChunkMax / B;
+    // eight items per lane whatever the CTA size: with 512-thread CTAs a warp's
+    // output holds half a slice, and warp_discover appends the winners in halves
+    constexpr int PER = 8;
     constexpr int NW = B / 32;
-    constexpr int S = 32 * PER;  // items per slice == entries of a warp's output
+    constexpr int S = 32 * PER;           // items per slice
+    constexpr int CAP = kChunkMax / NW;   // entries of a warp's output
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int32_t *bv = s.out + warp * S;
-    int32_t *bc = s.colstart + warp * S;
-    int32_t *bd = s.rel + warp * S;
+    int32_t *bv = s.out + warp * CAP;
+    int32_t *bc = s.colstart + warp * CAP;
+    int32_t *bd = s.rel + warp * CAP;
     const int re = s.q;
     int count = 0;  // warp-uniform
     bool any = false;
@@ -943,7 +946,7 @@ __device__ __forceinline__ void contract_range_warp(const BfsParams &p, ExpandSm
             v[t] = go[t] ? ld_cg(in.v + i) : -1;
             u[t] = (PRED && go[t]) ? ld_cg(in.pred + i) : -1;
         }
-        any |= warp_discover<PER, PRED, false, S>(p, s.mask, v, u, go, level, bv, bc, bd, count, vout, qe_out);
+        any |= warp_discover<PER, PRED, false, CAP>(p, s.mask, v, u, go, level, bv, bc, bd, count, vout, qe_out);
     }
     if (count) warp_emit(p, bv, bc, bd, count, vout, qe_out);
     if (__any_sync(0xffffffffu, any) && lane == 0) s.flag = 1;  // benign race: every writer stores 1
