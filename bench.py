@@ -134,7 +134,13 @@ def visited(deg, labels):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """nvidia-smi clocks and throttle reasons sampled during the timed region.
+
+    The sampler starts before the warm-up (nvidia-smi needs a moment before its
+    first line) and samples every 20 ms; begin() and stop() bracket the timed
+    region and only the samples taken inside it count.  A region too short for
+    any sample (a few steps of a small case) falls back to the samples of the
+    0.3 s after it, and the record says which window it describes."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -143,27 +149,36 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.lines = []
+        self.lines = []  # (host monotonic time, csv line)
         self._t = None
+        self.t0 = self.t1 = None
 
-    def start(self):
+    def start(self, ready_s=5.0):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "20"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except OSError:
             self.proc = None
+            return
+        deadline = time.monotonic() + ready_s
+        while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
+            time.sleep(0.01)
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.monotonic(), line.strip()))
+
+    def begin(self):
+        self.t0 = time.monotonic()
 
     def stop(self):
         if self.proc is None:
             return None
-        time.sleep(0.25)
+        self.t1 = time.monotonic()
+        time.sleep(0.3)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
@@ -171,9 +186,15 @@ class ClockSampler:
             self.proc.kill()
         if self._t:
             self._t.join(timeout=2)
+        t0 = self.t0 if self.t0 is not None else self.t1
+        inside = [ln for t, ln in self.lines if t0 <= t <= self.t1]
+        window = "timed region"
+        if not inside:
+            inside = [ln for t, ln in self.lines if self.t1 < t <= self.t1 + 0.3]
+            window = "0.3 s after the timed region (too short for a sample)"
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for ln in inside:
             f = [x.strip() for x in ln.split(",")]
             if len(f) < 9:
                 continue
@@ -188,7 +209,7 @@ class ClockSampler:
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 def measured_peak():
@@ -684,15 +705,16 @@ def main():
         for s in srcs:
             enact(s)
 
+    clocks = ClockSampler(local)
+    clocks.start()  # before the warm-up: nvidia-smi takes a moment to print its first sample
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clocks = ClockSampler(local)
-    clocks.start()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
+    clocks.begin()
     ev0.record(stream)
     for _ in range(args.steps):
         step()
