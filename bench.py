@@ -138,11 +138,13 @@ class ClockSampler:
 
     The sampler starts before the warm-up (nvidia-smi needs a moment before its
     first line) and samples every 20 ms; begin() and stop() bracket the timed
-    region and only the samples taken inside it count.  A region too short for
-    any sample (a few steps of a small case) falls back to the samples of the
-    0.3 s after it, and the record says which window it describes."""
+    region on the host clock and only the samples whose own nvidia-smi
+    timestamp falls inside it count (its piped output arrives in bursts, so
+    arrival times say little).  A region too short for any sample (a few steps
+    of a small case) falls back to the samples of the 0.3 s after it, and the
+    record says which window it describes."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -167,17 +169,28 @@ class ClockSampler:
         while not self.lines and time.monotonic() < deadline and self.proc.poll() is None:
             time.sleep(0.01)
 
+    @staticmethod
+    def _stamp(line):
+        """The sample's own time (nvidia-smi's local timestamp) in seconds since the epoch, or None."""
+        import datetime
+        try:
+            return datetime.datetime.strptime(line.split(",")[0].strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return None
+
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append((time.monotonic(), line.strip()))
+            line = line.strip()
+            t = self._stamp(line)
+            self.lines.append((t if t is not None else time.time(), line))
 
     def begin(self):
-        self.t0 = time.monotonic()
+        self.t0 = time.time()
 
     def stop(self):
         if self.proc is None:
             return None
-        self.t1 = time.monotonic()
+        self.t1 = time.time()
         time.sleep(0.3)
         self.proc.terminate()
         try:
@@ -195,7 +208,7 @@ class ClockSampler:
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for ln in inside:
-            f = [x.strip() for x in ln.split(",")]
+            f = [x.strip() for x in ln.split(",")][1:]  # past the timestamp
             if len(f) < 9:
                 continue
             try:
