@@ -21,6 +21,10 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
     if ((rc = ensure_vf(p, 0, vcap))) return rc;
     if ((rc = ensure_slots(p))) return rc;
     BfsParams k = make_params(p, pol);
+    // hybrid's hand-off: saturation_quit queue items per 256 threads of the grid,
+    // so the frontier size at which it leaves the fused kernel does not move
+    // with the CTA size (the grid of 512-thread CTAs has half as many)
+    k.saturation = (int32_t)std::max<int64_t>(1, (int64_t)pol.saturation_quit * B / 256);
     k.edge_pingpong = pingpong ? 1 : 0;
     k.vcap = (int32_t)p->vcap[0];
     k.ecap = (int32_t)(pingpong ? std::min(p->ecap[0], p->ecap[1]) : p->ecap[0]);
@@ -62,7 +66,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         kf.hybrid = 1;
         kf.max_levels = INT32_MAX;
         kf.skip_arrival_cta = injected_skip_cta();
-        const int threshold = grid * pol.saturation_quit;
+        const int threshold = grid * k.saturation;
         while (true) {
             CUDA_TRY(cudaMemsetAsync(&p->st->barrier, 0, sizeof(unsigned long long), p->stream), "barrier reset");
             CUDA_TRY(cudaMemsetAsync(&p->st->saturated, 0, sizeof(int32_t), p->stream), "flag reset");

@@ -926,14 +926,14 @@ int b40c_bfs_enact_limited(b40c_bfs_problem *p, int strategy, int mode, int32_t 
     int rc = resolve_policy(strategy, policy, &pol);
     if (rc) return rc;
     // A caller that passes no policy at all (the reference's enactor calls)
-    // gets 512-thread CTAs for the distance searches of expand-contract,
-    // contract-expand and two-phase: measured 2-10% faster than 256 threads on
-    // R-MAT 22, random 2^21, grid2d-1000 and grid3d-256.  Predecessor searches
-    // keep 256 (their warp-by-warp levels need CTAs of at most 256 threads),
-    // and so does hybrid (its hand-off threshold scales with the grid, which
-    // halves: grid3d-256 10.4 -> 11.6 ms).
+    // gets 512-thread CTAs for the distance searches of the top-down
+    // strategies: measured 2-10% faster than 256 threads on R-MAT 22, random
+    // 2^21, grid2d-1000 and grid3d-256 (hybrid with its hand-off scaled to the
+    // CTA size, enact_edge.cu).  Predecessor searches keep 256: their
+    // warp-by-warp levels need CTAs of at most 256 threads.
     if (!policy && !p->mark_pred &&
-        (strategy == B40C_EXPAND_CONTRACT || strategy == B40C_CONTRACT_EXPAND || strategy == B40C_TWO_PHASE))
+        (strategy == B40C_EXPAND_CONTRACT || strategy == B40C_CONTRACT_EXPAND || strategy == B40C_TWO_PHASE ||
+         strategy == B40C_HYBRID))
         pol.threads = 512;
     DeviceGuard guard(p->device);
     p->timed = false;

@@ -81,13 +81,14 @@ enum {
 typedef struct b40c_bfs_policy {
     int32_t threads;               /* CTA size: 128, 256 or 512 (default 256; b40c_bfs_enact with no policy
                                       at all runs 512 for the distance searches of expand-contract,
-                                      contract-expand and two-phase) */
+                                      contract-expand, two-phase and hybrid) */
     int32_t ctas_per_sm;           /* resident CTAs per SM for persistent grids (0 = occupancy limit) */
     int32_t chunk_edges;           /* edges (or edge-frontier items) per sub-round of a CTA's share of a level:
                                       a multiple of 32 in [256, 2048] (default 2048) */
     int32_t warp_gather_threshold; /* run length at or above which a warp gathers cooperatively (>= 32) */
     int32_t cta_gather_threshold;  /* run length at or above which the CTA gathers with bulk staging */
-    int32_t saturation_quit;       /* hybrid: queue items per CTA above which the search leaves the fused kernel */
+    int32_t saturation_quit;       /* hybrid: queue items per CTA of 256 threads (scaled for other CTA sizes)
+                                      above which the search leaves the fused kernel */
     int32_t warp_cull;             /* 1: drop duplicate neighbours within a warp before the bitmask test,
                                       -1: do not (default) */
     int32_t bitmask_precheck;      /* 1: read the visited word (through L1) before the atomic test-and-set
