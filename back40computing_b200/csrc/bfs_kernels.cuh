@@ -2389,10 +2389,12 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
         if (s.flag) max_level_seen = level + 1;
         if (!p.persistent) break;
         stamp(p, pass, kPhaseArrive);
-        if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
         if ((int)blockIdx.x == p.skip_arrival_cta)
             return;  // test-only: never arrives, so the others' bounded waits must run out
         if (!duty.barrier(p.st, generation, &s_ok)) break;
+        // only after the barrier: a CTA that starts late reads cur_level as its
+        // first level, so it must not move on before every CTA has arrived once
+        if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
     }
     if (tid == 0 && max_level_seen >= 0) atomicMax(&p.st->max_level, max_level_seen);
     duty.finish();
@@ -2478,8 +2480,9 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
             __syncthreads();
             completed_level = true;
             if (p.persistent) {
-                if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
                 if (!duty.barrier(p.st, generation, &s_ok)) break;
+                // after the barrier, as in ec_kernel: late-starting CTAs read cur_level
+                if (tid == 0 && blockIdx.x == 0) p.st->cur_level = level + 1;
             }
         }
         if (!p.persistent) break;
