@@ -176,6 +176,21 @@ __device__ __forceinline__ void stamp_synced(const BfsParams &p, int pass, int p
     }
 }
 
+// Test-only (p.late_start_ns): every CTA but CTA 0 waits that long before it
+// reads its start state, like a CTA the hardware schedules late.  The wait is
+// on the global timer, with an iteration cap as well.
+__device__ __forceinline__ void late_start(const BfsParams &p)
+{
+    if (p.late_start_ns && blockIdx.x != 0) {
+        if (threadIdx.x == 0) {
+            const unsigned long long t0 = globaltimer_ns();
+            for (unsigned i = 0; i < (p.late_start_ns >> 8) + 1024 && globaltimer_ns() - t0 < p.late_start_ns; i++)
+                __nanosleep(256);
+        }
+        __syncthreads();
+    }
+}
+
 // Packed (count, degree) pair: count in the high 32 bits.
 __device__ __forceinline__ unsigned long long pack(unsigned cnt, unsigned deg)
 {
@@ -2155,6 +2170,7 @@ __global__ void __launch_bounds__(B, 1024 / B) ec_kernel(BfsParams p)
     hist_init<B, PRED>(p, s, smem_raw);
     unsigned bar_phase = 0, generation = 0;
     int max_level_seen = -1;
+    late_start(p);
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, worked = false;
     int solo_phase = 0;  // small-frontier phases so far (the same count in every CTA)
@@ -2426,6 +2442,7 @@ __global__ void __launch_bounds__(B, 1024 / B) edge_kernel(BfsParams p)
     hist_init<B, PRED>(p, s, smem_raw);
     unsigned bar_phase = 0, generation = 0;
     int max_level_seen = -1;
+    late_start(p);
     int level = ld_cg(&p.st->cur_level);
     bool limit_hit = false, saturated = false, completed_level = false;
     DutyClock duty(p);

@@ -143,6 +143,7 @@ struct BfsParams {
     int32_t saturation;       // hybrid: leave the fused kernel when items > gridDim * saturation
     int32_t persistent;       // 1: loop over levels with the grid barrier
     int32_t skip_arrival_cta; // test-only fault injection: this CTA never arrives (-1 = off)
+    uint32_t late_start_ns;   // test-only: CTAs other than 0 of a persistent launch start this late (0 = off)
     uint32_t spin_limit;      // polls before a device-side wait gives up (dev::kSpinLimit; tests pass less)
     int32_t bulk_ok;          // 1: a sub-round inside one adjacency list may be staged by cp.async.bulk
                               // (column_indices is device memory; 0 for a host-mapped CSR)

@@ -66,6 +66,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         kf.hybrid = 1;
         kf.max_levels = INT32_MAX;
         kf.skip_arrival_cta = injected_skip_cta();
+        kf.late_start_ns = injected_late_start_ns();
         const int threshold = grid * k.saturation;
         while (true) {
             CUDA_TRY(cudaMemsetAsync(&p->st->barrier, 0, sizeof(unsigned long long), p->stream), "barrier reset");
@@ -93,6 +94,7 @@ int enact_edge_t(b40c_bfs_problem *p, int strategy, int mode, int32_t src, int m
         kf.phase_mask = 3;
         kf.max_levels = INT32_MAX;
         kf.skip_arrival_cta = injected_skip_cta();
+        kf.late_start_ns = injected_late_start_ns();
         if ((rc = launch_cooperative(p, kern, grid, B, smem, kf, "cooperative launch of the contract-expand kernel")))
             return rc;
     } else if (mode == B40C_ENACT_ITERATIVE) {

@@ -73,6 +73,7 @@ int enact_ec_t(b40c_bfs_problem *p, int mode, int32_t src, int max_grid, const b
         k.persistent = 1;
         k.max_levels = INT32_MAX;
         k.skip_arrival_cta = injected_skip_cta();
+        k.late_start_ns = injected_late_start_ns();
         if ((rc = launch_cooperative(p, kern, grid, B, smem, k, "cooperative launch of the expand-contract kernel")))
             return rc;
     } else if (mode == B40C_ENACT_ITERATIVE) {

@@ -104,5 +104,16 @@ inline int injected_skip_cta()
     return inj ? atoi(inj) : -1;
 }
 
+// Test-only: B40C_TEST_LATE_START_NS=<ns> (at most 10 ms) makes every CTA
+// but CTA 0 of a persistent launch start that much later, as a CTA the
+// hardware schedules late would: the first levels then run while most of
+// the grid has not read its start state yet.
+inline uint32_t injected_late_start_ns()
+{
+    const char *inj = getenv("B40C_TEST_LATE_START_NS");
+    const long v = inj ? atol(inj) : 0;
+    return v > 0 ? (uint32_t)std::min(v, 10000000L) : 0u;
+}
+
 }  // namespace rt
 }  // namespace b40c

@@ -179,3 +179,29 @@ def test_barrier_wait_runs_out_and_the_problem_stays_usable(monkeypatch, strateg
     got = search(p, s, strategy=strategy, policy=pol)
     assert oracle.compare_labels(got, want) == -1
     p.Destroy()
+
+
+# ---- CTAs that start late ------------------------------------------------------------
+
+@pytest.mark.parametrize("strategy", [EXPAND_CONTRACT, DIRECTION_OPTIMIZING, CONTRACT_EXPAND, HYBRID])
+@pytest.mark.parametrize("threads", [256, 512])
+def test_ctas_that_start_late_join_at_the_first_level(monkeypatch, strategy, threads):
+    """Every CTA but CTA 0 of the persistent launch starts 300 us late (a
+    test-only switch), long after CTA 0 has finished its share of the first
+    level: the late CTAs still start at that level (block 0 advances the level
+    only after the end-of-level barrier), so the labels and the search depth
+    are the oracle's."""
+    g = _rmat(14)
+    p = CsrProblem.from_graph(g)
+    pol = N.Policy()
+    pol.threads = threads
+    pol.small_frontier_edges = -1  # the first level on the whole grid, not CTA 0 alone
+    monkeypatch.setenv("B40C_TEST_LATE_START_NS", "300000")
+    for s in sample_sources(g, 3, seed=9):
+        want, depth = oracle.bfs(g.row_offsets, g.column_indices, int(s))
+        got = search(p, int(s), strategy=strategy, policy=pol)
+        assert oracle.compare_labels(got, want) == -1
+        e = ENACTORS[strategy]()
+        e._problem = p
+        assert e.GetStatistics()[1] == depth
+    p.Destroy()
