@@ -4,7 +4,8 @@ Every summary gives the command that made its figures.  These checks keep
 those commands in step with bench.py: each `python bench.py ...` command line
 parses with bench.py's own parser (policy overrides included), every `ncu`
 command leaves the GPU clocks alone (`--clock-control none`), and the folder
-holds text summaries only, naming committed files.
+holds text summaries only, naming committed files (no scratch folder, no
+home-directory paths).
 """
 import glob
 import json
@@ -93,4 +94,5 @@ def test_profiles_hold_text_summaries_only():
     for path in _summaries():
         assert os.path.splitext(path)[1] in (".md", ".txt", ".json"), path
         text = open(path).read()
-        assert "_work/" not in text and "/root/" not in text, os.path.basename(path)
+        home = os.path.expanduser("~").rstrip("/") + "/"
+        assert "_work/" not in text and home not in text, os.path.basename(path)
